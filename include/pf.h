@@ -1,0 +1,170 @@
+/*
+ * pf.h -- C ABI of periodfind_b200, a B200 (sm_100a) implementation of
+ * periodfind's batched periodogram hot path: Conditional Entropy (CE),
+ * Analysis of Variance (AOV) and Lomb-Scargle (LS) over every
+ * (light curve x trial period x period derivative).
+ *
+ * Conventions
+ *  - Every function returns PF_OK (0) or a negative PF_E* code and never
+ *    exits the process; pf_last_error() describes the last failure.
+ *  - Host-pointer entry points take the same arguments the reference's
+ *    Cython wrappers pass to its C++ drivers: one host array per curve for
+ *    times and magnitudes, the curve lengths, the trial periods and period
+ *    derivatives, and a caller-owned output of n_curves * n_per * n_pdt
+ *    floats laid out [curve][period][pdt] (C order).  Magnitudes are used as
+ *    given: centring / normalisation is the caller's job, as in the
+ *    reference (periodfind/ce.pyx:167).
+ *  - A context owns its device buffers, pinned staging, stream and tuning
+ *    cache.  A context is used by one host thread at a time; distinct
+ *    contexts may run concurrently.
+ *  - Times must be finite (checked, PF_EINVAL).  Empty curves are allowed
+ *    and produce the reference CPU path's values (CE NaN, AOV 0, LS 0).
+ *
+ * mode bits
+ *  PF_MODE_PLAIN   the reference's fold operation for operation: an FP64
+ *                  divide per (point, period) (periodfind/cuda/ce.cu:141-143).
+ *  PF_MODE_CHOSEN  the tuned form: the same folded phase computed from a
+ *                  per-period reciprocal with a correction step (bit-identical
+ *                  to the plain fold), fused binning/statistics and the
+ *                  strategy the tuner picked for the curve-length class.
+ *  PF_SEM_CPU      arithmetic of the reference's CPU (Rust) path: IEEE
+ *                  divides, no multiply-add contraction, accurate libm-style
+ *                  log/sin/cos.  Without it the arithmetic follows the
+ *                  reference's CUDA build (compiled with -use_fast_math).
+ *  PF_FOLD_F32     (LS precision study) fold t/P entirely in FP32.
+ *  PF_FOLD_DF      (LS) split-precision FP32 phase frac(t * f) with the
+ *                  frequency as an unevaluated float pair; no FP64 per point.
+ */
+#ifndef PERIODFIND_B200_PF_H
+#define PERIODFIND_B200_PF_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PF_OK 0
+#define PF_EINVAL (-1)       /* bad argument                              */
+#define PF_ECUDA (-2)        /* CUDA runtime error                        */
+#define PF_ENOMEM (-3)       /* device or pinned allocation failed        */
+#define PF_EUNSUPPORTED (-4) /* valid but unsupported configuration       */
+#define PF_ETIMEOUT (-5)     /* a bounded device wait gave up             */
+
+#define PF_MODE_PLAIN 0x0
+#define PF_MODE_CHOSEN 0x1
+#define PF_SEM_CPU 0x10
+#define PF_FOLD_F32 0x100
+#define PF_FOLD_DF 0x200
+
+typedef struct pf_ctx pf_ctx;
+
+/* Library version, major * 10000 + minor * 100 + patch. */
+int pf_version(void);
+
+/* Create a context on CUDA device `device`. */
+int pf_ctx_create(pf_ctx** out, int device);
+void pf_ctx_destroy(pf_ctx* ctx);
+/* Message for the last failure on this context ("" if none).  With a NULL
+ * context, the message of the last failed pf_ctx_create on this thread. */
+const char* pf_last_error(const pf_ctx* ctx);
+
+/* ---------------------------------------------------------- periodograms */
+
+/* Replaces ConditionalEntropy::CalcCEValsBatched
+ * (periodfind/cuda/ce.h, ce.cu:420-562; bound at periodfind/ce.pyx:25-39).
+ * n_phase x n_mag histogram with phase_overlap / mag_overlap bin extents;
+ * magnitudes are expected in [0, 1) (normalise first).  Minimum is best. */
+int pf_ce(pf_ctx* ctx, const float* const* times, const float* const* mags,
+          const uint64_t* lengths, uint64_t n_curves, const float* periods,
+          uint64_t n_per, const float* period_dts, uint64_t n_pdt,
+          uint32_t n_phase, uint32_t n_mag, uint32_t phase_overlap,
+          uint32_t mag_overlap, int mode, float* out);
+
+/* Replaces AOV::CalcAOVValsBatched (periodfind/cuda/aov.h, aov.cu:429-576;
+ * bound at periodfind/aov.pyx:24-36).  Maximum is best. */
+int pf_aov(pf_ctx* ctx, const float* const* times, const float* const* mags,
+           const uint64_t* lengths, uint64_t n_curves, const float* periods,
+           uint64_t n_per, const float* period_dts, uint64_t n_pdt,
+           uint32_t n_phase, uint32_t phase_overlap, int mode, float* out);
+
+/* Replaces LombScargle::CalcLSBatched (periodfind/cuda/ls.h, ls.cu:232-359;
+ * bound at periodfind/ls.pyx:24-35).  Maximum is best. */
+int pf_ls(pf_ctx* ctx, const float* const* times, const float* const* mags,
+          const uint64_t* lengths, uint64_t n_curves, const float* periods,
+          uint64_t n_per, const float* period_dts, uint64_t n_pdt, int mode,
+          float* out);
+
+/* ----------------------------------------------------------------- peaks */
+
+/* Periodogram + top-N peak search without returning the periodogram.
+ * Replaces calc_{ce,aov,ls}_peaks_batched (rust/src/lib.rs:559-677, used by
+ * periodfind/cpu/__init__.py:148-161, :255-266, :352-362) with the peak
+ * semantics of rust/src/peaks.rs:18-238 on the flattened [period][pdt]
+ * grid: strict interior local extrema (minima for CE, maxima for AOV/LS),
+ * greedy min_distance, sorted best-first.  out_idx / out_val are
+ * [n_curves][n_peaks]; unused slots hold index -1 and value 0. */
+int pf_ce_peaks(pf_ctx* ctx, const float* const* times,
+                const float* const* mags, const uint64_t* lengths,
+                uint64_t n_curves, const float* periods, uint64_t n_per,
+                const float* period_dts, uint64_t n_pdt, uint32_t n_phase,
+                uint32_t n_mag, uint32_t phase_overlap, uint32_t mag_overlap,
+                uint32_t n_peaks, uint32_t min_distance, int mode,
+                int64_t* out_idx, float* out_val);
+int pf_aov_peaks(pf_ctx* ctx, const float* const* times,
+                 const float* const* mags, const uint64_t* lengths,
+                 uint64_t n_curves, const float* periods, uint64_t n_per,
+                 const float* period_dts, uint64_t n_pdt, uint32_t n_phase,
+                 uint32_t phase_overlap, uint32_t n_peaks,
+                 uint32_t min_distance, int mode, int64_t* out_idx,
+                 float* out_val);
+int pf_ls_peaks(pf_ctx* ctx, const float* const* times,
+                const float* const* mags, const uint64_t* lengths,
+                uint64_t n_curves, const float* periods, uint64_t n_per,
+                const float* period_dts, uint64_t n_pdt, uint32_t n_peaks,
+                uint32_t min_distance, int mode, int64_t* out_idx,
+                float* out_val);
+
+/* Peak search alone on periodograms already on the host, [n_curves][flat];
+ * replaces find_top_peaks_batched (rust/src/lib.rs:508-548). */
+int pf_find_peaks(pf_ctx* ctx, const float* data, uint64_t n_curves,
+                  uint64_t flat_len, uint32_t n_peaks, uint32_t min_distance,
+                  int use_max, int64_t* out_idx, float* out_val);
+
+/* ------------------------------------------------ device-resident callers */
+
+/* Same computations on device memory, enqueued on `stream` (a cudaStream_t;
+ * NULL = the context stream).  Curves are packed: curve c occupies
+ * [offsets[c], offsets[c+1]) of d_times / d_mags; `offsets` is a HOST array
+ * of n_curves + 1 entries (it drives the launch decomposition).  d_out is a
+ * device array of n_curves * n_per * n_pdt floats.  The call returns once
+ * the work is enqueued; it does not synchronise the stream. */
+int pf_ce_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
+              const int64_t* offsets, uint64_t n_curves,
+              const float* d_periods, uint64_t n_per, const float* d_pdts,
+              uint64_t n_pdt, uint32_t n_phase, uint32_t n_mag,
+              uint32_t phase_overlap, uint32_t mag_overlap, int mode,
+              float* d_out, void* stream);
+int pf_aov_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
+               const int64_t* offsets, uint64_t n_curves,
+               const float* d_periods, uint64_t n_per, const float* d_pdts,
+               uint64_t n_pdt, uint32_t n_phase, uint32_t phase_overlap,
+               int mode, float* d_out, void* stream);
+int pf_ls_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
+              const int64_t* offsets, uint64_t n_curves,
+              const float* d_periods, uint64_t n_per, const float* d_pdts,
+              uint64_t n_pdt, int mode, float* d_out, void* stream);
+
+/* Number of kernels this context has launched since creation (telemetry
+ * for benchmarks: launches of the library's own kernels only). */
+uint64_t pf_launch_count(const pf_ctx* ctx);
+
+/* Device time in milliseconds of the most recent fold/statistics kernel
+ * launch on this context (CUDA events around that launch), or -1. */
+double pf_last_kernel_ms(const pf_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PERIODFIND_B200_PF_H */

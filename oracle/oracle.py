@@ -1,0 +1,269 @@
+"""ctypes wrapper over the CPU oracle (oracle/oracle.c) and, when built, the
+reference's own CUDA drivers (oracle/_ref/libpfref.so via ref_shim.cu).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py.  The periodfind_b200 product never imports it.
+
+Every function takes curves as lists of float32 arrays (the reference's
+calling convention, periodfind/ce.pyx:86-95) and returns float32 arrays of
+shape [n_curves, n_periods, n_pdts] like the reference's Calc*Batched.
+Magnitude preparation (normalize / center) is the caller's job, exactly as in
+the reference, where the Cython wrapper prepares magnitudes before calling the
+batched driver (periodfind/ce.pyx:167).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+_REF_PATH = os.path.join(HERE, "_ref", "libpfref.so")
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+
+_lib = None
+_ref = None
+
+
+def build() -> str:
+    """Compile liboracle.so (the recipe is oracle/Makefile)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return _LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(
+        os.path.join(HERE, "oracle.c")
+    ):
+        build()
+    lib = ctypes.CDLL(_LIB_PATH)
+    i64, u32, c_int = ctypes.c_int64, ctypes.c_uint32, ctypes.c_int
+    lib.orc_ce_batched.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
+                                   u32, u32, u32, u32, c_int, c_int, _f32p]
+    lib.orc_aov_batched.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
+                                    u32, u32, c_int, c_int, _f32p]
+    lib.orc_ls_batched.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
+                                   c_int, c_int, _f32p]
+    lib.orc_ls_batched_f64.argtypes = [_f32p, _f32p, _i64p, i64, _f64p, i64, _f64p, i64,
+                                       c_int, _f64p]
+    lib.orc_aov_batched_f64.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
+                                        u32, u32, c_int, c_int, _f64p]
+    lib.orc_phase_f64.argtypes = [_f32p, i64, _f64p, i64, ctypes.c_double, c_int, _f64p]
+    lib.orc_ce_counts.argtypes = [_f32p, _f32p, i64, ctypes.c_float, ctypes.c_float,
+                                  u32, u32, u32, u32, c_int, _u32p]
+    lib.orc_ce_counts.restype = ctypes.c_float
+    lib.orc_aov_counts.argtypes = [_f32p, _f32p, i64, ctypes.c_float, ctypes.c_float,
+                                   u32, u32, c_int, _u32p]
+    lib.orc_aov_counts.restype = ctypes.c_float
+    lib.orc_find_top_peaks.argtypes = [_f32p, i64, i64, i64, c_int, _i64p, _f32p]
+    lib.orc_find_top_peaks.restype = i64
+    lib.orc_find_top_peaks_batched.argtypes = [_f32p, i64, i64, i64, i64, c_int, c_int,
+                                               _i64p, _f32p]
+    _lib = lib
+    return lib
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+def pack(times, mags):
+    """Concatenate per-curve arrays into CSR form (times, mags, offsets)."""
+    if len(times) != len(mags):
+        raise ValueError("times and mags must have the same number of curves")
+    lens = np.array([len(t) for t in times], dtype=np.int64)
+    offsets = np.zeros(len(times) + 1, dtype=np.int64)
+    np.cumsum(lens, out=offsets[1:])
+    t = (np.concatenate([np.asarray(x, np.float32) for x in times])
+         if len(times) else np.zeros(0, np.float32))
+    m = (np.concatenate([np.asarray(x, np.float32) for x in mags])
+         if len(mags) else np.zeros(0, np.float32))
+    return np.ascontiguousarray(t), np.ascontiguousarray(m), offsets
+
+
+def _grid(periods, pdts):
+    return (np.ascontiguousarray(periods, dtype=np.float32),
+            np.ascontiguousarray(pdts, dtype=np.float32))
+
+
+def ce(times, mags, periods, pdts, n_phase=10, n_mag=10, phase_overlap=1, mag_overlap=1,
+       fused_tcorr=False, n_threads=0):
+    """rust/src/ce.rs:39-116 batched as rust/src/lib.rs:31-88."""
+    lib = _load()
+    t, m, off = pack(times, mags)
+    p, d = _grid(periods, pdts)
+    out = np.zeros((len(off) - 1, len(p), len(d)), np.float32)
+    lib.orc_ce_batched(_ptr(t, _f32p), _ptr(m, _f32p), _ptr(off, _i64p), len(off) - 1,
+                       _ptr(p, _f32p), len(p), _ptr(d, _f32p), len(d), n_phase, n_mag,
+                       phase_overlap, mag_overlap, int(fused_tcorr), n_threads,
+                       _ptr(out, _f32p))
+    return out
+
+
+def aov(times, mags, periods, pdts, n_phase=10, phase_overlap=1, fused_tcorr=False,
+        n_threads=0):
+    """rust/src/aov.rs:12-89 batched as rust/src/lib.rs:93-145."""
+    lib = _load()
+    t, m, off = pack(times, mags)
+    p, d = _grid(periods, pdts)
+    out = np.zeros((len(off) - 1, len(p), len(d)), np.float32)
+    lib.orc_aov_batched(_ptr(t, _f32p), _ptr(m, _f32p), _ptr(off, _i64p), len(off) - 1,
+                        _ptr(p, _f32p), len(p), _ptr(d, _f32p), len(d), n_phase,
+                        phase_overlap, int(fused_tcorr), n_threads, _ptr(out, _f32p))
+    return out
+
+
+def aov_f64(times, mags, periods, pdts, n_phase=10, phase_overlap=1, fused_tcorr=False,
+            n_threads=0):
+    """AOV on the reference CPU path's bins with double sums and statistic."""
+    lib = _load()
+    t, m, off = pack(times, mags)
+    p, d = _grid(periods, pdts)
+    out = np.zeros((len(off) - 1, len(p), len(d)), np.float64)
+    lib.orc_aov_batched_f64(_ptr(t, _f32p), _ptr(m, _f32p), _ptr(off, _i64p), len(off) - 1,
+                            _ptr(p, _f32p), len(p), _ptr(d, _f32p), len(d), n_phase,
+                            phase_overlap, int(fused_tcorr), n_threads, _ptr(out, _f64p))
+    return out
+
+
+def ls(times, mags, periods, pdts, fused_tcorr=False, n_threads=0):
+    """rust/src/ls.rs:15-79 batched as rust/src/lib.rs:150-190."""
+    lib = _load()
+    t, m, off = pack(times, mags)
+    p, d = _grid(periods, pdts)
+    out = np.zeros((len(off) - 1, len(p), len(d)), np.float32)
+    lib.orc_ls_batched(_ptr(t, _f32p), _ptr(m, _f32p), _ptr(off, _i64p), len(off) - 1,
+                       _ptr(p, _f32p), len(p), _ptr(d, _f32p), len(d), int(fused_tcorr),
+                       n_threads, _ptr(out, _f32p))
+    return out
+
+
+def ls_f64(times, mags, periods, pdts, n_threads=0):
+    """All-double LS (exact oracle for precision studies); periods are taken as
+    given (pass float32 periods to evaluate on the same grid as the kernels)."""
+    lib = _load()
+    t, m, off = pack(times, mags)
+    p = np.ascontiguousarray(np.asarray(periods, dtype=np.float64))
+    d = np.ascontiguousarray(np.asarray(pdts, dtype=np.float64))
+    out = np.zeros((len(off) - 1, len(p), len(d)), np.float64)
+    lib.orc_ls_batched_f64(_ptr(t, _f32p), _ptr(m, _f32p), _ptr(off, _i64p), len(off) - 1,
+                           _ptr(p, _f64p), len(p), _ptr(d, _f64p), len(d), n_threads,
+                           _ptr(out, _f64p))
+    return out
+
+
+def phase_f64(times, periods, period_dt=0.0, n_threads=0):
+    """Exact folded phase frac((t - c t^2)/P) in double, shape [n_periods, n]."""
+    lib = _load()
+    t = np.ascontiguousarray(times, dtype=np.float32)
+    p = np.ascontiguousarray(np.asarray(periods, dtype=np.float64))
+    out = np.zeros((len(p), len(t)), np.float64)
+    lib.orc_phase_f64(_ptr(t, _f32p), len(t), _ptr(p, _f64p), len(p), float(period_dt),
+                      n_threads, _ptr(out, _f64p))
+    return out
+
+
+def ce_counts(t, m, period, pdt, n_phase=10, n_mag=10, po=1, mo=1, fused_tcorr=False):
+    """(CE value, raw u32 histogram [n_phase, n_mag]) for one cell."""
+    lib = _load()
+    t = np.ascontiguousarray(t, np.float32)
+    m = np.ascontiguousarray(m, np.float32)
+    counts = np.zeros((n_phase, n_mag), np.uint32)
+    v = lib.orc_ce_counts(_ptr(t, _f32p), _ptr(m, _f32p), len(t), float(period), float(pdt),
+                          n_phase, n_mag, po, mo, int(fused_tcorr), _ptr(counts, _u32p))
+    return v, counts
+
+
+def aov_counts(t, m, period, pdt, n_phase=10, po=1, fused_tcorr=False):
+    """(AOV value, raw u32 bin counts [n_phase]) for one cell."""
+    lib = _load()
+    t = np.ascontiguousarray(t, np.float32)
+    m = np.ascontiguousarray(m, np.float32)
+    counts = np.zeros(n_phase, np.uint32)
+    v = lib.orc_aov_counts(_ptr(t, _f32p), _ptr(m, _f32p), len(t), float(period), float(pdt),
+                           n_phase, po, int(fused_tcorr), _ptr(counts, _u32p))
+    return v, counts
+
+
+def find_top_peaks(data, n_peaks, min_distance, use_max):
+    """rust/src/peaks.rs:228-238: (indices int64, values float32), trimmed."""
+    lib = _load()
+    d = np.ascontiguousarray(np.asarray(data, dtype=np.float32).ravel())
+    n_peaks = int(n_peaks)
+    idx = np.zeros(max(n_peaks, 1), np.int64)
+    val = np.zeros(max(n_peaks, 1), np.float32)
+    k = lib.orc_find_top_peaks(_ptr(d, _f32p), len(d), n_peaks, int(min_distance),
+                               int(bool(use_max)), _ptr(idx, _i64p), _ptr(val, _f32p))
+    return idx[:k].copy(), val[:k].copy()
+
+
+def find_top_peaks_batched(data3d, n_peaks, min_distance, use_max, n_threads=0):
+    """rust/src/lib.rs:508-548: idx [n_curves, n_peaks] (-1 padded), val (0 padded)."""
+    lib = _load()
+    d = np.ascontiguousarray(np.asarray(data3d, dtype=np.float32))
+    nc = d.shape[0]
+    flat = int(np.prod(d.shape[1:])) if d.ndim > 1 else 0
+    idx = np.full((nc, n_peaks), -1, np.int64)
+    val = np.zeros((nc, n_peaks), np.float32)
+    lib.orc_find_top_peaks_batched(_ptr(d, _f32p), nc, flat, n_peaks, int(min_distance),
+                                   int(bool(use_max)), n_threads, _ptr(idx, _i64p),
+                                   _ptr(val, _f32p))
+    return idx, val
+
+
+# ----------------------------------------------------------- reference CUDA
+
+
+def ref_available() -> bool:
+    return os.path.exists(_REF_PATH)
+
+
+def _load_ref():
+    global _ref
+    if _ref is not None:
+        return _ref
+    if not ref_available():
+        raise FileNotFoundError(
+            "oracle/_ref/libpfref.so is absent (build it with `make -C oracle ref` "
+            "where the reference checkout exists)")
+    lib = ctypes.CDLL(_REF_PATH)
+    i64, u32 = ctypes.c_int64, ctypes.c_uint32
+    lib.pfref_ce.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
+                             u32, u32, u32, u32, _f32p]
+    lib.pfref_aov.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
+                              u32, u32, _f32p]
+    lib.pfref_ls.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64, _f32p]
+    _ref = lib
+    return lib
+
+
+def ref_cuda(algo, times, mags, periods, pdts, **kw):
+    """Run the reference's own CUDA driver (built from its sources) on the GPU."""
+    lib = _load_ref()
+    t, m, off = pack(times, mags)
+    p, d = _grid(periods, pdts)
+    out = np.zeros((len(off) - 1, len(p), len(d)), np.float32)
+    args = [_ptr(t, _f32p), _ptr(m, _f32p), _ptr(off, _i64p), len(off) - 1,
+            _ptr(p, _f32p), len(p), _ptr(d, _f32p), len(d)]
+    if algo == "ce":
+        lib.pfref_ce(*args, kw.get("n_phase", 10), kw.get("n_mag", 10),
+                     kw.get("phase_overlap", 1), kw.get("mag_overlap", 1), _ptr(out, _f32p))
+    elif algo == "aov":
+        lib.pfref_aov(*args, kw.get("n_phase", 10), kw.get("phase_overlap", 1),
+                      _ptr(out, _f32p))
+    elif algo == "ls":
+        lib.pfref_ls(*args, _ptr(out, _f32p))
+    else:
+        raise ValueError(algo)
+    return out

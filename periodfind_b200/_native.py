@@ -1,0 +1,168 @@
+"""ctypes binding of the C ABI in include/pf.h (libpfb200.so, built in-tree).
+
+There is no fallback: if the library is missing or no B200 is present, the
+GPU classes raise.  Build with `python -m periodfind_b200.build`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpfb200.so")
+
+PF_OK = 0
+PF_EINVAL = -1
+PF_ECUDA = -2
+PF_ENOMEM = -3
+PF_EUNSUPPORTED = -4
+PF_ETIMEOUT = -5
+
+PF_MODE_PLAIN = 0x0
+PF_MODE_CHOSEN = 0x1
+PF_SEM_CPU = 0x10
+PF_FOLD_F32 = 0x100
+PF_FOLD_DF = 0x200
+
+_vp = ctypes.c_void_p
+_u64 = ctypes.c_uint64
+_u32 = ctypes.c_uint32
+_int = ctypes.c_int
+
+# Every symbol the header declares, with its argument types.
+SIGNATURES = {
+    "pf_version": ([], _int),
+    "pf_ctx_create": ([ctypes.POINTER(_vp), _int], _int),
+    "pf_ctx_destroy": ([_vp], None),
+    "pf_last_error": ([_vp], ctypes.c_char_p),
+    "pf_ce": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32, _int,
+               _vp], _int),
+    "pf_aov": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int, _vp], _int),
+    "pf_ls": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _int, _vp], _int),
+    "pf_ce_peaks": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32,
+                     _u32, _u32, _int, _vp, _vp], _int),
+    "pf_aov_peaks": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32,
+                      _int, _vp, _vp], _int),
+    "pf_ls_peaks": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int, _vp,
+                     _vp], _int),
+    "pf_find_peaks": ([_vp, _vp, _u64, _u64, _u32, _u32, _int, _vp, _vp], _int),
+    "pf_ce_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32, _int,
+                   _vp, _vp], _int),
+    "pf_aov_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int, _vp, _vp],
+                   _int),
+    "pf_ls_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _int, _vp, _vp], _int),
+    "pf_launch_count": ([_vp], _u64),
+    "pf_last_kernel_ms": ([_vp], ctypes.c_double),
+}
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+class PeriodfindError(RuntimeError):
+    """A failure reported by the native library (status code + message)."""
+
+    def __init__(self, code, message):
+        super().__init__(f"periodfind_b200 error {code}: {message}")
+        self.code = code
+
+
+def load():
+    """Load libpfb200.so and declare its signatures (raises if absent)."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is not built; run `python -m periodfind_b200.build` "
+                "(there is no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+        return lib
+
+
+class Context:
+    """One native context (device buffers, stream, pinned staging).
+
+    Calls on one Context are serialised with a lock; the native call itself
+    runs without the GIL (ctypes releases it).
+    """
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = _vp()
+        rc = self.lib.pf_ctx_create(ctypes.byref(h), int(device))
+        if rc != PF_OK:
+            raise PeriodfindError(rc, self.lib.pf_last_error(None).decode())
+        self.handle = h
+        self.device = device
+        self.lock = threading.Lock()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.pf_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc):
+        if rc != PF_OK:
+            raise PeriodfindError(rc, self.lib.pf_last_error(self.handle).decode())
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.pf_launch_count(self.handle))
+
+    @property
+    def last_kernel_ms(self) -> float:
+        return float(self.lib.pf_last_kernel_ms(self.handle))
+
+
+_contexts: dict = {}
+_ctx_lock = threading.Lock()
+
+
+def default_context(device: int = 0) -> Context:
+    with _ctx_lock:
+        ctx = _contexts.get(device)
+        if ctx is None:
+            ctx = Context(device)
+            _contexts[device] = ctx
+        return ctx
+
+
+class CurveBatch:
+    """Per-curve host pointers and lengths for the host-pointer entry points.
+
+    Keeps references to the (contiguous float32) arrays so the pointers stay
+    valid for the duration of the native call.
+    """
+
+    def __init__(self, times, mags):
+        self.times = [np.ascontiguousarray(t, dtype=np.float32) for t in times]
+        self.mags = [np.ascontiguousarray(m, dtype=np.float32) for m in mags]
+        n = len(self.times)
+        self.n = n
+        self.tptr = np.fromiter((a.ctypes.data for a in self.times), dtype=np.uintp, count=n)
+        self.mptr = np.fromiter((a.ctypes.data for a in self.mags), dtype=np.uintp, count=n)
+        self.lengths = np.fromiter((a.shape[0] for a in self.times), dtype=np.uint64, count=n)
+
+    def args(self):
+        return (self.tptr.ctypes.data, self.mptr.ctypes.data, self.lengths.ctypes.data, self.n)
+
+
+def ptr(a) -> int:
+    return a.ctypes.data

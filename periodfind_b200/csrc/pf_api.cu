@@ -1,0 +1,852 @@
+// pf_api.cu -- the C ABI (include/pf.h): argument checks, packing, launch
+// decomposition and the device pipeline
+//     pack (host, pinned) -> one H2D copy -> preparation kernel ->
+//     fused fold/bin/statistic kernel -> periodogram D2H, or peak search
+//     on the device and a D2H of the peaks only.
+//
+// Compared with the reference's drivers (periodfind/cuda/ce.cu:420-562,
+// aov.cu:429-576, ls.cu:232-359), which allocate and free every buffer per
+// call, copy each curve with its own pageable memcpy, launch one or two
+// kernels per curve and exit() on any CUDA error, this driver keeps
+// grow-only device and pinned buffers in the context, moves the whole batch
+// in one copy, launches one kernel for the whole batch and reports errors
+// as status codes.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/pf.h"
+#include "pf_launch.h"
+#include "pf_types.h"
+
+using namespace pfk;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+thread_local std::string g_create_error;
+
+}  // namespace
+
+struct pf_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // around the fold kernel
+    cudaEvent_t ev_staged = nullptr;            // staging block copied out
+    cudaEvent_t ev_done = nullptr;              // last device-pointer call done
+    bool staged_pending = false, done_recorded = false, timed_pending = false;
+    std::string err;
+    DevBuf d_in, d_aux32, d_aux64, d_out, d_pidx, d_pval, d_pack;
+    PinnedBuf h_in;
+    uint64_t launches = 0;
+    double last_ms = -1.0;
+    int n_sm = 0;
+    size_t smem_optin = 0;
+};
+
+namespace {
+
+int fail(pf_ctx* ctx, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+    return code;
+}
+
+int cuda_fail(pf_ctx* ctx, cudaError_t e, const char* what) {
+    return fail(ctx, PF_ECUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+#define PF_CUDA(call, what)                                   \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+    } while (0)
+
+int ensure_dev(pf_ctx* ctx, DevBuf& b, size_t bytes) {
+    if (bytes <= b.cap) return PF_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t want = std::max(bytes, (size_t)256);
+    want = (want + (want >> 3) + 255) & ~(size_t)255;  // 12.5% headroom
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, PF_ENOMEM, "device allocation of %zu bytes failed: %s", want,
+                    cudaGetErrorString(e));
+    }
+    b.cap = want;
+    return PF_OK;
+}
+
+int ensure_pinned(pf_ctx* ctx, PinnedBuf& b, size_t bytes) {
+    if (bytes <= b.cap) return PF_OK;
+    if (b.p) cudaFreeHost(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t want = std::max(bytes, (size_t)4096);
+    want = (want + (want >> 3) + 4095) & ~(size_t)4095;
+    cudaError_t e = cudaHostAlloc(&b.p, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, PF_ENOMEM, "pinned allocation of %zu bytes failed: %s", want,
+                    cudaGetErrorString(e));
+    }
+    b.cap = want;
+    return PF_OK;
+}
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// What one call computes.
+struct Job {
+    int algo = ALGO_CE;
+    int mode = 0;
+    uint64_t n_curves = 0;
+    const float* periods = nullptr;  // host or device (see dev)
+    uint64_t n_per = 0;
+    const float* pdts = nullptr;
+    uint64_t n_pdt = 0;
+    uint32_t n_phase = 10, n_mag = 10, po = 1, mo = 1;
+    // outputs
+    float* out = nullptr;  // host periodogram, or device periodogram (dev)
+    bool peaks = false;
+    uint32_t n_peaks = 0, min_distance = 1;
+    int64_t* out_idx = nullptr;
+    float* out_val = nullptr;
+};
+
+// Layout of the packed input block (host staging and its device copy).
+struct Layout {
+    std::vector<int64_t> off;  // per curve, in points (multiple of 4)
+    std::vector<uint32_t> len;
+    size_t total_pts = 0;      // padded
+    size_t o_t = 0, o_m = 0, o_curves = 0, o_work = 0, o_periods = 0, o_pdts = 0, o_srcoff = 0;
+    size_t bytes = 0;
+    uint32_t n_work = 0;
+    uint32_t max_len = 0;
+};
+
+bool use_cpu_semantics(int mode) { return (mode & PF_SEM_CPU) != 0; }
+
+// The bin width the reference stores: CUDA keeps 1.0 / (float)n computed in
+// double and rounded to float (ce.cu:34-35, aov.cu:24); Rust divides in f32
+// (ce.rs:54-55, aov.rs:141).
+float bin_size(uint32_t n, bool cpu_sem) {
+    if (cpu_sem) return 1.0f / (float)n;
+    return (float)(1.0 / static_cast<float>(n));
+}
+
+int validate_common(pf_ctx* ctx, const Job& j) {
+    if (!ctx) return PF_EINVAL;
+    if (j.n_curves > 0 && (j.n_per == 0 || j.n_pdt == 0)) return PF_OK;  // nothing to compute
+    if (j.n_per > 0 && !j.periods) return fail(ctx, PF_EINVAL, "periods is NULL");
+    if (j.n_pdt > 0 && !j.pdts) return fail(ctx, PF_EINVAL, "period_dts is NULL");
+    if (j.n_per > 0xFFFFFFFFull || j.n_pdt > 0xFFFFull)
+        return fail(ctx, PF_EINVAL, "grid too large (n_per %llu, n_pdt %llu)",
+                    (unsigned long long)j.n_per, (unsigned long long)j.n_pdt);
+    if (j.n_curves > 0x7FFFFFFFull) return fail(ctx, PF_EINVAL, "too many curves");
+    if (j.algo == ALGO_CE || j.algo == ALGO_AOV) {
+        if (j.n_phase < 1 || j.n_phase > 4096)
+            return fail(ctx, PF_EINVAL, "n_phase must be in [1, 4096], got %u", j.n_phase);
+        if (j.po < 1 || j.po > j.n_phase)
+            return fail(ctx, PF_EINVAL, "phase overlap must be in [1, n_phase], got %u", j.po);
+        if (j.algo == ALGO_AOV && j.n_phase < 2)
+            return fail(ctx, PF_EINVAL, "AOV needs n_phase >= 2");
+    }
+    if (j.algo == ALGO_CE) {
+        if (j.n_mag < 1 || j.n_mag > 4096)
+            return fail(ctx, PF_EINVAL, "n_mag must be in [1, 4096], got %u", j.n_mag);
+        if (j.mo < 1 || j.mo > j.n_mag)
+            return fail(ctx, PF_EINVAL, "mag overlap must be in [1, n_mag], got %u", j.mo);
+    }
+    if (j.peaks && (!j.out_idx || !j.out_val) && j.n_peaks > 0)
+        return fail(ctx, PF_EINVAL, "peak outputs are NULL");
+    if (!j.peaks && !j.out && j.n_curves > 0) return fail(ctx, PF_EINVAL, "out is NULL");
+    return PF_OK;
+}
+
+int check_grid_host(pf_ctx* ctx, const Job& j) {
+    for (uint64_t i = 0; i < j.n_per; i++) {
+        const float P = j.periods[i];
+        if (!std::isfinite(P) || P == 0.0f)
+            return fail(ctx, PF_EINVAL, "periods[%llu] = %g must be finite and non-zero",
+                        (unsigned long long)i, (double)P);
+    }
+    for (uint64_t i = 0; i < j.n_pdt; i++) {
+        if (!std::isfinite(j.pdts[i]))
+            return fail(ctx, PF_EINVAL, "period_dts[%llu] is not finite", (unsigned long long)i);
+    }
+    return PF_OK;
+}
+
+// Launch configuration.  The private histogram must fit with at least two
+// CTAs per SM where possible; LS has no histogram.
+FoldConfig choose_config(pf_ctx* ctx, const Job& j, uint32_t max_len, bool& ok) {
+    FoldConfig c{};
+    c.algo = j.algo;
+    const bool chosen = (j.mode & PF_MODE_CHOSEN) != 0;
+    c.fold = chosen ? FOLD_EXACT : FOLD_REF;
+    if (j.algo == ALGO_LS) {
+        if (j.mode & PF_FOLD_DF) c.fold = FOLD_DF;
+        if (j.mode & PF_FOLD_F32) c.fold = FOLD_F32;
+    }
+    c.acc = AOVACC_F32;
+    if (j.algo == ALGO_AOV && chosen &&
+        (uint64_t)max_len * j.po < (1ull << (64 - kFixCountShift)) - 1ull)
+        c.acc = AOVACC_FIX;
+    c.ovl = (j.algo == ALGO_CE) ? (j.po > 1 || j.mo > 1) : (j.algo == ALGO_AOV && j.po > 1);
+    ok = false;
+    const size_t budget2 = ctx->smem_optin / 2 - 1024;  // two CTAs per SM
+    const int blocks[3] = {256, 128, 64};
+    for (int b : blocks) {
+        c.block = b;
+        if (fold_smem(c, j.n_phase, j.n_mag) <= budget2) {
+            ok = true;
+            return c;
+        }
+    }
+    for (int b : blocks) {
+        c.block = b;
+        if (fold_smem(c, j.n_phase, j.n_mag) <= ctx->smem_optin) {
+            ok = true;
+            return c;
+        }
+    }
+    return c;
+}
+
+// Work list: for each curve (longest first) and each period derivative,
+// tiles of `block` consecutive periods.
+void build_work(const Job& j, const Layout& L, int block, WorkItem* w) {
+    std::vector<uint32_t> order(j.n_curves);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return L.len[a] > L.len[b]; });
+    size_t k = 0;
+    for (uint32_t c : order) {
+        for (uint32_t d = 0; d < j.n_pdt; d++) {
+            for (uint64_t p0 = 0; p0 < j.n_per; p0 += block) {
+                w[k].curve = c;
+                w[k].pdt = d;
+                w[k].p0 = (uint32_t)p0;
+                w[k].np = (uint32_t)std::min<uint64_t>(block, j.n_per - p0);
+                k++;
+            }
+        }
+    }
+}
+
+// Copy one curve into the packed staging area, checking times are finite.
+bool copy_curve(const float* t, const float* m, uint32_t n, float* dt, float* dm, uint32_t pad) {
+    bool ok = true;
+    for (uint32_t i = 0; i < n; i++) {
+        const float x = t[i];
+        ok &= std::isfinite(x);
+        dt[i] = x;
+    }
+    if (n) memcpy(dm, m, (size_t)n * sizeof(float));
+    for (uint32_t i = n; i < pad; i++) {
+        dt[i] = 0.0f;
+        dm[i] = 0.0f;
+    }
+    return ok;
+}
+
+// Host-side plan: packed layout, launch configuration and the offsets of
+// each section in the staging block.  With `with_points` the staging block
+// also carries the curve points (host-pointer callers); device callers'
+// points are gathered on the device instead.
+int plan(pf_ctx* ctx, const Job& j, const uint64_t* lengths, bool with_points, bool with_grid,
+         Layout& L, FoldConfig& cfg) {
+    L.off.resize(j.n_curves);
+    L.len.resize(j.n_curves);
+    size_t run = 0;
+    for (uint64_t c = 0; c < j.n_curves; c++) {
+        if (lengths[c] > 0xFFFFFFFFull)
+            return fail(ctx, PF_EINVAL, "curve %llu too long", (unsigned long long)c);
+        L.off[c] = (int64_t)run;
+        L.len[c] = (uint32_t)lengths[c];
+        L.max_len = std::max(L.max_len, L.len[c]);
+        run += align_up(lengths[c], 4);
+    }
+    L.total_pts = run;
+
+    bool ok_cfg = false;
+    cfg = choose_config(ctx, j, L.max_len, ok_cfg);
+    if (!ok_cfg)
+        return fail(ctx, PF_EUNSUPPORTED,
+                    "histogram of %u x %u bins does not fit in shared memory", j.n_phase,
+                    j.algo == ALGO_CE ? j.n_mag : 1u);
+    const uint64_t tiles_per = (j.n_per + cfg.block - 1) / cfg.block;
+    const uint64_t n_work64 = j.n_curves * j.n_pdt * tiles_per;
+    if (n_work64 > 0x7FFFFFFFull) return fail(ctx, PF_EINVAL, "too much work for one launch");
+    L.n_work = (uint32_t)n_work64;
+
+    size_t o = 0;
+    L.o_t = o;
+    if (with_points) o = align_up(o + L.total_pts * 4, 256);
+    L.o_m = o;
+    if (with_points) o = align_up(o + L.total_pts * 4, 256);
+    L.o_curves = o;
+    o = align_up(o + j.n_curves * sizeof(CurveDesc), 256);
+    L.o_work = o;
+    o = align_up(o + (size_t)L.n_work * sizeof(WorkItem), 256);
+    L.o_periods = o;
+    if (with_grid) o = align_up(o + j.n_per * 4, 256);
+    L.o_pdts = o;
+    if (with_grid) o = align_up(o + j.n_pdt * 4, 256);
+    L.o_srcoff = o;
+    if (!with_points) o = align_up(o + j.n_curves * 8, 256);
+    L.bytes = o;
+    return PF_OK;
+}
+
+// Wait until the previous call's copy out of the pinned staging block has
+// finished, so the block can be rewritten.
+int staging_ready(pf_ctx* ctx) {
+    if (ctx->staged_pending) {
+        PF_CUDA(cudaEventSynchronize(ctx->ev_staged), "staging event");
+        ctx->staged_pending = false;
+    }
+    return PF_OK;
+}
+
+void fill_meta(const Job& j, const Layout& L, const FoldConfig& cfg, char* hb) {
+    CurveDesc* hc = (CurveDesc*)(hb + L.o_curves);
+    for (uint64_t c = 0; c < j.n_curves; c++) {
+        CurveDesc d{};
+        d.off = L.off[c];
+        d.n = L.len[c];
+        hc[c] = d;
+    }
+    build_work(j, L, cfg.block, (WorkItem*)(hb + L.o_work));
+}
+
+// Device pipeline shared by both entry styles: preparation kernel, fused
+// kernel, optional peak search.  `p` has the input pointers set.
+int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig& cfg,
+                    FoldParams& p, CurveDesc* dcurves, float* d_out, cudaStream_t s) {
+    const bool cpu = use_cpu_semantics(j.mode);
+    p.n_per = (uint32_t)j.n_per;
+    p.n_pdt = (uint32_t)j.n_pdt;
+    p.n_phase = j.n_phase;
+    p.n_mag = j.n_mag;
+    p.p_overlap = j.po;
+    p.m_overlap = j.mo;
+    p.phase_bin_size = bin_size(j.n_phase, cpu);
+    p.mag_bin_size = bin_size(j.n_mag, cpu);
+    p.out = d_out;
+    const uint32_t ncur = (uint32_t)j.n_curves;
+    int rc;
+    if (j.algo == ALGO_CE) {
+        if ((rc = ensure_dev(ctx, ctx->d_aux32, L.total_pts * 4 + 16)) != PF_OK) return rc;
+        p.aux32 = (const uint32_t*)ctx->d_aux32.p;
+        const int flag_sat = j.mo > 1 ? 1 : 0;
+        cudaError_t e = cpu ? launch_magbin_cpusem(p.m, (uint32_t*)ctx->d_aux32.p, dcurves, ncur,
+                                                   j.n_mag, p.mag_bin_size, flag_sat, s)
+                            : launch_magbin_cudasem(p.m, (uint32_t*)ctx->d_aux32.p, dcurves,
+                                                    ncur, j.n_mag, p.mag_bin_size, flag_sat, s);
+        PF_CUDA(e, "magnitude-bin kernel");
+        ctx->launches++;
+    } else if (j.algo == ALGO_AOV) {
+        if (cfg.acc == AOVACC_FIX) {
+            if ((rc = ensure_dev(ctx, ctx->d_aux64, L.total_pts * 8 + 32)) != PF_OK) return rc;
+            p.aux64 = (const uint64_t*)ctx->d_aux64.p;
+            PF_CUDA(launch_aov_fix_prep(p.m, (uint64_t*)ctx->d_aux64.p, dcurves, ncur, j.po, s),
+                    "AOV fixed-point preparation kernel");
+        } else {
+            PF_CUDA(launch_aov_mean(p.m, dcurves, ncur, s), "AOV mean kernel");
+        }
+        ctx->launches++;
+    }
+    PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
+    cudaError_t e = cpu ? launch_fold_cpusem(cfg, p, L.n_work, s)
+                        : launch_fold_cudasem(cfg, p, L.n_work, s);
+    PF_CUDA(e, "fold kernel launch");
+    ctx->launches++;
+    PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
+    ctx->timed_pending = true;
+    if (j.peaks && j.n_peaks > 0) {
+        const size_t pk = (size_t)j.n_curves * j.n_peaks;
+        if ((rc = ensure_dev(ctx, ctx->d_pidx, pk * 8)) != PF_OK) return rc;
+        if ((rc = ensure_dev(ctx, ctx->d_pval, pk * 4)) != PF_OK) return rc;
+        const int use_max = (j.algo == ALGO_CE) ? 0 : 1;
+        PF_CUDA(launch_peaks(d_out, j.n_curves, j.n_per * j.n_pdt, j.n_peaks, j.min_distance,
+                             use_max, (int64_t*)ctx->d_pidx.p, (float*)ctx->d_pval.p, s),
+                "peak kernel launch");
+        ctx->launches++;
+    }
+    return PF_OK;
+}
+
+void read_kernel_time(pf_ctx* ctx) {
+    if (!ctx->timed_pending) return;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->last_ms = ms;
+    else cudaGetLastError();
+    ctx->timed_pending = false;
+}
+
+// The whole pipeline for host-pointer inputs.
+int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* const* mags,
+             const uint64_t* lengths) {
+    int rc = validate_common(ctx, j);
+    if (rc != PF_OK) return rc;
+    if (j.n_curves == 0) return PF_OK;
+    if (!times || !mags || !lengths) return fail(ctx, PF_EINVAL, "times/mags/lengths is NULL");
+    const uint64_t n_cells = j.n_per * j.n_pdt;
+    if (n_cells == 0) return PF_OK;
+    if ((rc = check_grid_host(ctx, j)) != PF_OK) return rc;
+    for (uint64_t c = 0; c < j.n_curves; c++)
+        if (lengths[c] > 0 && (!times[c] || !mags[c]))
+            return fail(ctx, PF_EINVAL, "curve %llu has a NULL array", (unsigned long long)c);
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+
+    Layout L;
+    FoldConfig cfg;
+    if ((rc = plan(ctx, j, lengths, true, true, L, cfg)) != PF_OK) return rc;
+    if (cfg.fold == FOLD_DF) {
+        for (uint64_t d = 0; d < j.n_pdt; d++)
+            if (j.pdts[d] != 0.0f)
+                return fail(ctx, PF_EUNSUPPORTED,
+                            "the FP32 split-precision fold needs period_dt == 0");
+    }
+    if ((rc = staging_ready(ctx)) != PF_OK) return rc;
+    if ((rc = ensure_pinned(ctx, ctx->h_in, L.bytes)) != PF_OK) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_in, L.bytes)) != PF_OK) return rc;
+    char* hb = (char*)ctx->h_in.p;
+    float* ht = (float*)(hb + L.o_t);
+    float* hm = (float*)(hb + L.o_m);
+
+    // Pack the curves (several host threads for large batches).
+    {
+        const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        const unsigned nthr = (L.total_pts > (1u << 20)) ? hw : 1u;
+        std::vector<int> bad(nthr, 0);
+        auto worker = [&](unsigned w) {
+            for (uint64_t c = w; c < j.n_curves; c += nthr) {
+                const uint32_t n = L.len[c];
+                const uint32_t pad = (uint32_t)align_up(n, 4);
+                if (!copy_curve(times[c], mags[c], n, ht + L.off[c], hm + L.off[c], pad))
+                    bad[w] = 1;
+            }
+        };
+        if (nthr == 1) {
+            worker(0);
+        } else {
+            std::vector<std::thread> th;
+            for (unsigned w = 0; w < nthr; w++) th.emplace_back(worker, w);
+            for (auto& t : th) t.join();
+        }
+        for (int b : bad)
+            if (b) return fail(ctx, PF_EINVAL, "times must be finite");
+    }
+    fill_meta(j, L, cfg, hb);
+    memcpy(hb + L.o_periods, j.periods, j.n_per * 4);
+    memcpy(hb + L.o_pdts, j.pdts, j.n_pdt * 4);
+
+    cudaStream_t s = ctx->stream;
+    char* db = (char*)ctx->d_in.p;
+    PF_CUDA(cudaMemcpyAsync(db, hb, L.bytes, cudaMemcpyHostToDevice, s), "H2D inputs");
+    PF_CUDA(cudaEventRecord(ctx->ev_staged, s), "event");
+    ctx->staged_pending = true;
+
+    FoldParams p{};
+    p.t = (const float*)(db + L.o_t);
+    p.m = (const float*)(db + L.o_m);
+    p.curves = (const CurveDesc*)(db + L.o_curves);
+    p.work = (const WorkItem*)(db + L.o_work);
+    p.periods = (const float*)(db + L.o_periods);
+    p.pdts = (const float*)(db + L.o_pdts);
+    const size_t out_bytes = (size_t)j.n_curves * n_cells * 4;
+    if ((rc = ensure_dev(ctx, ctx->d_out, out_bytes)) != PF_OK) return rc;
+    rc = device_pipeline(ctx, j, L, cfg, p, (CurveDesc*)(db + L.o_curves), (float*)ctx->d_out.p,
+                         s);
+    if (rc != PF_OK) return rc;
+    if (!j.peaks) {
+        PF_CUDA(cudaMemcpyAsync(j.out, ctx->d_out.p, out_bytes, cudaMemcpyDeviceToHost, s),
+                "D2H periodogram");
+    } else if (j.n_peaks > 0) {
+        const size_t pk = (size_t)j.n_curves * j.n_peaks;
+        PF_CUDA(cudaMemcpyAsync(j.out_idx, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
+                "D2H peak indices");
+        PF_CUDA(cudaMemcpyAsync(j.out_val, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s),
+                "D2H peak values");
+    }
+    PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
+    ctx->staged_pending = false;
+    read_kernel_time(ctx);
+    return PF_OK;
+}
+
+// Device-pointer inputs and output, enqueued on the caller's stream.
+int run_dev(pf_ctx* ctx, const Job& j, const float* d_times, const float* d_mags,
+            const int64_t* offsets, void* stream_v) {
+    int rc = validate_common(ctx, j);
+    if (rc != PF_OK) return rc;
+    if (j.n_curves == 0) return PF_OK;
+    if (!offsets) return fail(ctx, PF_EINVAL, "offsets is NULL");
+    if (j.mode & (PF_FOLD_DF | PF_FOLD_F32))
+        return fail(ctx, PF_EUNSUPPORTED, "fold study modes take host inputs");
+    const uint64_t n_cells = j.n_per * j.n_pdt;
+    if (n_cells == 0) return PF_OK;
+    std::vector<uint64_t> lengths(j.n_curves);
+    for (uint64_t c = 0; c < j.n_curves; c++) {
+        if (offsets[c + 1] < offsets[c] || offsets[c] < 0)
+            return fail(ctx, PF_EINVAL, "offsets must be non-decreasing and non-negative");
+        lengths[c] = (uint64_t)(offsets[c + 1] - offsets[c]);
+    }
+    if (offsets[j.n_curves] > 0 && (!d_times || !d_mags))
+        return fail(ctx, PF_EINVAL, "d_times/d_mags is NULL");
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = stream_v ? (cudaStream_t)stream_v : ctx->stream;
+
+    Layout L;
+    FoldConfig cfg;
+    if ((rc = plan(ctx, j, lengths.data(), false, false, L, cfg)) != PF_OK) return rc;
+    if ((rc = staging_ready(ctx)) != PF_OK) return rc;
+    if ((rc = ensure_pinned(ctx, ctx->h_in, L.bytes)) != PF_OK) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_in, L.bytes)) != PF_OK) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_pack, L.total_pts * 8 + 64)) != PF_OK) return rc;
+    char* hb = (char*)ctx->h_in.p;
+    fill_meta(j, L, cfg, hb);
+    memcpy(hb + L.o_srcoff, offsets, j.n_curves * 8);
+
+    // Order this call after the previous one on this context (its buffers
+    // are reused), whichever stream that one ran on.
+    if (ctx->done_recorded) PF_CUDA(cudaStreamWaitEvent(s, ctx->ev_done, 0), "stream wait");
+    char* db = (char*)ctx->d_in.p;
+    PF_CUDA(cudaMemcpyAsync(db, hb, L.bytes, cudaMemcpyHostToDevice, s), "H2D metadata");
+    PF_CUDA(cudaEventRecord(ctx->ev_staged, s), "event");
+    ctx->staged_pending = true;
+
+    float* pt = (float*)ctx->d_pack.p;
+    float* pm = pt + L.total_pts;
+    CurveDesc* dcurves = (CurveDesc*)(db + L.o_curves);
+    PF_CUDA(launch_pack(d_times, d_mags, (const int64_t*)(db + L.o_srcoff), dcurves,
+                        (uint32_t)j.n_curves, pt, pm, s),
+            "pack kernel");
+    ctx->launches++;
+    FoldParams p{};
+    p.t = pt;
+    p.m = pm;
+    p.curves = dcurves;
+    p.work = (const WorkItem*)(db + L.o_work);
+    p.periods = j.periods;
+    p.pdts = j.pdts;
+    rc = device_pipeline(ctx, j, L, cfg, p, dcurves, j.out, s);
+    if (rc != PF_OK) return rc;
+    PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
+    ctx->done_recorded = true;
+    return PF_OK;
+}
+
+}  // namespace
+
+size_t pfk::fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag) {
+    return fold_smem_bytes(c.algo, c.fold, c.acc, c.block, c.ovl, n_phase, n_mag);
+}
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" {
+
+int pf_version(void) { return 100; }
+
+int pf_ctx_create(pf_ctx** out, int device) {
+    if (!out) return PF_EINVAL;
+    *out = nullptr;
+    int n_dev = 0;
+    cudaError_t e = cudaGetDeviceCount(&n_dev);
+    if (e != cudaSuccess || n_dev == 0) {
+        cudaGetLastError();
+        g_create_error = std::string("no CUDA device available: ") + cudaGetErrorString(e);
+        return PF_ECUDA;
+    }
+    if (device < 0 || device >= n_dev) {
+        g_create_error = "device index out of range";
+        return PF_EINVAL;
+    }
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) {
+        g_create_error = cudaGetErrorString(e);
+        return PF_ECUDA;
+    }
+    if (prop.major != 10) {
+        g_create_error = "this library is built for sm_100a (B200); device is sm_" +
+                         std::to_string(prop.major) + std::to_string(prop.minor);
+        return PF_EUNSUPPORTED;
+    }
+    pf_ctx* ctx = new pf_ctx();
+    ctx->device = device;
+    ctx->n_sm = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+    if ((e = cudaSetDevice(device)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&ctx->ev0)) != cudaSuccess ||
+        (e = cudaEventCreate(&ctx->ev1)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_staged, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_done, cudaEventDisableTiming)) != cudaSuccess) {
+        g_create_error = cudaGetErrorString(e);
+        delete ctx;
+        return PF_ECUDA;
+    }
+    *out = ctx;
+    return PF_OK;
+}
+
+void pf_ctx_destroy(pf_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->done_recorded) cudaEventSynchronize(ctx->ev_done);
+    for (DevBuf* b : {&ctx->d_in, &ctx->d_aux32, &ctx->d_aux64, &ctx->d_out, &ctx->d_pidx,
+                      &ctx->d_pval, &ctx->d_pack})
+        if (b->p) cudaFree(b->p);
+    if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->ev_staged) cudaEventDestroy(ctx->ev_staged);
+    if (ctx->ev_done) cudaEventDestroy(ctx->ev_done);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* pf_last_error(const pf_ctx* ctx) {
+    if (!ctx) return g_create_error.c_str();
+    return ctx->err.c_str();
+}
+
+uint64_t pf_launch_count(const pf_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+double pf_last_kernel_ms(const pf_ctx* ctx) {
+    if (!ctx) return -1.0;
+    pf_ctx* c = const_cast<pf_ctx*>(ctx);
+    if (c->timed_pending && cudaEventQuery(c->ev1) == cudaSuccess) read_kernel_time(c);
+    return c->last_ms;
+}
+
+int pf_ce(pf_ctx* ctx, const float* const* times, const float* const* mags,
+          const uint64_t* lengths, uint64_t n_curves, const float* periods, uint64_t n_per,
+          const float* period_dts, uint64_t n_pdt, uint32_t n_phase, uint32_t n_mag,
+          uint32_t phase_overlap, uint32_t mag_overlap, int mode, float* out) {
+    Job j;
+    j.algo = ALGO_CE;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = period_dts;
+    j.n_pdt = n_pdt;
+    j.n_phase = n_phase;
+    j.n_mag = n_mag;
+    j.po = phase_overlap;
+    j.mo = mag_overlap;
+    j.out = out;
+    return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_aov(pf_ctx* ctx, const float* const* times, const float* const* mags,
+           const uint64_t* lengths, uint64_t n_curves, const float* periods, uint64_t n_per,
+           const float* period_dts, uint64_t n_pdt, uint32_t n_phase, uint32_t phase_overlap,
+           int mode, float* out) {
+    Job j;
+    j.algo = ALGO_AOV;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = period_dts;
+    j.n_pdt = n_pdt;
+    j.n_phase = n_phase;
+    j.po = phase_overlap;
+    j.out = out;
+    return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_ls(pf_ctx* ctx, const float* const* times, const float* const* mags,
+          const uint64_t* lengths, uint64_t n_curves, const float* periods, uint64_t n_per,
+          const float* period_dts, uint64_t n_pdt, int mode, float* out) {
+    Job j;
+    j.algo = ALGO_LS;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = period_dts;
+    j.n_pdt = n_pdt;
+    j.out = out;
+    return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_ce_peaks(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                const uint64_t* lengths, uint64_t n_curves, const float* periods,
+                uint64_t n_per, const float* period_dts, uint64_t n_pdt, uint32_t n_phase,
+                uint32_t n_mag, uint32_t phase_overlap, uint32_t mag_overlap, uint32_t n_peaks,
+                uint32_t min_distance, int mode, int64_t* out_idx, float* out_val) {
+    Job j;
+    j.algo = ALGO_CE;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = period_dts;
+    j.n_pdt = n_pdt;
+    j.n_phase = n_phase;
+    j.n_mag = n_mag;
+    j.po = phase_overlap;
+    j.mo = mag_overlap;
+    j.peaks = true;
+    j.n_peaks = n_peaks;
+    j.min_distance = min_distance;
+    j.out_idx = out_idx;
+    j.out_val = out_val;
+    return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_aov_peaks(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                 const uint64_t* lengths, uint64_t n_curves, const float* periods,
+                 uint64_t n_per, const float* period_dts, uint64_t n_pdt, uint32_t n_phase,
+                 uint32_t phase_overlap, uint32_t n_peaks, uint32_t min_distance, int mode,
+                 int64_t* out_idx, float* out_val) {
+    Job j;
+    j.algo = ALGO_AOV;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = period_dts;
+    j.n_pdt = n_pdt;
+    j.n_phase = n_phase;
+    j.po = phase_overlap;
+    j.peaks = true;
+    j.n_peaks = n_peaks;
+    j.min_distance = min_distance;
+    j.out_idx = out_idx;
+    j.out_val = out_val;
+    return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_ls_peaks(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                const uint64_t* lengths, uint64_t n_curves, const float* periods,
+                uint64_t n_per, const float* period_dts, uint64_t n_pdt, uint32_t n_peaks,
+                uint32_t min_distance, int mode, int64_t* out_idx, float* out_val) {
+    Job j;
+    j.algo = ALGO_LS;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = period_dts;
+    j.n_pdt = n_pdt;
+    j.peaks = true;
+    j.n_peaks = n_peaks;
+    j.min_distance = min_distance;
+    j.out_idx = out_idx;
+    j.out_val = out_val;
+    return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_ce_dev(pf_ctx* ctx, const float* d_times, const float* d_mags, const int64_t* offsets,
+              uint64_t n_curves, const float* d_periods, uint64_t n_per, const float* d_pdts,
+              uint64_t n_pdt, uint32_t n_phase, uint32_t n_mag, uint32_t phase_overlap,
+              uint32_t mag_overlap, int mode, float* d_out, void* stream) {
+    Job j;
+    j.algo = ALGO_CE;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = d_periods;
+    j.n_per = n_per;
+    j.pdts = d_pdts;
+    j.n_pdt = n_pdt;
+    j.n_phase = n_phase;
+    j.n_mag = n_mag;
+    j.po = phase_overlap;
+    j.mo = mag_overlap;
+    j.out = d_out;
+    return run_dev(ctx, j, d_times, d_mags, offsets, stream);
+}
+
+int pf_aov_dev(pf_ctx* ctx, const float* d_times, const float* d_mags, const int64_t* offsets,
+               uint64_t n_curves, const float* d_periods, uint64_t n_per, const float* d_pdts,
+               uint64_t n_pdt, uint32_t n_phase, uint32_t phase_overlap, int mode, float* d_out,
+               void* stream) {
+    Job j;
+    j.algo = ALGO_AOV;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = d_periods;
+    j.n_per = n_per;
+    j.pdts = d_pdts;
+    j.n_pdt = n_pdt;
+    j.n_phase = n_phase;
+    j.po = phase_overlap;
+    j.out = d_out;
+    return run_dev(ctx, j, d_times, d_mags, offsets, stream);
+}
+
+int pf_ls_dev(pf_ctx* ctx, const float* d_times, const float* d_mags, const int64_t* offsets,
+              uint64_t n_curves, const float* d_periods, uint64_t n_per, const float* d_pdts,
+              uint64_t n_pdt, int mode, float* d_out, void* stream) {
+    Job j;
+    j.algo = ALGO_LS;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = d_periods;
+    j.n_per = n_per;
+    j.pdts = d_pdts;
+    j.n_pdt = n_pdt;
+    j.out = d_out;
+    return run_dev(ctx, j, d_times, d_mags, offsets, stream);
+}
+
+int pf_find_peaks(pf_ctx* ctx, const float* data, uint64_t n_curves, uint64_t flat_len,
+                  uint32_t n_peaks, uint32_t min_distance, int use_max, int64_t* out_idx,
+                  float* out_val) {
+    if (!ctx) return PF_EINVAL;
+    if (n_curves == 0 || n_peaks == 0) return PF_OK;
+    if (!data || !out_idx || !out_val) return fail(ctx, PF_EINVAL, "NULL argument");
+    if (n_curves > 0x7FFFFFFFull) return fail(ctx, PF_EINVAL, "too many curves");
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const size_t in_bytes = (size_t)n_curves * flat_len * 4;
+    const size_t pk = (size_t)n_curves * n_peaks;
+    int rc = ensure_dev(ctx, ctx->d_out, in_bytes);
+    if (rc != PF_OK) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_pidx, pk * 8)) != PF_OK) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_pval, pk * 4)) != PF_OK) return rc;
+    cudaStream_t s = ctx->stream;
+    PF_CUDA(cudaMemcpyAsync(ctx->d_out.p, data, in_bytes, cudaMemcpyHostToDevice, s), "H2D");
+    PF_CUDA(launch_peaks((const float*)ctx->d_out.p, n_curves, flat_len, n_peaks, min_distance,
+                         use_max, (int64_t*)ctx->d_pidx.p, (float*)ctx->d_pval.p, s),
+            "peak kernel launch");
+    ctx->launches++;
+    PF_CUDA(cudaMemcpyAsync(out_idx, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    PF_CUDA(cudaMemcpyAsync(out_val, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
+    return PF_OK;
+}
+
+}  // extern "C"

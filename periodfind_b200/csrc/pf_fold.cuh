@@ -1,0 +1,467 @@
+// pf_fold.cuh -- fused fold / bin / statistic kernels for CE, AOV and LS.
+//
+// Included by exactly two translation units that differ only in compiler
+// flags, which is how the reference's two implementations differ:
+//   kern_cudasem.cu  -use_fast_math: approximate f32 divides, fast log/sincos,
+//                    FTZ, multiply-add contraction -- the reference's CUDA
+//                    build (setup.py:129, periodfind/cuda/*.cu).
+//   kern_cpusem.cu   IEEE divides, accurate log/sin/cos, no contraction --
+//                    the reference's CPU path (rust/src/{fold,ce,aov,ls}.rs).
+// Expressions that the reference writes the same way in both are written
+// here once, verbatim in shape, so each translation unit reproduces its
+// reference's rounding.  Arithmetic that must not depend on the flags
+// (the exact fold, fixed-point statistics) uses explicit _rn intrinsics.
+//
+// Decomposition (thread per cell): a CTA takes one curve, one period
+// derivative and up to BLOCK consecutive trial periods; thread j owns trial
+// period p0 + j for the whole curve.  The curve is streamed through shared
+// memory in tiles of kTile points; every thread of a warp reads the same
+// point (a broadcast), so point data costs one shared load per warp-step.
+// Each thread's histogram is private and laid out [bin][thread] in shared
+// memory, so every warp-wide update hits 32 distinct banks; updates are
+// fire-and-forget shared atomics (no read-after-write chain between points).
+// The statistic is finished in the same kernel from the private histogram:
+// no histogram round trip through global memory (periodfind/cuda/ce.cu:
+// 160-167 writes one 4*n_bins-byte histogram per (period, pdt) to HBM).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+#include "pf_types.h"
+
+#ifndef PF_SEM_CPU_TU
+#error "define PF_SEM_CPU_TU to 0 (reference CUDA arithmetic) or 1 (reference CPU arithmetic)"
+#endif
+#ifndef PF_KNS
+#error "define PF_KNS, the namespace that keeps this unit's kernels distinct"
+#endif
+
+namespace pfk {
+// Each including unit gets its own namespace: the two units compile the same
+// templates with different arithmetic, so their symbols must not merge.
+namespace PF_KNS {
+
+// periodfind/cuda/ls.cu:18 and rust/src/ls.rs:13 (both 6.2831855f).
+constexpr float kTwoPi = 6.283185307179586f;
+
+struct Cell {
+    float period, pdt_corr;
+    double Pd, yhi, ylo, c;
+    float fhi, flo;
+};
+
+template <int FOLD>
+__device__ __forceinline__ void cell_setup(Cell& s, float period, float period_dt) {
+    s.period = period;
+    // periodfind/cuda/ce.cu:125, aov.cu:68, ls.cu:65; rust/src/fold.rs:13-15.
+    s.pdt_corr = (period_dt / period) / 2;
+    if (FOLD == FOLD_EXACT || FOLD == FOLD_DF) {
+        // 1/P as a double-double (yhi + ylo): yhi = RN(1/P); the residual
+        // 1 - P*yhi is exact in one fma, and ylo = residual * yhi.
+        s.Pd = (double)period;
+        s.yhi = __drcp_rn(s.Pd);
+        const double r = __fma_rn(-s.Pd, s.yhi, 1.0);
+        s.ylo = __dmul_rn(r, s.yhi);
+        s.c = (double)s.pdt_corr;
+    }
+    if (FOLD == FOLD_DF) {
+        // f = 1/P as an unevaluated float pair for the FP32 phase.
+        s.fhi = __double2float_rn(s.yhi);
+        s.flo = __double2float_rn(__dadd_rn(__dadd_rn(s.yhi, -(double)s.fhi), s.ylo));
+    }
+}
+
+// The reference fold, operation for operation (periodfind/cuda/ce.cu:140-143,
+// aov.cu:106-109, ls.cu:95-97; rust/src/fold.rs:22-26).
+__device__ __forceinline__ float fold_ref(float t, const Cell& s) {
+    double t_corr_d = (double)t - (double)s.pdt_corr * (double)t * (double)t;
+    double ratio_d = t_corr_d / (double)s.period;
+    return fabsf((float)(ratio_d - floor(ratio_d)));
+}
+
+// Same result as fold_ref without a divide.  For a double a and a period P
+// that is an f32 value, the exact quotient a/P is at least 2^-77 (relative)
+// away from every rounding midpoint of double precision (a - m*P is a
+// nonzero multiple of 2^(e_a - 77) for any 54-bit midpoint m), while
+// qh + lo below approximates a/P to ~2^-103.  RN(qh + lo) is therefore the
+// correctly rounded quotient, i.e. exactly what the FP64 divide returns.
+template <bool HAS_PDT>
+__device__ __forceinline__ float fold_exact(double td, const Cell& s) {
+    double a;
+    if constexpr (HAS_PDT) {
+        // Same expression as the reference, so the same contraction.
+        a = td - s.c * td * td;
+    } else {
+        a = td;
+    }
+    const double qh = __dmul_rn(a, s.yhi);
+    const double e = __fma_rn(a, s.yhi, -qh);
+    const double lo = __fma_rn(a, s.ylo, e);
+    const double q = __dadd_rn(qh, lo);
+    return fabsf((float)(q - floor(q)));
+}
+
+// All-FP32 fold (precision study only: loses ~1e-3 cycles at 1e4-1e5 cycles).
+__device__ __forceinline__ float fold_f32(float t, const Cell& s) {
+    const float tc = t - s.pdt_corr * t * t;
+    const float r = tc / s.period;
+    return fabsf(r - floorf(r));
+}
+
+// Split-precision FP32 phase frac(t * f), f = fhi + flo; result in turns in
+// [-0.5, 0.5] (pdt == 0 only; |t * fhi| < 2^22 checked on the host).
+__device__ __forceinline__ float fold_df(float t, const Cell& s) {
+    const float p = __fmul_rn(t, s.fhi);
+    const float e = __fmaf_rn(t, s.fhi, -p);
+    const float e2 = __fmaf_rn(t, s.flo, e);
+    const float k = __fsub_rn(__fadd_rn(p, 12582912.0f), 12582912.0f);
+    return __fadd_rn(__fsub_rn(p, k), e2);
+}
+
+// trunc(q) for finite q in [0, 2^23): identical to the reference's
+// (size_t) conversion on that range, without a conversion instruction.
+__device__ __forceinline__ unsigned trunc_u(float q) {
+    return __float_as_uint(__fadd_rz(q, 8388608.0f)) - 0x4B000000u;
+}
+
+template <int FOLD>
+using tile_t_type = typename std::conditional<FOLD == FOLD_EXACT, double, float>::type;
+
+// Private per-thread accumulators (LS) and shared-memory views of one CTA.
+struct Views {
+    float* tile_tf;
+    double* tile_td;
+    uint32_t* tile_a;
+    unsigned long long* tile_a64;
+    uint32_t* hist;               // CE counts, [slot][BLOCK]
+    unsigned long long* hist64;   // AOV FIX, [slot][BLOCK]
+    uint32_t* a_cnt;              // AOV F32, [bin][BLOCK] x 3
+    float* a_sum;
+    float* a_sq;
+};
+
+struct LSAcc {
+    float mag_cos, mag_sin, cos_cos, cos_sin;
+};
+
+// Stream the curve through shared memory and accumulate this thread's cell.
+template <int ALGO, int FOLD, int ACC, int BLOCK, bool OVL, bool HAS_PDT>
+__device__ __forceinline__ void accumulate(const FoldParams& p, const Views& v, const Cell& s,
+                                           int64_t off, uint32_t n, bool active, LSAcc& ls) {
+    using TT = tile_t_type<FOLD>;
+    TT* tile_t;
+    if constexpr (FOLD == FOLD_EXACT) tile_t = v.tile_td; else tile_t = v.tile_tf;
+    const int tid = threadIdx.x;
+    const uint32_t nP = p.n_phase, nM = p.n_mag;
+    const uint32_t po = p.p_overlap, mo = p.m_overlap;
+    const float phase_bin_size = p.phase_bin_size;
+
+    for (uint32_t base = 0; base < n; base += kTile) {
+        const uint32_t cnt = min(kTile, n - base);
+        __syncthreads();
+        // Stage the tile with 16-byte loads (curves start 16-byte aligned
+        // and are padded to a multiple of 4 points).
+        {
+            const float4* gt = reinterpret_cast<const float4*>(p.t + off + base);
+            const uint32_t n4 = (cnt + 3) >> 2;
+            for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
+                const float4 q = gt[i4];
+                tile_t[4 * i4 + 0] = (TT)q.x;
+                tile_t[4 * i4 + 1] = (TT)q.y;
+                tile_t[4 * i4 + 2] = (TT)q.z;
+                tile_t[4 * i4 + 3] = (TT)q.w;
+            }
+            if constexpr (ALGO == ALGO_CE) {
+                const uint4* ga = reinterpret_cast<const uint4*>(p.aux32 + off + base);
+                uint4* sa = reinterpret_cast<uint4*>(v.tile_a);
+                for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) sa[i4] = ga[i4];
+            } else if constexpr (ALGO == ALGO_AOV && ACC == AOVACC_FIX) {
+                const ulonglong2* ga = reinterpret_cast<const ulonglong2*>(p.aux64 + off + base);
+                ulonglong2* sa = reinterpret_cast<ulonglong2*>(v.tile_a64);
+                for (uint32_t i2 = tid; i2 < 2 * n4; i2 += BLOCK) sa[i2] = ga[i2];
+            } else {
+                const uint4* ga = reinterpret_cast<const uint4*>(p.m + off + base);
+                uint4* sa = reinterpret_cast<uint4*>(v.tile_a);
+                for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) sa[i4] = ga[i4];
+            }
+        }
+        __syncthreads();
+        if (!active) continue;
+
+#pragma unroll 4
+        for (uint32_t i = 0; i < cnt; i++) {
+            float folded;
+            if constexpr (FOLD == FOLD_REF) {
+                folded = fold_ref(tile_t[i], s);
+            } else if constexpr (FOLD == FOLD_EXACT) {
+                folded = fold_exact<HAS_PDT>(tile_t[i], s);
+            } else if constexpr (FOLD == FOLD_F32) {
+                folded = fold_f32(tile_t[i], s);
+            } else {
+                folded = fold_df(tile_t[i], s);
+            }
+
+            if constexpr (ALGO == ALGO_LS) {
+                // periodfind/cuda/ls.cu:92-104; rust/src/ls.rs:242-251.
+                const float mag = __uint_as_float(v.tile_a[i]);
+                float sin_val, cos_val;
+                sincosf(kTwoPi * folded, &sin_val, &cos_val);
+                ls.mag_cos += mag * cos_val;
+                ls.mag_sin += mag * sin_val;
+                ls.cos_cos += cos_val * cos_val;
+                ls.cos_sin += cos_val * sin_val;
+            } else {
+                // PhaseBin: (size_t)(folded / phase_bin_size)  (ce.cu:66-68,
+                // aov.cu:35-37; ce.rs:78, aov.rs:172).  folded <= 1, so the
+                // bin is at most n_phase (the reference wraps it with %).
+                const unsigned pb = min(trunc_u(folded / phase_bin_size), nP);
+                if constexpr (ALGO == ALGO_CE) {
+                    const uint32_t a = v.tile_a[i];
+                    if constexpr (!OVL) {
+                        // Row n_phase is folded into row 0 after the loop.
+                        atomicAdd(&v.hist[(pb * nM + a) * BLOCK + tid], 1u);
+                    } else {
+                        // ce.cu:148-155 / ce.rs:82-89 with wrapping bins.
+                        const uint32_t mb = a & 0x7FFFFFFFu;
+                        const bool sat = (a >> 31) != 0u;
+                        for (uint32_t ii = 0; ii < po; ii++) {
+                            const uint32_t row = (pb + ii) % nP;
+                            for (uint32_t jj = 0; jj < mo; jj++) {
+                                const uint32_t col =
+                                    sat ? (jj == 0 ? mb : (jj - 1) % nM) : (mb + jj) % nM;
+                                atomicAdd(&v.hist[(row * nM + col) * BLOCK + tid], 1u);
+                            }
+                        }
+                    }
+                } else {  // AOV
+                    if constexpr (ACC == AOVACC_FIX) {
+                        const unsigned long long q = v.tile_a64[i];
+                        if constexpr (!OVL) {
+                            atomicAdd(&v.hist64[pb * BLOCK + tid], q);
+                        } else {
+                            for (uint32_t o = 0; o < po; o++)
+                                atomicAdd(&v.hist64[((pb + o) % nP) * BLOCK + tid], q);
+                        }
+                    } else {
+                        // aov.cu:111-122 / aov.rs:173-180, in point order.
+                        const float mag = __uint_as_float(v.tile_a[i]);
+                        const float mag_sq = mag * mag;
+                        if constexpr (!OVL) {
+                            const uint32_t b = (pb >= nP) ? pb - nP : pb;
+                            atomicAdd(&v.a_cnt[b * BLOCK + tid], 1u);
+                            atomicAdd(&v.a_sum[b * BLOCK + tid], mag);
+                            atomicAdd(&v.a_sq[b * BLOCK + tid], mag_sq);
+                        } else {
+                            for (uint32_t o = 0; o < po; o++) {
+                                const uint32_t b = (pb + o) % nP;
+                                atomicAdd(&v.a_cnt[b * BLOCK + tid], 1u);
+                                atomicAdd(&v.a_sum[b * BLOCK + tid], mag);
+                                atomicAdd(&v.a_sq[b * BLOCK + tid], mag_sq);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int ALGO, int FOLD, int ACC, int BLOCK, bool OVL>
+__global__ void __launch_bounds__(BLOCK) fold_kernel(const FoldParams p) {
+    using TT = tile_t_type<FOLD>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr size_t kAuxBytes = (ALGO == ALGO_AOV && ACC == AOVACC_FIX) ? 8 : 4;
+    unsigned char* after_t = smem + kTile * sizeof(TT);
+    unsigned char* hist_raw = after_t + kTile * kAuxBytes;
+
+    const uint32_t nP = p.n_phase, nM = p.n_mag;
+    const uint32_t po = p.p_overlap, mo = p.m_overlap;
+
+    Views v;
+    v.tile_tf = reinterpret_cast<float*>(smem);
+    v.tile_td = reinterpret_cast<double*>(smem);
+    v.tile_a = reinterpret_cast<uint32_t*>(after_t);
+    v.tile_a64 = reinterpret_cast<unsigned long long*>(after_t);
+    v.hist = reinterpret_cast<uint32_t*>(hist_raw);
+    v.hist64 = reinterpret_cast<unsigned long long*>(hist_raw);
+    v.a_cnt = reinterpret_cast<uint32_t*>(hist_raw);
+    v.a_sum = reinterpret_cast<float*>(hist_raw) + (size_t)nP * BLOCK;
+    v.a_sq = reinterpret_cast<float*>(hist_raw) + (size_t)2 * nP * BLOCK;
+
+    const WorkItem w = p.work[blockIdx.x];
+    const CurveDesc cd = p.curves[w.curve];
+    const uint32_t n = cd.n;
+    const int tid = threadIdx.x;
+    const bool active = (uint32_t)tid < w.np;
+    const uint32_t pi = w.p0 + (active ? (uint32_t)tid : 0u);
+    const float period_dt = p.pdts[w.pdt];
+
+    Cell s;
+    cell_setup<FOLD>(s, p.periods[pi], period_dt);
+
+    // Zero this thread's column of the private histogram.
+    if constexpr (ALGO == ALGO_CE) {
+        const uint32_t slots = (OVL ? nP : nP + 1) * nM;
+        for (uint32_t k = 0; k < slots; k++) v.hist[k * BLOCK + tid] = 0u;
+    } else if constexpr (ALGO == ALGO_AOV) {
+        if constexpr (ACC == AOVACC_FIX) {
+            const uint32_t slots = OVL ? nP : nP + 1;
+            for (uint32_t k = 0; k < slots; k++) v.hist64[k * BLOCK + tid] = 0ull;
+        } else {
+            for (uint32_t k = 0; k < nP; k++) {
+                v.a_cnt[k * BLOCK + tid] = 0u;
+                v.a_sum[k * BLOCK + tid] = 0.0f;
+                v.a_sq[k * BLOCK + tid] = 0.0f;
+            }
+        }
+    }
+
+    LSAcc ls{0.0f, 0.0f, 0.0f, 0.0f};
+    // The period derivative is uniform over the CTA: pick the loop once.
+    if (period_dt != 0.0f)
+        accumulate<ALGO, FOLD, ACC, BLOCK, OVL, true>(p, v, s, cd.off, n, active, ls);
+    else
+        accumulate<ALGO, FOLD, ACC, BLOCK, OVL, false>(p, v, s, cd.off, n, active, ls);
+
+    if (!active) return;
+    const size_t out_idx =
+        (size_t)w.curve * ((size_t)p.n_per * p.n_pdt) + (size_t)pi * p.n_pdt + w.pdt;
+
+    if constexpr (ALGO == ALGO_CE) {
+        uint32_t* hist = v.hist;
+        if constexpr (!OVL) {
+            for (uint32_t mb = 0; mb < nM; mb++)
+                hist[mb * BLOCK + tid] += hist[(nP * nM + mb) * BLOCK + tid];
+        }
+        const float divf = (float)((unsigned long long)n * po * mo);
+        float ce = 0.0f;
+        for (uint32_t j = 0; j < nP; j++) {
+            float p_j = 0.0f;
+            for (uint32_t i = 0; i < nM; i++) p_j += (float)hist[(j * nM + i) * BLOCK + tid] / divf;
+#if PF_SEM_CPU_TU
+            // rust/src/ce.rs:96-110: one running sum over all cells.
+            for (uint32_t i = 0; i < nM; i++) {
+                const float p_ij = (float)hist[(j * nM + i) * BLOCK + tid] / divf;
+                if (p_ij != 0.0f) ce += p_ij * logf(p_j / p_ij);
+            }
+#else
+            // periodfind/cuda/ce.cu:231-243: per-phase-row contribution,
+            // then the rows are summed (here in row order).
+            float ce_contrib = 0.0f;
+            for (uint32_t i = 0; i < nM; i++) {
+                const float p_ij = (float)hist[(j * nM + i) * BLOCK + tid] / divf;
+                if (p_ij != 0) ce_contrib += p_ij * logf(p_j / p_ij);
+            }
+            ce += ce_contrib;
+#endif
+        }
+        p.out[out_idx] = ce;
+    } else if constexpr (ALGO == ALGO_AOV) {
+        if constexpr (ACC == AOVACC_FIX) {
+            unsigned long long* hist64 = v.hist64;
+            if constexpr (!OVL) hist64[tid] += hist64[nP * BLOCK + tid];
+            const unsigned long long mask = (1ull << kFixCountShift) - 1ull;
+            const double xbar = cd.fix_sumx / (double)n;
+            double s1 = 0.0, sbx = 0.0;
+            for (uint32_t b = 0; b < nP; b++) {
+                const unsigned long long h = hist64[b * BLOCK + tid];
+                const unsigned long long c = h >> kFixCountShift;
+                if (c != 0ull) {
+                    const double nb = (double)c;
+                    const double X = (double)(h & mask);
+                    const double mu = X / nb;
+                    const double r = mu - xbar;
+                    s1 = __fma_rn(nb * r, r, s1);
+                    sbx = __fma_rn(X, mu, sbx);
+                }
+            }
+            const double s2 = __dadd_rn((double)po * cd.fix_sumx2, -sbx);
+            const double scale = ((double)n - (double)nP) / ((double)nP - 1.0);
+            float res;
+#if PF_SEM_CPU_TU
+            res = (s2 <= 0.0) ? 0.0f : (float)(scale * (s1 / s2));  // aov.rs:197-201
+#else
+            res = (float)(scale * (s1 / (s2 <= 0.0 ? 0.0 : s2)));      // aov.cu:242-244
+#endif
+            p.out[out_idx] = res;
+        } else {
+            // periodfind/cuda/aov.cu:225-244 / rust/src/aov.rs:184-201.
+            const float avg = cd.avg;
+            float s1 = 0;
+            float s2 = 0;
+            for (uint32_t b = 0; b < nP; b++) {
+                float nn = static_cast<float>(v.a_cnt[b * BLOCK + tid]);
+                float sum = v.a_sum[b * BLOCK + tid];
+                float sq_sum = v.a_sq[b * BLOCK + tid];
+                if (nn != 0) {
+                    float aux = sum / nn;
+                    float residual = aux - avg;
+                    s1 += nn * residual * residual;
+                    s2 += sq_sum - nn * aux * aux;
+                }
+            }
+            const float length = (float)n;
+#if PF_SEM_CPU_TU
+            p.out[out_idx] = (s2 == 0.0f)
+                                 ? 0.0f
+                                 : ((length - (float)nP) / ((float)nP - 1.0f)) * (s1 / s2);
+#else
+            p.out[out_idx] = (static_cast<float>(length - nP) / static_cast<float>(nP - 1)) *
+                             (s1 / s2);
+#endif
+        }
+    } else {
+        // periodfind/cuda/ls.cu:144-165 / rust/src/ls.rs:253-280.
+        const float mag_cos = ls.mag_cos, mag_sin = ls.mag_sin;
+        const float cos_cos = ls.cos_cos, cos_sin = ls.cos_sin;
+        float sin_sin = static_cast<float>(n) - cos_cos;
+        float cos_tau, sin_tau;
+        sincosf(0.5f * atan2f(2.0f * cos_sin, cos_cos - sin_sin), &sin_tau, &cos_tau);
+        float numerator_l = cos_tau * mag_cos + sin_tau * mag_sin;
+        numerator_l *= numerator_l;
+        float numerator_r = cos_tau * mag_sin - sin_tau * mag_cos;
+        numerator_r *= numerator_r;
+        float denominator_l = cos_tau * cos_tau * cos_cos + 2 * cos_tau * sin_tau * cos_sin +
+                              sin_tau * sin_tau * sin_sin;
+        float denominator_r = cos_tau * cos_tau * sin_sin - 2 * cos_tau * sin_tau * cos_sin +
+                              sin_tau * sin_tau * cos_cos;
+#if PF_SEM_CPU_TU
+        p.out[out_idx] = (denominator_l == 0.0f || denominator_r == 0.0f)
+                             ? 0.0f
+                             : 0.5f * (numerator_l / denominator_l + numerator_r / denominator_r);
+#else
+        p.out[out_idx] = 0.5f * ((numerator_l / denominator_l) + (numerator_r / denominator_r));
+#endif
+    }
+}
+
+// ------------------------------------------------------------- preparation
+
+// CE magnitude bins, once per point (the reference recomputes
+// MagBin(mags[idx]) for every (point, period), ce.cu:146).  Stored as
+// (mag_bin % n_mag) | (saturated << 31); a saturated bin is 2^64-1, whose
+// wrapped successors are 0, 1, ... (size_t arithmetic, ce.cu:150-152).
+__global__ void ce_magbin_kernel(const float* __restrict__ m, uint32_t* __restrict__ aux,
+                                 const CurveDesc* __restrict__ curves, uint32_t n_curves,
+                                 uint32_t n_mag, float mag_bin_size, int flag_saturated) {
+    const uint32_t c = blockIdx.x;
+    if (c >= n_curves) return;
+    const CurveDesc cd = curves[c];
+    const uint32_t n4 = (cd.n + 3u) & ~3u;
+    for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) {
+        uint32_t v = 0;
+        if (i < cd.n) {
+            const float mag_val = m[cd.off + i];
+            const unsigned long long mb = static_cast<unsigned long long>(mag_val / mag_bin_size);
+            v = (uint32_t)(mb % n_mag);
+            if (flag_saturated && mb == ~0ull) v |= 0x80000000u;
+        }
+        aux[cd.off + i] = v;
+    }
+}
+
+}  // namespace PF_KNS
+}  // namespace pfk

@@ -1,0 +1,50 @@
+// pf_launch.h -- host-side entry points into the kernel translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "pf_types.h"
+
+namespace pfk {
+
+struct FoldConfig {
+    int algo;   // ALGO_*
+    int fold;   // FOLD_*
+    int acc;    // AOVACC_* (AOV only)
+    int block;  // threads per CTA: 64, 128 or 256
+    bool ovl;   // general bin-overlap path
+};
+
+size_t fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag);
+
+// Semantics of the reference's CUDA build (-use_fast_math).
+cudaError_t launch_fold_cudasem(const FoldConfig& c, const FoldParams& p, uint32_t n_work,
+                                cudaStream_t stream);
+cudaError_t launch_magbin_cudasem(const float* m, uint32_t* aux, const CurveDesc* curves,
+                                  uint32_t n_curves, uint32_t n_mag, float mag_bin_size,
+                                  int flag_saturated, cudaStream_t stream);
+// Semantics of the reference's CPU path (IEEE, no contraction).
+cudaError_t launch_fold_cpusem(const FoldConfig& c, const FoldParams& p, uint32_t n_work,
+                               cudaStream_t stream);
+cudaError_t launch_magbin_cpusem(const float* m, uint32_t* aux, const CurveDesc* curves,
+                                 uint32_t n_curves, uint32_t n_mag, float mag_bin_size,
+                                 int flag_saturated, cudaStream_t stream);
+
+// Preparation kernels (pf_prep.cu).
+cudaError_t launch_aov_mean(const float* m, CurveDesc* curves, uint32_t n_curves,
+                            cudaStream_t stream);
+cudaError_t launch_aov_fix_prep(const float* m, uint64_t* aux64, CurveDesc* curves,
+                                uint32_t n_curves, uint32_t overlap, cudaStream_t stream);
+
+cudaError_t launch_pack(const float* src_t, const float* src_m, const int64_t* src_off,
+                        const CurveDesc* curves, uint32_t n_curves, float* dst_t, float* dst_m,
+                        cudaStream_t stream);
+
+// Peak search (pf_peaks.cu): one CTA per curve over a [n_curves][flat]
+// periodogram; rust/src/peaks.rs semantics.
+cudaError_t launch_peaks(const float* pg, uint64_t n_curves, uint64_t flat_len,
+                         uint32_t n_peaks, uint32_t min_distance, int use_max,
+                         int64_t* out_idx, float* out_val, cudaStream_t stream);
+
+}  // namespace pfk

@@ -1,0 +1,196 @@
+// pf_peaks.cu -- top-N peak search over periodograms on the device.
+//
+// Semantics of rust/src/peaks.rs:18-238 (find_top_peaks on one chunk): the
+// interior samples 1 .. n-2 of the flattened [period][pdt] grid are fed in
+// order; a strict local extremum that beats the current threshold (the
+// worst of the top-N once it is full) becomes the candidate unless a better
+// candidate is pending; the candidate is promoted into the best-first list
+// once min_distance samples have been fed since it was set, and at the end.
+//
+// Only extrema change the state; every other sample just advances the
+// distance counter.  A CTA per curve therefore (1) flags extrema in chunks,
+// (2) compacts them in index order with a block scan, and (3) one thread
+// replays the state machine over the compacted extrema, reconstructing the
+// distance counter from index gaps:
+//   - a candidate set at index c is promoted while feeding index
+//     c + min_distance - 1 (after that index's own peak test), or at the
+//     end if no such index is fed;
+//   - a better extremum fed before that replaces it.
+// The sorted top-N list lives in the caller's output rows.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "pf_launch.h"
+
+namespace pfk {
+
+namespace {
+
+constexpr int kPeakThreads = 256;
+constexpr int kPerThread = 8;
+constexpr uint32_t kChunk = kPeakThreads * kPerThread;
+
+struct PeakState {
+    int64_t* idx;
+    float* val;
+    uint32_t count, n_peaks;
+    bool use_max;
+    bool has_cand;
+    int64_t cand_idx;
+    float cand_val;
+};
+
+__device__ __forceinline__ bool better(bool use_max, float a, float b) {
+    return use_max ? (a > b) : (a < b);
+}
+
+__device__ __forceinline__ float threshold(const PeakState& s) {
+    if (s.count < s.n_peaks) return s.use_max ? -INFINITY : INFINITY;
+    return s.val[s.count - 1];
+}
+
+// peaks.rs:104-130: append (or replace the worst) and bubble toward the front.
+__device__ void insert(PeakState& s, int64_t idx, float v) {
+    uint32_t i;
+    if (s.count < s.n_peaks) {
+        i = s.count++;
+    } else if (better(s.use_max, v, s.val[s.count - 1])) {
+        i = s.count - 1;
+    } else {
+        return;
+    }
+    s.idx[i] = idx;
+    s.val[i] = v;
+    while (i > 0 && better(s.use_max, s.val[i], s.val[i - 1])) {
+        const float tv = s.val[i];
+        s.val[i] = s.val[i - 1];
+        s.val[i - 1] = tv;
+        const int64_t ti = s.idx[i];
+        s.idx[i] = s.idx[i - 1];
+        s.idx[i - 1] = ti;
+        i--;
+    }
+}
+
+// peaks.rs:134-140.
+__device__ __forceinline__ void promote(PeakState& s) {
+    if (s.has_cand && better(s.use_max, s.cand_val, threshold(s))) insert(s, s.cand_idx, s.cand_val);
+    s.has_cand = false;
+}
+
+__global__ void __launch_bounds__(kPeakThreads)
+    peaks_kernel(const float* __restrict__ pg, uint64_t flat_len, uint32_t n_peaks,
+                 uint32_t min_distance, int use_max_i, int64_t* __restrict__ out_idx,
+                 float* __restrict__ out_val) {
+    __shared__ int64_t ext_idx[kChunk];
+    __shared__ float ext_val[kChunk];
+    __shared__ uint32_t warp_tot[kPeakThreads / 32];
+    __shared__ uint32_t chunk_count;
+
+    const uint64_t c = blockIdx.x;
+    const float* d = pg + c * flat_len;
+    const bool use_max = use_max_i != 0;
+    int64_t* row_idx = out_idx + c * n_peaks;
+    float* row_val = out_val + c * n_peaks;
+
+    PeakState s;
+    s.idx = row_idx;
+    s.val = row_val;
+    s.count = 0;
+    s.n_peaks = n_peaks;
+    s.use_max = use_max;
+    s.has_cand = false;
+    s.cand_idx = -1;
+    s.cand_val = use_max ? -INFINITY : INFINITY;
+    const uint64_t md = min_distance;
+
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    // Interior samples 1 .. flat_len-2.
+    const uint64_t first = 1, last = (flat_len >= 2) ? flat_len - 2 : 0;
+    for (uint64_t base = first; flat_len >= 3 && base <= last; base += kChunk) {
+        // (1) flag this thread's kPerThread consecutive samples.
+        uint32_t flags = 0;
+        const uint64_t i0 = base + (uint64_t)tid * kPerThread;
+#pragma unroll
+        for (int k = 0; k < kPerThread; k++) {
+            const uint64_t i = i0 + k;
+            if (i <= last) {
+                const float l = d[i - 1], v = d[i], r = d[i + 1];
+                const bool pk = use_max ? (v > l && v > r) : (v < l && v < r);
+                flags |= (pk ? 1u : 0u) << k;
+            }
+        }
+        // (2) order-preserving compaction: exclusive scan of popcounts.
+        const uint32_t mine = __popc(flags);
+        uint32_t incl = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warp_tot[wid] = incl;
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t run = 0;
+            for (int w = 0; w < kPeakThreads / 32; w++) {
+                const uint32_t t = warp_tot[w];
+                warp_tot[w] = run;
+                run += t;
+            }
+            chunk_count = run;
+        }
+        __syncthreads();
+        uint32_t pos = warp_tot[wid] + incl - mine;
+#pragma unroll
+        for (int k = 0; k < kPerThread; k++) {
+            if (flags & (1u << k)) {
+                ext_idx[pos] = (int64_t)(i0 + k);
+                ext_val[pos] = d[i0 + k];
+                pos++;
+            }
+        }
+        __syncthreads();
+        // (3) replay.
+        if (tid == 0) {
+            const uint32_t ne = chunk_count;
+            for (uint32_t e = 0; e < ne; e++) {
+                const int64_t i = ext_idx[e];
+                const float v = ext_val[e];
+                // Promotion that happened strictly before index i.
+                if (s.has_cand && (uint64_t)s.cand_idx + (md > 0 ? md - 1 : 0) < (uint64_t)i)
+                    promote(s);
+                // feed(i): peak test against the current threshold.
+                if (better(use_max, v, threshold(s)) &&
+                    (!s.has_cand || better(use_max, v, s.cand_val))) {
+                    s.cand_idx = i;
+                    s.cand_val = v;
+                    s.has_cand = true;
+                }
+                // Distance after feeding i: i - cand_idx + 1.
+                if (s.has_cand && (uint64_t)(i - s.cand_idx) + 1 >= md) promote(s);
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        promote(s);  // finalize (peaks.rs:207-209)
+        for (uint32_t k = s.count; k < n_peaks; k++) {
+            row_idx[k] = -1;
+            row_val[k] = 0.0f;
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_peaks(const float* pg, uint64_t n_curves, uint64_t flat_len,
+                         uint32_t n_peaks, uint32_t min_distance, int use_max,
+                         int64_t* out_idx, float* out_val, cudaStream_t stream) {
+    if (n_curves == 0 || n_peaks == 0) return cudaSuccess;
+    peaks_kernel<<<(unsigned)n_curves, kPeakThreads, 0, stream>>>(
+        pg, flat_len, n_peaks, min_distance, use_max, out_idx, out_val);
+    return cudaGetLastError();
+}
+
+}  // namespace pfk

@@ -1,0 +1,249 @@
+"""GPU periodogram classes: drop-ins for periodfind.gpu.{ConditionalEntropy,
+AOV, LombScargle} (periodfind/ce.pyx:41-209, aov.pyx:38-192, ls.pyx:37-176).
+
+Constructor arguments and `calc()` keep the reference's names, defaults and
+errors.  `calc()` takes the superset signature of the reference's CPU
+classes (periodfind/cpu/__init__.py:73-397): `output` may also be 'peaks'
+(with `n_peaks`, `min_distance`), and `errs` is accepted and ignored, as
+CE, AOV and LS do not use uncertainties.
+
+Two keyword-only additions select the implementation:
+  mode       'chosen' (default) or 'plain' (the reference's fold, op for op)
+  semantics  'cuda' (default: the reference CUDA build's arithmetic) or
+             'cpu' (the reference CPU path's IEEE arithmetic)
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native as nat
+from ._utils import ensure_float32, prepare_magnitudes, validate_inputs
+from .stats import Periodogram, Statistics
+
+N_PEAKS_DEFAULT = 32
+MIN_DISTANCE_DEFAULT = 1
+_OUTPUTS = ("stats", "periodogram", "peaks")
+
+
+def _mode_flags(mode: str, semantics: str, fold: str | None = None) -> int:
+    if mode not in ("chosen", "plain"):
+        raise ValueError(f"mode must be 'chosen' or 'plain', got {mode!r}")
+    if semantics not in ("cuda", "cpu"):
+        raise ValueError(f"semantics must be 'cuda' or 'cpu', got {semantics!r}")
+    f = nat.PF_MODE_CHOSEN if mode == "chosen" else nat.PF_MODE_PLAIN
+    if semantics == "cpu":
+        f |= nat.PF_SEM_CPU
+    if fold == "df":
+        f |= nat.PF_FOLD_DF
+    elif fold == "f32":
+        f |= nat.PF_FOLD_F32
+    elif fold not in (None, "exact", "ref"):
+        raise ValueError(f"unknown fold {fold!r}")
+    return f
+
+
+def _grid(a, name):
+    # The reference types these as 1-D float32 ndarrays (ce.pyx:89-90).
+    if not isinstance(a, np.ndarray):
+        raise TypeError(f"Argument '{name}' has incorrect type (expected numpy.ndarray, "
+                        f"got {type(a).__name__})")
+    if a.ndim != 1:
+        raise ValueError(f"Buffer has wrong number of dimensions (expected 1, got {a.ndim})")
+    if a.dtype != np.float32:
+        raise ValueError(f"Buffer dtype mismatch, expected 'float32_t' but got '{a.dtype}'")
+    return np.ascontiguousarray(a)
+
+
+def unravel_peaks(peak_indices, peak_values, periods, period_dts, n_peaks):
+    """Flat peak indices -> list (per curve) of lists of Statistics, stopping
+    at the first -1 (periodfind/cpu/__init__.py:46-70)."""
+    n_pdts = len(period_dts)
+    results = []
+    for ci in range(peak_indices.shape[0]):
+        curve = []
+        for pi in range(n_peaks):
+            k = peak_indices[ci, pi]
+            if k < 0:
+                break
+            curve.append(Statistics(
+                params=[float(periods[int(k // n_pdts)]), float(period_dts[int(k % n_pdts)])],
+                value=float(peak_values[ci, pi]), mean=0.0, std=1.0, median=0.0, mad=1.0))
+        results.append(curve)
+    return results
+
+
+class _Periodogram:
+    _use_max = True
+    _normalize_default = False
+    _center_default = False
+
+    def __init__(self, *, mode="chosen", semantics="cuda", device=0):
+        self.mode = mode
+        self.semantics = semantics
+        self.device = device
+        self._flags = _mode_flags(mode, semantics, getattr(self, "_fold", None))
+
+    # -- native calls, implemented per algorithm
+    def _native_pgram(self, ctx, b, periods, pdts, out):
+        raise NotImplementedError
+
+    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
+        raise NotImplementedError
+
+    def periodograms(self, times, mags, periods, period_dts):
+        """Raw [n_curves, n_periods, n_pdts] float32 array for prepared mags."""
+        ctx = nat.default_context(self.device)
+        b = nat.CurveBatch(times, mags)
+        out = np.empty((b.n, len(periods), len(period_dts)), dtype=np.float32)
+        with ctx.lock:
+            ctx.check(self._native_pgram(ctx, b, periods, period_dts, out))
+        return out
+
+    def peaks(self, times, mags, periods, period_dts, n_peaks=N_PEAKS_DEFAULT,
+              min_distance=MIN_DISTANCE_DEFAULT):
+        """(indices int64 [n_curves, n_peaks] with -1 padding, values float32)."""
+        ctx = nat.default_context(self.device)
+        b = nat.CurveBatch(times, mags)
+        n_peaks = int(n_peaks)
+        if n_peaks < 0:
+            raise ValueError("n_peaks must be >= 0")
+        idx = np.full((b.n, n_peaks), -1, dtype=np.int64)
+        val = np.zeros((b.n, n_peaks), dtype=np.float32)
+        with ctx.lock:
+            ctx.check(self._native_peaks(ctx, b, periods, period_dts, n_peaks,
+                                         int(min_distance), idx, val))
+        return idx, val
+
+    def calc(self, times, mags, periods, period_dts, output="stats", normalize=None,
+             center=None, n_stats=1, significance_type="stdmean", n_peaks=N_PEAKS_DEFAULT,
+             min_distance=MIN_DISTANCE_DEFAULT, errs=None):
+        """Compute the periodogram of every light curve.
+
+        Returns a list of Statistics (output='stats'; lists of them when
+        n_stats > 1), a list of Periodogram (output='periodogram'), or a list
+        of lists of Statistics for the top peaks (output='peaks').
+        """
+        if normalize is None:
+            normalize = self._normalize_default
+        if center is None:
+            center = self._center_default
+        if output not in _OUTPUTS:
+            raise NotImplementedError(
+                f'Output type "{output}" is not implemented. '
+                f'Use "stats", "periodogram", or "peaks".')
+        validate_inputs(times, mags)
+        ensure_float32(times, "times")
+        ensure_float32(mags, "mags")
+        periods = _grid(periods, "periods")
+        period_dts = _grid(period_dts, "period_dts")
+        mags_use = prepare_magnitudes(mags, center, normalize)
+
+        if output == "peaks":
+            idx, val = self.peaks(times, mags_use, periods, period_dts, n_peaks, min_distance)
+            return unravel_peaks(idx, val, periods, period_dts, int(n_peaks))
+
+        data = self.periodograms(times, mags_use, periods, period_dts)
+        if output == "stats":
+            return [Statistics.statistics_from_data(
+                data[i], [periods, period_dts], self._use_max, n=n_stats,
+                significance_type=significance_type) for i in range(len(times))]
+        return [Periodogram(d, [periods, period_dts], self._use_max) for d in data]
+
+
+class ConditionalEntropy(_Periodogram):
+    """Conditional Entropy periodogram (minimum is best).
+
+    n_phase x n_mag histogram of (folded phase, normalised magnitude);
+    phase_bin_extent / mag_bin_extent widen each entry over neighbouring
+    bins with wrap-around (periodfind/ce.pyx:41-80).
+    """
+
+    _use_max = False
+    _normalize_default = True
+
+    def __init__(self, n_phase=10, n_mag=10, phase_bin_extent=1, mag_bin_extent=1, *,
+                 mode="chosen", semantics="cuda", device=0):
+        super().__init__(mode=mode, semantics=semantics, device=device)
+        self.n_phase = int(n_phase)
+        self.n_mag = int(n_mag)
+        self.phase_bin_extent = int(phase_bin_extent)
+        self.mag_bin_extent = int(mag_bin_extent)
+
+    def _native_pgram(self, ctx, b, periods, pdts, out):
+        return ctx.lib.pf_ce(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
+                             nat.ptr(pdts), len(pdts), self.n_phase, self.n_mag,
+                             self.phase_bin_extent, self.mag_bin_extent, self._flags,
+                             nat.ptr(out))
+
+    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
+        return ctx.lib.pf_ce_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
+                                   nat.ptr(pdts), len(pdts), self.n_phase, self.n_mag,
+                                   self.phase_bin_extent, self.mag_bin_extent, n_peaks,
+                                   min_distance, self._flags, nat.ptr(idx), nat.ptr(val))
+
+
+class AOV(_Periodogram):
+    """Analysis-of-Variance periodogram (maximum is best)
+    (periodfind/aov.pyx:38-67)."""
+
+    _use_max = True
+
+    def __init__(self, n_phase=10, phase_bin_extent=1, *, mode="chosen", semantics="cuda",
+                 device=0):
+        super().__init__(mode=mode, semantics=semantics, device=device)
+        self.n_phase = int(n_phase)
+        self.phase_bin_extent = int(phase_bin_extent)
+
+    def _native_pgram(self, ctx, b, periods, pdts, out):
+        return ctx.lib.pf_aov(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
+                              nat.ptr(pdts), len(pdts), self.n_phase, self.phase_bin_extent,
+                              self._flags, nat.ptr(out))
+
+    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
+        return ctx.lib.pf_aov_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
+                                    nat.ptr(pdts), len(pdts), self.n_phase,
+                                    self.phase_bin_extent, n_peaks, min_distance, self._flags,
+                                    nat.ptr(idx), nat.ptr(val))
+
+
+class LombScargle(_Periodogram):
+    """Lomb-Scargle periodogram (maximum is best; magnitudes centred by
+    default) (periodfind/ls.pyx:37-62).
+
+    fold='df' selects the split-precision FP32 phase (period_dt == 0 only);
+    fold='f32' the all-FP32 fold (precision studies).
+    """
+
+    _use_max = True
+    _center_default = True
+
+    def __init__(self, *, mode="chosen", semantics="cuda", device=0, fold=None):
+        self._fold = fold
+        super().__init__(mode=mode, semantics=semantics, device=device)
+
+    def _native_pgram(self, ctx, b, periods, pdts, out):
+        return ctx.lib.pf_ls(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
+                             nat.ptr(pdts), len(pdts), self._flags, nat.ptr(out))
+
+    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
+        return ctx.lib.pf_ls_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
+                                   nat.ptr(pdts), len(pdts), n_peaks, min_distance,
+                                   self._flags, nat.ptr(idx), nat.ptr(val))
+
+
+def find_top_peaks_batched(data, n_peaks, min_distance, use_max, device=0):
+    """Top peaks of precomputed periodograms [n_curves, n_periods, n_pdts]
+    (rust/src/lib.rs:508-548), computed on the GPU."""
+    d = np.ascontiguousarray(data, dtype=np.float32)
+    if d.ndim != 3:
+        raise ValueError("data must have shape (n_curves, n_periods, n_pdts)")
+    ctx = nat.default_context(device)
+    n_peaks = int(n_peaks)
+    idx = np.full((d.shape[0], n_peaks), -1, dtype=np.int64)
+    val = np.zeros((d.shape[0], n_peaks), dtype=np.float32)
+    with ctx.lock:
+        ctx.check(ctx.lib.pf_find_peaks(ctx.handle, nat.ptr(d), d.shape[0],
+                                        d.shape[1] * d.shape[2], n_peaks, int(min_distance),
+                                        int(bool(use_max)), nat.ptr(idx), nat.ptr(val)))
+    return idx, val

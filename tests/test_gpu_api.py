@@ -1,0 +1,149 @@
+"""The reference's GPU integration expectations (tests/test_periodfind.py:
+452-850, 957-1305; tests/test_cpu_standalone.py:992-1155 for 'peaks'),
+exercised on the drop-in classes."""
+
+import warnings
+
+import numpy as np
+import pytest
+
+from periodfind_b200 import Periodogram, Statistics
+from tests import lightcurves as lc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from periodfind_b200 import gpu as g
+
+    return g
+
+
+ZERO = np.array([0.0], np.float32)
+
+
+def _detect(obj, true_p, **kw):
+    t, m = lc.sine_curve(true_p, n=800, noise=0.02, t_span=200.0)
+    res = obj.calc([t], [m], lc.trial_periods(true_p, n=500), ZERO, output="stats", **kw)
+    return res[0].params[0]
+
+
+@pytest.mark.parametrize("mode", ["chosen", "plain"])
+def test_known_period_all_algorithms(gpu, mode):
+    for obj in (gpu.ConditionalEntropy(15, 10, mode=mode), gpu.AOV(15, mode=mode),
+                gpu.LombScargle(mode=mode)):
+        got = _detect(obj, 5.0)
+        assert abs(got - 5.0) / 5.0 < 0.05, (type(obj).__name__, got)
+
+
+def test_stats_output_types(gpu):
+    t, m = lc.sine_curve(2.5)
+    res = gpu.ConditionalEntropy().calc([t], [m], lc.trial_periods(2.5), ZERO)
+    assert isinstance(res, list) and len(res) == 1 and isinstance(res[0], Statistics)
+    assert res[0].significance > 0
+    multi = gpu.ConditionalEntropy().calc([t], [m], np.linspace(1, 10, 200, dtype=np.float32),
+                                          ZERO, n_stats=5)
+    assert isinstance(multi[0], list) and len(multi[0]) == 5
+
+
+def test_periodogram_shapes_and_use_max(gpu):
+    t, m = lc.sine_curve(3.0)
+    P = np.linspace(1, 10, 100, dtype=np.float32)
+    D2 = np.array([0.0, 0.001], np.float32)
+    pg = gpu.ConditionalEntropy().calc([t], [m], P, D2, output="periodogram")[0]
+    assert isinstance(pg, Periodogram) and pg.data.shape == (100, 2) and pg.use_max is False
+    assert gpu.AOV().calc([t], [m], P, ZERO, output="periodogram")[0].use_max is True
+    assert gpu.LombScargle().calc([t], [m], P, ZERO, output="periodogram")[0].use_max is True
+    D5 = np.linspace(-0.01, 0.01, 5, dtype=np.float32)
+    assert gpu.ConditionalEntropy().calc([t], [m], P[:50], D5,
+                                         output="periodogram")[0].data.shape == (50, 5)
+
+
+def test_short_lightcurve_all_algorithms(gpu):
+    t = np.array([0, 1, 2, 3, 4], np.float32)
+    m = np.array([1.0, 0.5, 1.0, 0.5, 1.0], np.float32)
+    P = np.linspace(1, 5, 20, dtype=np.float32)
+    for cls in (gpu.ConditionalEntropy, gpu.AOV, gpu.LombScargle):
+        assert isinstance(cls().calc([t], [m], P, ZERO)[0], Statistics)
+
+
+def test_center_normalize_warning(gpu):
+    t, m = lc.sine_curve(3.0)
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        gpu.ConditionalEntropy().calc([t], [m], np.linspace(1, 10, 50, dtype=np.float32), ZERO,
+                                      normalize=True, center=True)
+    assert any(issubclass(x.category, RuntimeWarning) for x in w)
+
+
+def test_significance_types(gpu):
+    t, m = lc.sine_curve(3.0, n=300)
+    for st in ("stdmean", "madmedian"):
+        r = gpu.AOV().calc([t], [m], np.linspace(1, 10, 100, dtype=np.float32), ZERO,
+                           significance_type=st)
+        assert r[0].significance_type == st and r[0].significance > 0
+
+
+def test_aov_overlap_smoother(gpu):
+    t, m = lc.sine_curve(3.0, n=800, noise=0.03, t_span=200.0)
+    P = lc.trial_periods(3.0, n=300)
+    a = gpu.AOV(10, 1).calc([t], [m], P, ZERO, output="periodogram")[0].data.ravel()
+    b = gpu.AOV(10, 3).calc([t], [m], P, ZERO, output="periodogram")[0].data.ravel()
+    assert not np.allclose(a, b, atol=1e-6)
+    assert np.std(np.diff(b)) < np.std(np.diff(a))
+    assert abs(_detect(gpu.AOV(15, 3), 4.0) - 4.0) / 4.0 < 0.05
+
+
+def test_batched_and_large_grid(gpu):
+    curves = [lc.sine_curve(p, seed=i) for i, p in enumerate([2.0, 4.0, 6.0])]
+    ts = [c[0] for c in curves]
+    ms = [c[1] for c in curves]
+    P = np.linspace(1, 10, 5000, dtype=np.float32)
+    res = gpu.LombScargle().calc(ts, ms, P, ZERO)
+    assert len(res) == 3
+    for true_p, r in zip([2.0, 4.0, 6.0], res):
+        got = r.params[0]
+        assert any(abs(got - c) / c < 0.05 for c in (true_p, true_p / 2, 2 * true_p))
+
+
+def test_stats_best_matches_periodogram_best(gpu):
+    t, m = lc.sine_curve(3.0, n=500, noise=0.02)
+    P = lc.trial_periods(3.0, n=300)
+    s = gpu.AOV(10).calc([t], [m], P, ZERO, output="stats")[0]
+    pg = gpu.AOV(10).calc([t], [m], P, ZERO, output="periodogram")[0]
+    assert s.params[0] == pytest.approx(pg.best_params(n=1).params[0])
+
+
+def test_peaks_output_contract(gpu):
+    t, m = lc.sine_curve(5.0, n=800, noise=0.02, t_span=200.0)
+    P = lc.trial_periods(5.0, n=500)
+    for obj, use_max in ((gpu.ConditionalEntropy(15, 10), False), (gpu.AOV(15), True),
+                         (gpu.LombScargle(), True)):
+        stats = obj.calc([t], [m], P, ZERO, output="stats")
+        peaks = obj.calc([t], [m], P, ZERO, output="peaks", n_peaks=32, min_distance=1)
+        assert isinstance(peaks, list) and isinstance(peaks[0], list)
+        assert 0 < len(peaks[0]) <= 32 and isinstance(peaks[0][0], Statistics)
+        assert stats[0].params[0] == pytest.approx(peaks[0][0].params[0])
+        vals = [p.value for p in peaks[0]]
+        assert all((a >= b) if use_max else (a <= b) for a, b in zip(vals, vals[1:]))
+    D2 = np.array([0.0, 0.001], np.float32)
+    pk = gpu.AOV().calc([t], [m], P[:100], D2, output="peaks", n_peaks=16)
+    assert len(pk[0][0].params) == 2
+    close = gpu.AOV().calc([t], [m], P, ZERO, output="peaks", min_distance=1)
+    far = gpu.AOV().calc([t], [m], P, ZERO, output="peaks", min_distance=20)
+    assert len(far[0]) <= len(close[0])
+
+
+def test_lsst_like_cadence(gpu):
+    rng = np.random.default_rng(3)
+    t = lc.seasonal_times(rng, 600, 3000.0)
+    for shape, true_p in (("sine", 0.73), ("eclipse", 2.31)):
+        y = lc.sinusoid(t, true_p) if shape == "sine" else lc.v_eclipse(t, true_p)
+        m = lc.noisy(rng, y, 0.03)
+        P = lc.trial_periods(true_p, n=4000, margin=0.3)
+        for obj in (gpu.ConditionalEntropy(), gpu.AOV(15), gpu.LombScargle()):
+            if shape == "eclipse" and isinstance(obj, gpu.LombScargle):
+                continue
+            got = obj.calc([t], [m], P, ZERO)[0].params[0]
+            assert any(abs(got - c) / c < 0.01 for c in (true_p, true_p / 2, 2 * true_p)), got

@@ -1,0 +1,308 @@
+"""GPU parity tests: the CUDA path (through the C ABI) against the oracle
+(the reference's CPU arithmetic), against the reference's own CUDA build
+(when oracle/_ref is present), and between the plain and chosen forms.
+
+Tolerances, written per comparison:
+  * CPU semantics vs the oracle
+      AOV plain: bit-exact (same bins, same f32 adds in the same order).
+      CE: rtol 2e-6 (bins are identical; logf on the GPU and in glibc may
+          differ by an ulp).
+      LS: |diff| <= 2e-5 * max|P| + 2e-5 * |P| (sinf/cosf ulp differences
+          accumulated over the curve).
+  * chosen vs plain (same semantics): CE and LS bit-exact (the exact fold
+    is the reference fold's quotient without a divide); AOV chosen uses the
+    exact fixed-point accumulator and must match the FP64 statistic on the
+    same bins to rtol 1e-6.
+  * CUDA semantics vs the reference CUDA build: CE rtol 1e-5 (the reference
+    sums rows in atomic order), AOV rtol 2e-4 and LS rtol 1e-4 with an
+    absolute floor (the reference's f32 sums are order-dependent).
+"""
+
+import numpy as np
+import pytest
+
+from tests import lightcurves as lc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from periodfind_b200 import gpu as g
+
+    return g
+
+
+def _grid(n_per=300, pdts=(0.0,), lo=0.5, hi=10.0):
+    return (np.linspace(lo, hi, n_per, dtype=np.float32), np.array(pdts, np.float32))
+
+
+def _ragged(seed=7, lengths=(1, 2, 5, 31, 32, 33, 255, 256, 257, 1023, 1024, 1025, 2049)):
+    rng = np.random.default_rng(seed)
+    ts, ms = [], []
+    for n in lengths:
+        t = lc.uniform_times(rng, n, 400.0)
+        p = float(rng.uniform(0.5, 10))
+        ms.append(lc.noisy(rng, lc.sinusoid(t, p, amp=0.3, offset=15.0), 0.05))
+        ts.append(t)
+    return ts, ms
+
+
+def _ls_close(a, b, rel=2e-5):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = np.nanmax(np.abs(b)) if b.size else 1.0
+    assert np.all(np.abs(a - b) <= rel * scale + rel * np.abs(b)), np.nanmax(np.abs(a - b))
+
+
+# ------------------------------------------------- CPU semantics vs oracle
+
+
+@pytest.mark.parametrize("mode", ["plain", "chosen"])
+def test_ce_cpu_semantics_vs_oracle(gpu, oracle, mode):
+    ts, ms = _ragged()
+    ms = [lc.normalize(m) if len(m) > 1 else np.full(1, 0.5, np.float32) for m in ms]
+    P, D = _grid(pdts=(0.0, 1e-4, -3e-4))
+    got = gpu.ConditionalEntropy(10, 10, mode=mode, semantics="cpu").periodograms(ts, ms, P, D)
+    want = oracle.ce(ts, ms, P, D, 10, 10)
+    np.testing.assert_allclose(got, want, rtol=2e-6, atol=0)
+
+
+def test_aov_plain_cpu_semantics_bit_exact(gpu, oracle):
+    ts, ms = _ragged()
+    P, D = _grid(pdts=(0.0, 1e-4))
+    got = gpu.AOV(15, mode="plain", semantics="cpu").periodograms(ts, ms, P, D)
+    want = oracle.aov(ts, ms, P, D, 15)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_aov_chosen_matches_fp64_statistic(gpu, oracle):
+    ts, ms = _ragged()
+    keep = [i for i, t in enumerate(ts) if len(t) >= 16]
+    ts = [ts[i] for i in keep]
+    ms = [ms[i] for i in keep]
+    P, D = _grid(pdts=(0.0, 1e-4))
+    got = gpu.AOV(15, mode="chosen", semantics="cpu").periodograms(ts, ms, P, D)
+    want = oracle.aov_f64(ts, ms, P, D, 15)
+    np.testing.assert_allclose(got, want, rtol=1e-6, atol=1e-6 * np.max(np.abs(want)))
+
+
+@pytest.mark.parametrize("mode", ["plain", "chosen"])
+def test_ls_cpu_semantics_vs_oracle(gpu, oracle, mode):
+    ts, ms = _ragged()
+    ms = [lc.center(m) for m in ms]
+    P, D = _grid(pdts=(0.0, 1e-4))
+    got = gpu.LombScargle(mode=mode, semantics="cpu").periodograms(ts, ms, P, D)
+    want = oracle.ls(ts, ms, P, D)
+    _ls_close(got, want)
+
+
+@pytest.mark.parametrize("po,mo", [(3, 1), (1, 2), (2, 3)])
+def test_ce_overlap_vs_oracle(gpu, oracle, po, mo):
+    t, m = lc.sine_curve(3.0, n=600)
+    m = lc.normalize(m)
+    P, D = _grid(200)
+    got = gpu.ConditionalEntropy(10, 10, po, mo, semantics="cpu").periodograms([t], [m], P, D)
+    want = oracle.ce([t], [m], P, D, 10, 10, po, mo)
+    np.testing.assert_allclose(got, want, rtol=2e-6)
+
+
+@pytest.mark.parametrize("mode", ["plain", "chosen"])
+def test_aov_overlap_vs_oracle(gpu, oracle, mode):
+    t, m = lc.sine_curve(4.0, n=600)
+    P, D = _grid(200)
+    got = gpu.AOV(10, 3, mode=mode, semantics="cpu").periodograms([t], [m], P, D)
+    if mode == "plain":
+        np.testing.assert_array_equal(got, oracle.aov([t], [m], P, D, 10, 3))
+    else:
+        want = oracle.aov_f64([t], [m], P, D, 10, 3)
+        np.testing.assert_allclose(got, want, rtol=1e-6)
+
+
+def test_ce_custom_bins_vs_oracle(gpu, oracle):
+    t, m = lc.eclipse_curve(2.5, n=600)
+    m = lc.normalize(m)
+    P, D = _grid(200)
+    got = gpu.ConditionalEntropy(15, 10, semantics="cpu").periodograms([t], [m], P, D)
+    np.testing.assert_allclose(got, oracle.ce([t], [m], P, D, 15, 10), rtol=2e-6)
+    got = gpu.ConditionalEntropy(20, 5, 2, 2, semantics="cpu").periodograms([t], [m], P, D)
+    np.testing.assert_allclose(got, oracle.ce([t], [m], P, D, 20, 5, 2, 2), rtol=2e-6)
+
+
+# ------------------------------------------------------- chosen vs plain
+
+
+@pytest.mark.parametrize("sem", ["cuda", "cpu"])
+def test_chosen_equals_plain_ce_ls(gpu, sem):
+    ts, ms = _ragged(seed=3)
+    msn = [lc.normalize(m) if len(m) > 1 else np.full(1, 0.5, np.float32) for m in ms]
+    P, D = _grid(500, pdts=(0.0, 2e-4))
+    a = gpu.ConditionalEntropy(mode="plain", semantics=sem).periodograms(ts, msn, P, D)
+    b = gpu.ConditionalEntropy(mode="chosen", semantics=sem).periodograms(ts, msn, P, D)
+    np.testing.assert_array_equal(a, b)
+    msc = [lc.center(m) for m in ms]
+    a = gpu.LombScargle(mode="plain", semantics=sem).periodograms(ts, msc, P, D)
+    b = gpu.LombScargle(mode="chosen", semantics=sem).periodograms(ts, msc, P, D)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_exact_fold_long_baseline(gpu, oracle):
+    """Times ~ MJD 6e4 with short periods (1e5..1e6 cycles): the chosen fold
+    still reproduces the divide bit for bit (bins identical => CE equal)."""
+    rng = np.random.default_rng(11)
+    t = np.sort(rng.uniform(58000.0, 60000.0, 2000)).astype(np.float32)
+    m = lc.normalize(lc.noisy(rng, lc.sinusoid(t, 0.0371), 0.05))
+    P = np.exp(np.linspace(np.log(0.01), np.log(0.1), 700)).astype(np.float32)
+    D = np.array([0.0, 1e-7], np.float32)
+    a = gpu.ConditionalEntropy(mode="plain", semantics="cpu").periodograms([t], [m], P, D)
+    b = gpu.ConditionalEntropy(mode="chosen", semantics="cpu").periodograms([t], [m], P, D)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_allclose(b, oracle.ce([t], [m], P, D), rtol=2e-6)
+
+
+# ----------------------------------------------------- peaks on the device
+
+
+@pytest.mark.parametrize("algo", ["ce", "aov", "ls"])
+@pytest.mark.parametrize("n_peaks,min_distance", [(32, 1), (8, 3), (16, 20), (1, 1)])
+def test_peaks_match_oracle_on_same_periodogram(gpu, oracle, algo, n_peaks, min_distance):
+    ts, ms = _ragged(seed=5, lengths=(40, 300, 700))
+    P, D = _grid(2500, pdts=(0.0, 1e-4))  # 5000 cells: crosses the 2048-sample chunk
+    if algo == "ce":
+        obj, ms, use_max = gpu.ConditionalEntropy(), [lc.normalize(m) for m in ms], False
+    elif algo == "aov":
+        obj, use_max = gpu.AOV(), True
+    else:
+        obj, ms, use_max = gpu.LombScargle(), [lc.center(m) for m in ms], True
+    pg = obj.periodograms(ts, ms, P, D)
+    idx, val = obj.peaks(ts, ms, P, D, n_peaks, min_distance)
+    oi, ov = oracle.find_top_peaks_batched(pg, n_peaks, min_distance, use_max)
+    np.testing.assert_array_equal(idx, oi)
+    np.testing.assert_array_equal(val, ov)
+
+
+def test_peaks_golden_vectors_on_device(gpu, oracle):
+    import json
+    import os
+
+    path = os.path.join(os.path.dirname(__file__), "golden", "peaks_golden.json")
+    for case in json.load(open(path))["cases"]:
+        data = np.array(case["data"], np.float32).reshape(1, -1, 1)
+        if data.size == 0:
+            data = np.zeros((1, 0, 1), np.float32)
+        idx, val = gpu.find_top_peaks_batched(data, case["n_peaks"], case["min_distance"],
+                                              case["use_max"])
+        oi, ov = oracle.find_top_peaks_batched(data, case["n_peaks"], case["min_distance"],
+                                               case["use_max"])
+        np.testing.assert_array_equal(idx, oi, err_msg=case["name"])
+        np.testing.assert_array_equal(val, ov, err_msg=case["name"])
+        if case["expect_idx"] is not None:
+            k = len(case["expect_idx"])
+            assert idx[0, :k].tolist() == case["expect_idx"], case["name"]
+
+
+# ------------------------------------------------- reference CUDA build
+
+
+def _ref_or_skip(oracle):
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref/libpfref.so not built (needs the reference checkout)")
+
+
+def test_ce_vs_reference_cuda(gpu, oracle):
+    _ref_or_skip(oracle)
+    ts, ms = _ragged(seed=9)
+    ms = [lc.normalize(m) if len(m) > 1 else np.full(1, 0.5, np.float32) for m in ms]
+    P, D = _grid(400, pdts=(0.0, 1e-4, -1e-3))
+    want = oracle.ref_cuda("ce", ts, ms, P, D, n_phase=10, n_mag=10)
+    for mode in ("plain", "chosen"):
+        got = gpu.ConditionalEntropy(mode=mode).periodograms(ts, ms, P, D)
+        np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-7)
+
+
+def test_aov_vs_reference_cuda(gpu, oracle):
+    _ref_or_skip(oracle)
+    ts, ms = _ragged(seed=9, lengths=(64, 300, 1025, 4096, 4097, 6000))
+    P, D = _grid(400, pdts=(0.0, 1e-4))
+    want = oracle.ref_cuda("aov", ts, ms, P, D, n_phase=15)
+    for mode in ("plain", "chosen"):
+        got = gpu.AOV(15, mode=mode).periodograms(ts, ms, P, D)
+        np.testing.assert_allclose(got, want, rtol=2e-4, atol=1e-4 * np.max(np.abs(want)))
+
+
+def test_ls_vs_reference_cuda(gpu, oracle):
+    _ref_or_skip(oracle)
+    ts, ms = _ragged(seed=9)
+    ms = [lc.center(m) for m in ms]
+    P, D = _grid(400, pdts=(0.0, 1e-4))
+    want = oracle.ref_cuda("ls", ts, ms, P, D)
+    for mode in ("plain", "chosen"):
+        got = gpu.LombScargle(mode=mode).periodograms(ts, ms, P, D)
+        _ls_close(got, want, rel=1e-4)
+
+
+# ----------------------------------------------------------- edge cases
+
+
+def test_empty_and_single_point_curves(gpu, oracle):
+    e = np.zeros(0, np.float32)
+    one = np.array([3.0], np.float32)
+    P, D = _grid(50)
+    ce = gpu.ConditionalEntropy(semantics="cpu").periodograms([e, one], [e, one * 0 + 0.5], P, D)
+    assert np.all(np.isnan(ce[0]))
+    np.testing.assert_allclose(ce[1], oracle.ce([one], [one * 0 + 0.5], P, D)[0], rtol=1e-6)
+    aov = gpu.AOV(semantics="cpu").periodograms([e], [e], P, D)
+    assert np.all(aov == 0)
+    ls = gpu.LombScargle(semantics="cpu").periodograms([e], [e], P, D)
+    assert np.all(ls == 0)
+
+
+def test_nonfinite_times_rejected(gpu):
+    from periodfind_b200._native import PeriodfindError
+
+    t = np.array([0.0, np.nan, 2.0], np.float32)
+    with pytest.raises(PeriodfindError, match="finite"):
+        gpu.AOV().periodograms([t], [t * 0], *_grid(10))
+
+
+def test_zero_period_rejected(gpu):
+    from periodfind_b200._native import PeriodfindError
+
+    t = np.arange(10, dtype=np.float32)
+    with pytest.raises(PeriodfindError, match="non-zero"):
+        gpu.LombScargle().periodograms([t], [t], np.array([1.0, 0.0], np.float32),
+                                       np.zeros(1, np.float32))
+
+
+def test_repeat_calls_grow_and_shrink(gpu, oracle):
+    """Context buffers are reused across calls of different sizes."""
+    obj = gpu.AOV(semantics="cpu", mode="plain")
+    for n_curves, n in [(2, 50), (5, 3000), (1, 10), (3, 700)]:
+        ts, ms = _ragged(seed=n, lengths=[n] * n_curves)
+        P, D = _grid(123)
+        np.testing.assert_array_equal(obj.periodograms(ts, ms, P, D),
+                                      oracle.aov(ts, ms, P, D, 10))
+
+
+def test_device_pointer_entry_points(gpu):
+    torch = pytest.importorskip("torch")
+    from periodfind_b200 import _native as nat
+
+    ts, ms = _ragged(seed=21, lengths=(10, 333, 1500))
+    P, D = _grid(200, pdts=(0.0, 1e-4))
+    host = gpu.LombScargle(mode="chosen").periodograms(ts, [lc.center(m) for m in ms], P, D)
+    off = np.zeros(len(ts) + 1, np.int64)
+    np.cumsum([len(t) for t in ts], out=off[1:])
+    dt = torch.from_numpy(np.concatenate(ts)).cuda()
+    dm = torch.from_numpy(np.concatenate([lc.center(m) for m in ms])).cuda()
+    dp = torch.from_numpy(P).cuda()
+    dd = torch.from_numpy(D).cuda()
+    out = torch.empty((len(ts), len(P), len(D)), dtype=torch.float32, device="cuda")
+    ctx = nat.default_context(0)
+    stream = torch.cuda.current_stream().cuda_stream
+    with ctx.lock:
+        ctx.check(ctx.lib.pf_ls_dev(ctx.handle, dt.data_ptr(), dm.data_ptr(), off.ctypes.data,
+                                    len(ts), dp.data_ptr(), len(P), dd.data_ptr(), len(D),
+                                    nat.PF_MODE_CHOSEN, out.data_ptr(), stream))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy(), host)

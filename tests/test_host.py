@@ -1,0 +1,175 @@
+"""CPU tests of the host-side code: input helpers, result containers, the
+GPU classes' argument handling before any device work, and the C ABI
+library's exports (no GPU compute)."""
+
+import ctypes
+import os
+import re
+import warnings
+
+import numpy as np
+import pytest
+
+from periodfind_b200 import Periodogram, Statistics
+from periodfind_b200 import _native
+from periodfind_b200._utils import ensure_float32, prepare_magnitudes, validate_inputs
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+# ---------------------------------------------------------------- _utils
+# Behaviour of periodfind/_utils.py (tests/test_periodfind.py:64-117).
+
+def test_prepare_normalize_range():
+    r = prepare_magnitudes([np.array([1, 2, 3], np.float32)], False, True)[0]
+    assert r.dtype == np.float32
+    assert r.min() >= 0.0 and r.max() <= 1.0
+
+
+def test_prepare_center():
+    r = prepare_magnitudes([np.array([1, 2, 3], np.float32)], True, False)[0]
+    assert abs(np.mean(r)) < 1e-6
+
+
+def test_prepare_passthrough():
+    a = np.array([1, 2, 3], np.float32)
+    assert prepare_magnitudes([a], False, False)[0] is a
+
+
+def test_prepare_conflict_warns_and_centers():
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        r = prepare_magnitudes([np.array([1, 2, 3], np.float32)], True, True)[0]
+    assert any(issubclass(x.category, RuntimeWarning) for x in w)
+    assert abs(np.mean(r)) < 1e-6
+
+
+def test_validate_inputs():
+    validate_inputs([np.zeros(2)], [np.zeros(2)])
+    with pytest.raises(ValueError, match="same number of light curves"):
+        validate_inputs([np.zeros(2), np.zeros(2)], [np.zeros(2)])
+    with pytest.raises(ValueError, match="different lengths"):
+        validate_inputs([np.zeros(3)], [np.zeros(2)])
+
+
+def test_ensure_float32():
+    ensure_float32([np.zeros(2, np.float32)], "x")
+    with pytest.raises(TypeError, match="float64.*expected float32"):
+        ensure_float32([np.zeros(2)], "x")
+
+
+# ------------------------------------------------- Statistics / Periodogram
+
+def test_statistics_significance():
+    s = Statistics([1.0, 0.0], 5.0, 2.0, 1.5, 2.5, 0.5)
+    assert s.significance == pytest.approx(2.0)
+    s.significance_type = "madmedian"
+    assert s.significance == pytest.approx(5.0)
+    s.significance_type = "nope"
+    with pytest.raises(NotImplementedError):
+        _ = s.significance
+    assert "Statistics(params=" in repr(s)
+
+
+def test_statistics_from_data_max_min_multi():
+    data = np.array([[1.0], [5.0], [3.0], [0.5]], np.float32)
+    params = [np.array([10, 20, 30, 40], np.float32), np.array([0.0], np.float32)]
+    s = Statistics.statistics_from_data(data, params, True)
+    assert s.params[0] == 20 and s.value == 5.0
+    s = Statistics.statistics_from_data(data, params, False)
+    assert s.params[0] == 40
+    lst = Statistics.statistics_from_data(data, params, True, n=3)
+    assert [x.value for x in lst] == [5.0, 3.0, 1.0]
+    assert lst[0].mean == pytest.approx(np.mean(data))
+    assert lst[0].median == pytest.approx(np.median(data))
+
+
+def test_periodogram_best_params():
+    data = np.array([[1.0], [5.0], [3.0]], np.float32)
+    params = [np.array([1, 2, 3], np.float32), np.array([0.0], np.float32)]
+    pg = Periodogram(data, params, True)
+    assert "use_max=True" in repr(pg)
+    b = pg.best_params()
+    assert b.params[0] == 2
+    assert pg.mean is not None and pg.mad is not None
+    assert Periodogram(data, params, False).best_params().params[0] == 1
+
+
+# -------------------------------------------------------------- C ABI
+
+
+def _declared_symbols():
+    with open(os.path.join(ROOT, "include", "pf.h")) as fh:
+        text = fh.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pf_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_and_binding_agree():
+    assert _declared_symbols() == sorted(_native.SIGNATURES)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_native.LIB_PATH)
+    for name in _declared_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_no_oracle_in_product_path():
+    """The product package never imports the test oracle."""
+    pkg = os.path.join(ROOT, "periodfind_b200")
+    for dirpath, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith((".py", ".cu", ".cuh", ".h", ".inc")):
+                with open(os.path.join(dirpath, f)) as fh:
+                    src = fh.read()
+                assert "oracle" not in src.lower().replace("oracle/", ""), f
+
+
+# ----------------------------------------- GPU classes: checks before device work
+
+def _gpu_classes():
+    from periodfind_b200 import gpu
+
+    return gpu
+
+
+def test_invalid_output_raises_before_device_work():
+    gpu = _gpu_classes()
+    t = np.arange(5, dtype=np.float32)
+    with pytest.raises(NotImplementedError):
+        gpu.ConditionalEntropy().calc([t], [t], np.ones(3, np.float32), np.zeros(1, np.float32),
+                                      output="invalid")
+
+
+def test_float64_inputs_raise():
+    gpu = _gpu_classes()
+    t = np.arange(3, dtype=np.float64)
+    with pytest.raises(TypeError, match="expected float32"):
+        gpu.ConditionalEntropy().calc([t], [t], np.ones(3, np.float32), np.zeros(1, np.float32))
+
+
+def test_mismatched_inputs_raise():
+    gpu = _gpu_classes()
+    t = np.arange(3, dtype=np.float32)
+    with pytest.raises(ValueError):
+        gpu.AOV().calc([t, t], [t], np.ones(3, np.float32), np.zeros(1, np.float32))
+
+
+def test_grid_type_checks():
+    gpu = _gpu_classes()
+    t = np.arange(3, dtype=np.float32)
+    with pytest.raises(ValueError, match="dtype mismatch"):
+        gpu.LombScargle().calc([t], [t], np.ones(3), np.zeros(1, np.float32))
+    with pytest.raises(TypeError):
+        gpu.LombScargle().calc([t], [t], [1.0, 2.0], np.zeros(1, np.float32))
+
+
+def test_mode_and_semantics_validation():
+    gpu = _gpu_classes()
+    with pytest.raises(ValueError):
+        gpu.AOV(mode="fast")
+    with pytest.raises(ValueError):
+        gpu.AOV(semantics="rust")
+    assert gpu.AOV(mode="plain", semantics="cpu")._flags == _native.PF_SEM_CPU
+    assert gpu.LombScargle(fold="df")._flags & _native.PF_FOLD_DF
