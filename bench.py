@@ -1,0 +1,441 @@
+"""Benchmark: curve x period x point evaluations per second on B200.
+
+Workload (one "step"): Conditional Entropy (10 x 10 bins) and AOV (15 bins)
+periodograms plus the top-32 peak search, over 1000 light curves x 4096
+points, 10000 trial periods log-spaced in [0.1, 100] days and period
+derivatives [0, 1e-6] -- 2 x 8.19e10 evaluations per step.  Synthetic
+curves (seeded): half sinusoids, a quarter sawtooth, a quarter box eclipses
+(depth 0.5, duty 0.05) with N(0, 0.05^2) noise, times uniform over 2000 days.
+
+Reported (one JSON line on rank 0):
+  value     evals/s of the chosen form, inputs resident in HBM, device-timed
+            with CUDA events around each step (max over ranks); L2 is
+            flushed (256 MB write) between timed steps, outside the events.
+  e2e       the same metric through the public API (gpu.ConditionalEntropy /
+            gpu.AOV .calc(..., output='peaks')) with host numpy inputs: the
+            timed region includes magnitude preparation, the H2D copy of the
+            step's inputs and the D2H copy of the peaks.
+  plain     the plain form (the reference's fold, op for op) on the same
+            device-resident workload, for the chosen-vs-plain ratio.
+  roofline  the dominant fold kernel against the measured FP64-pipe peak
+            (this path is FP64/XU issue bound; HBM traffic is given too).
+  cpu_baseline  the oracle (C/OpenMP restatement of the reference's Rust
+            CPU path) on all host cores over a bounded sample of curves.
+
+--impl reference runs that CPU restatement (the reference's CPU
+implementation is Rust; no Rust toolchain exists on these machines) as the
+reference arm, on rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CURVES = 1000
+N_POINTS = 4096
+N_PERIODS = 10000
+PDTS = (0.0, 1e-6)
+N_PEAKS = 32
+SEED = 20261205
+WORKLOAD = "CE(10x10)+AOV(15)+top32 peaks, 1000 curves x 4096 pts, 10000 log periods [0.1,100] d x pdts [0,1e-6]"
+METRIC = "curve*period*point evals/s on 1 B200, chosen vs plain, at stated error"
+
+
+def make_workload(n_curves=N_CURVES, seed=SEED):
+    from tests import lightcurves as lc
+
+    ts, ms = lc.batch_config2(n_curves, N_POINTS, seed)
+    periods = np.exp(np.linspace(np.log(0.1), np.log(100.0), N_PERIODS)).astype(np.float32)
+    pdts = np.array(PDTS, np.float32)
+    return ts, ms, periods, pdts
+
+
+def evals_per_step(n_curves):
+    return 2 * n_curves * N_POINTS * N_PERIODS * len(PDTS)
+
+
+# ----------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.idx)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        mhz, mx, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                mx = float(parts[2])
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz),
+                "power_w_max": max(power) if power else None}
+
+
+# -------------------------------------------------------------- pipe peaks
+
+
+def measure_pipes():
+    import ctypes
+
+    lib = ctypes.CDLL(os.path.join(ROOT, "periodfind_b200", "libpfpeaks.so"))
+
+    class R(ctypes.Structure):
+        _fields_ = [("name", ctypes.c_char * 32), ("ops_per_clk_per_sm", ctypes.c_double),
+                    ("ops_per_s", ctypes.c_double), ("sm_mhz", ctypes.c_double)]
+
+    arr = (R * 32)()
+    k = lib.pfpk_measure(0, arr, 32)
+    return {arr[i].name.decode(): {"per_s": arr[i].ops_per_s,
+                                   "per_clk_sm": arr[i].ops_per_clk_per_sm,
+                                   "mhz": arr[i].sm_mhz} for i in range(max(k, 0))}
+
+
+# ----------------------------------------------------------- device step
+
+
+class DeviceStep:
+    """CE + AOV + peaks on device-resident packed curves via the C ABI."""
+
+    def __init__(self, ts, ms, periods, pdts, mode_flags, torch, device=0):
+        from periodfind_b200 import _native as nat
+        from tests import lightcurves as lc
+
+        self.nat = nat
+        self.torch = torch
+        self.ctx = nat.default_context(device)
+        self.flags = mode_flags
+        off = np.zeros(len(ts) + 1, np.int64)
+        np.cumsum([len(t) for t in ts], out=off[1:])
+        self.off = off
+        dev = "cuda"
+        self.t = torch.from_numpy(np.concatenate(ts)).to(dev)
+        self.m_ce = torch.from_numpy(np.concatenate([lc.normalize(m) for m in ms])).to(dev)
+        self.m_aov = torch.from_numpy(np.concatenate(ms)).to(dev)
+        self.P = torch.from_numpy(periods).to(dev)
+        self.D = torch.from_numpy(pdts).to(dev)
+        n = len(ts)
+        self.n = n
+        cells = len(periods) * len(pdts)
+        self.cells = cells
+        self.pg_ce = torch.empty((n, cells), dtype=torch.float32, device=dev)
+        self.pg_aov = torch.empty((n, cells), dtype=torch.float32, device=dev)
+        self.pk_idx = torch.empty((2, n, N_PEAKS), dtype=torch.int64, device=dev)
+        self.pk_val = torch.empty((2, n, N_PEAKS), dtype=torch.float32, device=dev)
+        self.np_ = len(periods)
+        self.nd = len(pdts)
+
+    def run(self, stream):
+        c, lib, h, nat = self.ctx, self.ctx.lib, self.ctx.handle, self.nat
+        c.check(lib.pf_ce_dev(h, self.t.data_ptr(), self.m_ce.data_ptr(), self.off.ctypes.data,
+                              self.n, self.P.data_ptr(), self.np_, self.D.data_ptr(), self.nd,
+                              10, 10, 1, 1, self.flags, self.pg_ce.data_ptr(), stream))
+        c.check(lib.pf_find_peaks_dev(h, self.pg_ce.data_ptr(), self.n, self.cells, N_PEAKS, 1,
+                                      0, self.pk_idx[0].data_ptr(), self.pk_val[0].data_ptr(),
+                                      stream))
+        c.check(lib.pf_aov_dev(h, self.t.data_ptr(), self.m_aov.data_ptr(), self.off.ctypes.data,
+                               self.n, self.P.data_ptr(), self.np_, self.D.data_ptr(), self.nd,
+                               15, 1, self.flags, self.pg_aov.data_ptr(), stream))
+        c.check(lib.pf_find_peaks_dev(h, self.pg_aov.data_ptr(), self.n, self.cells, N_PEAKS, 1,
+                                      1, self.pk_idx[1].data_ptr(), self.pk_val[1].data_ptr(),
+                                      stream))
+
+
+def time_device(step, steps, warmup, torch, flush):
+    stream = torch.cuda.current_stream()
+    s = stream.cuda_stream
+    for _ in range(warmup):
+        step.run(s)
+    torch.cuda.synchronize()
+    launches0 = step.ctx.launches
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()  # evict L2 between timed steps (outside the events)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step.run(s)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    return total / steps, step.ctx.launches - launches0
+
+
+def time_kernels(step, torch, reps=3):
+    """Average duration of the CE and AOV fold kernels (their own events)."""
+    s = torch.cuda.current_stream().cuda_stream
+    ce, aov = [], []
+    c, lib, h = step.ctx, step.ctx.lib, step.ctx.handle
+    for _ in range(reps):
+        c.check(lib.pf_ce_dev(h, step.t.data_ptr(), step.m_ce.data_ptr(), step.off.ctypes.data,
+                              step.n, step.P.data_ptr(), step.np_, step.D.data_ptr(), step.nd,
+                              10, 10, 1, 1, step.flags, step.pg_ce.data_ptr(), s))
+        torch.cuda.synchronize()
+        ce.append(c.last_kernel_ms)
+        c.check(lib.pf_aov_dev(h, step.t.data_ptr(), step.m_aov.data_ptr(), step.off.ctypes.data,
+                               step.n, step.P.data_ptr(), step.np_, step.D.data_ptr(), step.nd,
+                               15, 1, step.flags, step.pg_aov.data_ptr(), s))
+        torch.cuda.synchronize()
+        aov.append(c.last_kernel_ms)
+    return float(np.mean(ce)), float(np.mean(aov))
+
+
+def time_e2e(ts, ms, periods, pdts, steps, warmup, device=0):
+    from periodfind_b200 import gpu
+
+    ce = gpu.ConditionalEntropy(10, 10, device=device)
+    aov = gpu.AOV(15, device=device)
+    for _ in range(warmup):
+        ce.calc(ts, ms, periods, pdts, output="peaks", n_peaks=N_PEAKS)
+        aov.calc(ts, ms, periods, pdts, output="peaks", n_peaks=N_PEAKS)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        a = ce.calc(ts, ms, periods, pdts, output="peaks", n_peaks=N_PEAKS)
+        b = aov.calc(ts, ms, periods, pdts, output="peaks", n_peaks=N_PEAKS)
+    dt = (time.perf_counter() - t0) / steps
+    assert len(a) == len(ts) and len(b) == len(ts)
+    return dt
+
+
+# ------------------------------------------------------------ CPU baseline
+
+
+def cpu_baseline(ts, ms, periods, pdts, target_s=12.0):
+    """The oracle (C/OpenMP restatement of the reference's Rust path) on all
+    host cores over the first k curves, k sized for ~target_s of work."""
+    from oracle import oracle as O
+    from tests import lightcurves as lc
+
+    cores = os.cpu_count() or 1
+    k = 1
+    t0 = time.perf_counter()
+    O.ce(ts[:k], [lc.normalize(m) for m in ms[:k]], periods, pdts, 10, 10, n_threads=cores)
+    O.aov(ts[:k], ms[:k], periods, pdts, 15, n_threads=cores)
+    one = time.perf_counter() - t0
+    k = int(max(1, min(len(ts), target_s / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    O.ce(ts[:k], [lc.normalize(m) for m in ms[:k]], periods, pdts, 10, 10, n_threads=cores)
+    O.aov(ts[:k], ms[:k], periods, pdts, 15, n_threads=cores)
+    dt = time.perf_counter() - t0
+    value = evals_per_step(k) / dt
+    return {"value": value, "unit": "evals/s", "cores": cores, "kind": "port",
+            "sample": f"{k} of {len(ts)} curves (CE 10x10 + AOV 15, full 10000x2 grid), "
+                      f"{dt:.1f} s on {cores} threads"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    ts, ms, periods, pdts = make_workload()
+    from oracle import oracle as O
+    from tests import lightcurves as lc
+
+    cores = os.cpu_count() or 1
+    k = 2
+    sub_t, sub_m = ts[:k], ms[:k]
+    run = lambda: (O.ce(sub_t, [lc.normalize(m) for m in sub_m], periods, pdts, 10, 10,
+                        n_threads=cores),
+                   O.aov(sub_t, sub_m, periods, pdts, 15, n_threads=cores))
+    for _ in range(args.warmup):
+        run()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    per_step = float(np.mean(times))
+    value = evals_per_step(k) / per_step
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 fold, f32 statistics", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_curves_per_step": k},
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "port",
+                         "sample": f"{k} of {N_CURVES} curves per step, full grid, "
+                                   f"C/OpenMP restatement of the reference's Rust CPU path"},
+        "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- main
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--curves", type=int, default=N_CURVES)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    # Each rank processes its own batch of curves (weak scaling, no exchange).
+    ts, ms, periods, pdts = make_workload(args.curves, SEED + rank)
+    from periodfind_b200 import _native as nat
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    pipes = measure_pipes() if rank == 0 else {}
+
+    chosen = DeviceStep(ts, ms, periods, pdts, nat.PF_MODE_CHOSEN, torch, local)
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ms_step, launches = time_device(chosen, args.steps, args.warmup, torch, flush)
+    clock_info = clocks.stop()
+    t_max = torch.tensor([ms_step], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_step = float(t_max.item())
+    ce_ms, aov_ms = time_kernels(chosen, torch)
+
+    plain = DeviceStep(ts, ms, periods, pdts, nat.PF_MODE_PLAIN, torch, local)
+    plain_ms, _ = time_device(plain, max(1, min(args.steps, 3)), 1, torch, flush)
+    pt = torch.tensor([plain_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(pt, op=dist.ReduceOp.MAX)
+    plain_ms = float(pt.item())
+    del plain
+
+    e2e_s = time_e2e(ts, ms, periods, pdts, max(1, min(args.steps, 3)), 1, local)
+    et = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    e2e_s = float(et.item())
+
+    n_eval = evals_per_step(args.curves) * world
+    value = n_eval / (ms_step * 1e-3)
+    if rank == 0:
+        # Roofline of the dominant kernel (CE fold): FP64-pipe operations.
+        evals_ce = args.curves * N_POINTS * N_PERIODS * len(PDTS)
+        fp64_per_eval = FP64_OPS_PER_EVAL
+        achieved = evals_ce * fp64_per_eval / (ce_ms * 1e-3) / 1e9
+        peak = pipes.get("dfma", {}).get("per_s", float("nan")) / 1e9
+        in_bytes = args.curves * N_POINTS * 8 + N_PERIODS * 4
+        out_bytes = args.curves * N_PERIODS * len(PDTS) * 4
+        hbm_gbs = (in_bytes + out_bytes) / (ce_ms * 1e-3) / 1e9
+        cpu = None if args.no_cpu else cpu_baseline(ts, ms, periods, pdts)
+        h2d = 2 * sum(t.nbytes + m.nbytes for t, m in zip(ts, ms)) + 2 * (periods.nbytes + pdts.nbytes)
+        d2h = 2 * args.curves * N_PEAKS * 12
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 fold (exact), f32/fixed-point statistics", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "curves_per_gpu": args.curves,
+                       "points": N_POINTS, "periods": N_PERIODS, "pdts": list(PDTS),
+                       "l2": "flushed (256 MB write) between timed steps",
+                       "parallelism": f"{world} independent replicas (curves sharded)"},
+            "plain": {"value": n_eval / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+                      "chosen_over_plain": plain_ms / ms_step},
+            "e2e": {"value": n_eval / e2e_s, "unit": "evals/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "ms_per_step": e2e_s * 1e3,
+                    "path": "gpu.ConditionalEntropy/AOV.calc(list of numpy, output='peaks')"},
+            "roofline": {"bound": "fp64", "kernel": "CE fold (chosen)",
+                         "achieved": achieved, "peak": peak, "unit": "Gop/s",
+                         "frac": achieved / peak if peak == peak else None,
+                         "ops_per_eval": fp64_per_eval, "kernel_ms": ce_ms,
+                         "peak_source": "measured DFMA rate (periodfind_b200/csrc/pipe_peaks.cu)",
+                         "traffic": None,
+                         "hbm_view": {"achieved_gbs": hbm_gbs, "peak_gbs": 6453.7,
+                                      "frac": hbm_gbs / 6453.7}},
+            "kernels_ms": {"ce_fold": ce_ms, "aov_fold": aov_ms},
+            "pipes": {k: round(v["per_s"] / 1e12, 3) for k, v in pipes.items()},
+            "cpu_baseline": cpu,
+            "clocks": clock_info,
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+# FP64-pipe operations per evaluation in the chosen CE fold: the exact
+# quotient (DMUL, 2 DFMA, DADD).  Updated with the kernel.
+FP64_OPS_PER_EVAL = 4
+
+if __name__ == "__main__":
+    main()

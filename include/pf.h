@@ -23,10 +23,12 @@
  * mode bits
  *  PF_MODE_PLAIN   the reference's fold operation for operation: an FP64
  *                  divide per (point, period) (periodfind/cuda/ce.cu:141-143).
- *  PF_MODE_CHOSEN  the tuned form: the same folded phase computed from a
- *                  per-period reciprocal with a correction step (bit-identical
- *                  to the plain fold), fused binning/statistics and the
- *                  strategy the tuner picked for the curve-length class.
+ *  PF_MODE_CHOSEN  the tuned form.  CE/AOV: the reference's quotient without
+ *                  a divide (bit-identical), bins from FP64/integer ops with
+ *                  the reference's exact sequence near bin edges (identical
+ *                  bin occupancies), 16-bit CE counters, exact fixed-point
+ *                  AOV sums.  LS: split-precision FP32 phase (more accurate
+ *                  than the reference's f32-rounded phase).
  *  PF_SEM_CPU      arithmetic of the reference's CPU (Rust) path: IEEE
  *                  divides, no multiply-add contraction, accurate libm-style
  *                  log/sin/cos.  Without it the arithmetic follows the
@@ -34,6 +36,8 @@
  *  PF_FOLD_F32     (LS precision study) fold t/P entirely in FP32.
  *  PF_FOLD_DF      (LS) split-precision FP32 phase frac(t * f) with the
  *                  frequency as an unevaluated float pair; no FP64 per point.
+ *  PF_FOLD_EXACT   (LS, chosen) the divide-free exact fold instead of the
+ *                  split-precision phase: bit-identical to the plain form.
  */
 #ifndef PERIODFIND_B200_PF_H
 #define PERIODFIND_B200_PF_H
@@ -56,6 +60,7 @@ extern "C" {
 #define PF_SEM_CPU 0x10
 #define PF_FOLD_F32 0x100
 #define PF_FOLD_DF 0x200
+#define PF_FOLD_EXACT 0x400
 
 typedef struct pf_ctx pf_ctx;
 
@@ -154,6 +159,13 @@ int pf_ls_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
               const int64_t* offsets, uint64_t n_curves,
               const float* d_periods, uint64_t n_per, const float* d_pdts,
               uint64_t n_pdt, int mode, float* d_out, void* stream);
+
+/* Peak search on device periodograms [n_curves][flat_len]; d_out_idx /
+ * d_out_val are device arrays [n_curves][n_peaks] (-1 / 0 padded). */
+int pf_find_peaks_dev(pf_ctx* ctx, const float* d_data, uint64_t n_curves,
+                      uint64_t flat_len, uint32_t n_peaks, uint32_t min_distance,
+                      int use_max, int64_t* d_out_idx, float* d_out_val,
+                      void* stream);
 
 /* Number of kernels this context has launched since creation (telemetry
  * for benchmarks: launches of the library's own kernels only). */

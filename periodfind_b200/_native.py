@@ -27,6 +27,7 @@ PF_MODE_CHOSEN = 0x1
 PF_SEM_CPU = 0x10
 PF_FOLD_F32 = 0x100
 PF_FOLD_DF = 0x200
+PF_FOLD_EXACT = 0x400
 
 _vp = ctypes.c_void_p
 _u64 = ctypes.c_uint64
@@ -55,6 +56,7 @@ SIGNATURES = {
     "pf_aov_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int, _vp, _vp],
                    _int),
     "pf_ls_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _int, _vp, _vp], _int),
+    "pf_find_peaks_dev": ([_vp, _vp, _u64, _u64, _u32, _u32, _int, _vp, _vp, _vp], _int),
     "pf_launch_count": ([_vp], _u64),
     "pf_last_kernel_ms": ([_vp], ctypes.c_double),
 }

@@ -6,4 +6,5 @@
 #define PF_SUFFIX cudasem
 #include "pf_launch.h"
 #include "pf_fold.cuh"
+#include "pf_bin.cuh"
 #include "pf_kern_dispatch.inc"

@@ -54,7 +54,7 @@ struct pf_ctx {
     cudaEvent_t ev_done = nullptr;              // last device-pointer call done
     bool staged_pending = false, done_recorded = false, timed_pending = false;
     std::string err;
-    DevBuf d_in, d_aux32, d_aux64, d_out, d_pidx, d_pval, d_pack;
+    DevBuf d_in, d_aux32, d_aux64, d_out, d_pidx, d_pval, d_pack, d_misc;
     PinnedBuf h_in;
     uint64_t launches = 0;
     double last_ms = -1.0;
@@ -202,40 +202,65 @@ int check_grid_host(pf_ctx* ctx, const Job& j) {
     return PF_OK;
 }
 
-// Launch configuration.  The private histogram must fit with at least two
-// CTAs per SM where possible; LS has no histogram.
+// Warps per SM a CTA shape reaches, limited by shared memory (228 KB per
+// SM, 1 KB reserved per CTA) and the 64-warp / 32-CTA limits.
+int warps_per_sm(size_t smem, int block) {
+    const size_t per_sm = 233472;
+    int by_smem = (int)(per_sm / (smem + 1024));
+    int ctas = std::min(std::min(by_smem, 32), 64 / (block / 32));
+    return ctas * (block / 32);
+}
+
+// Launch configuration: the kernel kind, fold, accumulator, and the block
+// size that gives the most resident warps for this histogram size.
 FoldConfig choose_config(pf_ctx* ctx, const Job& j, uint32_t max_len, bool& ok) {
     FoldConfig c{};
+    c.kind = KIND_FOLD;
+    c.cnt16 = false;
     c.algo = j.algo;
     const bool chosen = (j.mode & PF_MODE_CHOSEN) != 0;
     c.fold = chosen ? FOLD_EXACT : FOLD_REF;
     if (j.algo == ALGO_LS) {
+        if (chosen) c.fold = (j.mode & PF_FOLD_EXACT) ? FOLD_EXACT : FOLD_DF;
         if (j.mode & PF_FOLD_DF) c.fold = FOLD_DF;
         if (j.mode & PF_FOLD_F32) c.fold = FOLD_F32;
     }
     c.acc = AOVACC_F32;
-    if (j.algo == ALGO_AOV && chosen &&
-        (uint64_t)max_len * j.po < (1ull << (64 - kFixCountShift)) - 1ull)
-        c.acc = AOVACC_FIX;
     c.ovl = (j.algo == ALGO_CE) ? (j.po > 1 || j.mo > 1) : (j.algo == ALGO_AOV && j.po > 1);
+    if (chosen && !c.ovl && (j.algo == ALGO_CE || j.algo == ALGO_AOV) && max_len < 65536u) {
+        c.kind = KIND_BIN;
+        c.cnt16 = (j.algo == ALGO_CE);
+    } else if (j.algo == ALGO_AOV && chosen &&
+               (uint64_t)max_len * j.po < (1ull << (64 - kFixCountShift)) - 1ull) {
+        c.acc = AOVACC_FIX;
+    }
     ok = false;
-    const size_t budget2 = ctx->smem_optin / 2 - 1024;  // two CTAs per SM
+    int best_warps = 0;
     const int blocks[3] = {256, 128, 64};
     for (int b : blocks) {
-        c.block = b;
-        if (fold_smem(c, j.n_phase, j.n_mag) <= budget2) {
+        FoldConfig t = c;
+        t.block = b;
+        const size_t sm = fold_smem(t, j.n_phase, j.n_mag);
+        if (sm > ctx->smem_optin) continue;
+        const int wps = warps_per_sm(sm, b);
+        if (wps > best_warps) {
+            best_warps = wps;
+            c.block = b;
             ok = true;
-            return c;
-        }
-    }
-    for (int b : blocks) {
-        c.block = b;
-        if (fold_smem(c, j.n_phase, j.n_mag) <= ctx->smem_optin) {
-            ok = true;
-            return c;
         }
     }
     return c;
+}
+
+// Bin-edge guard of the bin kernel, in units of 2^-20 of a phase bin: the
+// reference's quotient folded / bin_size differs from frac(q) * n by less
+// than 2 ulp (f32 divide) + n * 2^-23 (bin width rounding) + n * 2^-25
+// (f64 -> f32 rounding of the phase), plus two units of margin.
+uint32_t edge_guard(uint32_t n) {
+    int cl = 0;
+    while ((1u << cl) < n + 1u) cl++;
+    const double delta = ldexp(1.0, cl - 22) + n * ldexp(1.0, -23) + n * ldexp(1.0, -25);
+    return (uint32_t)ceil(delta * 1048576.0) + 2u;
 }
 
 // Work list: for each curve (longest first) and each period derivative,
@@ -359,9 +384,30 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
     p.phase_bin_size = bin_size(j.n_phase, cpu);
     p.mag_bin_size = bin_size(j.n_mag, cpu);
     p.out = d_out;
+    p.edge_d = edge_guard(j.n_phase);
     const uint32_t ncur = (uint32_t)j.n_curves;
     int rc;
-    if (j.algo == ALGO_CE) {
+    if ((rc = ensure_dev(ctx, ctx->d_misc, 256)) != PF_OK) return rc;
+    p.tmax_bits = (const unsigned*)ctx->d_misc.p;
+    PF_CUDA(launch_tmax(p.t, L.total_pts, (unsigned*)ctx->d_misc.p, s), "max|t| kernel");
+    ctx->launches++;
+    if (cfg.kind == KIND_BIN && j.algo == ALGO_CE) {
+        if ((rc = ensure_dev(ctx, ctx->d_aux64, L.total_pts * 8 + 32)) != PF_OK) return rc;
+        p.aux64 = (const uint64_t*)ctx->d_aux64.p;
+        cudaError_t e = cpu ? launch_binaux_cpusem(p.m, ctx->d_aux64.p, dcurves, ncur, j.n_mag,
+                                                   p.mag_bin_size, cfg.block, cfg.cnt16, s)
+                            : launch_binaux_cudasem(p.m, ctx->d_aux64.p, dcurves, ncur,
+                                                    j.n_mag, p.mag_bin_size, cfg.block,
+                                                    cfg.cnt16, s);
+        PF_CUDA(e, "CE bin preparation kernel");
+        ctx->launches++;
+    } else if (cfg.kind == KIND_BIN && j.algo == ALGO_AOV) {
+        if ((rc = ensure_dev(ctx, ctx->d_aux32, L.total_pts * 4 + 16)) != PF_OK) return rc;
+        p.aux32 = (const uint32_t*)ctx->d_aux32.p;
+        PF_CUDA(launch_aov_fix32_prep(p.m, (uint32_t*)ctx->d_aux32.p, dcurves, ncur, s),
+                "AOV fixed-point preparation kernel");
+        ctx->launches++;
+    } else if (j.algo == ALGO_CE) {
         if ((rc = ensure_dev(ctx, ctx->d_aux32, L.total_pts * 4 + 16)) != PF_OK) return rc;
         p.aux32 = (const uint32_t*)ctx->d_aux32.p;
         const int flag_sat = j.mo > 1 ? 1 : 0;
@@ -428,12 +474,6 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
     Layout L;
     FoldConfig cfg;
     if ((rc = plan(ctx, j, lengths, true, true, L, cfg)) != PF_OK) return rc;
-    if (cfg.fold == FOLD_DF) {
-        for (uint64_t d = 0; d < j.n_pdt; d++)
-            if (j.pdts[d] != 0.0f)
-                return fail(ctx, PF_EUNSUPPORTED,
-                            "the FP32 split-precision fold needs period_dt == 0");
-    }
     if ((rc = staging_ready(ctx)) != PF_OK) return rc;
     if ((rc = ensure_pinned(ctx, ctx->h_in, L.bytes)) != PF_OK) return rc;
     if ((rc = ensure_dev(ctx, ctx->d_in, L.bytes)) != PF_OK) return rc;
@@ -509,8 +549,6 @@ int run_dev(pf_ctx* ctx, const Job& j, const float* d_times, const float* d_mags
     if (rc != PF_OK) return rc;
     if (j.n_curves == 0) return PF_OK;
     if (!offsets) return fail(ctx, PF_EINVAL, "offsets is NULL");
-    if (j.mode & (PF_FOLD_DF | PF_FOLD_F32))
-        return fail(ctx, PF_EUNSUPPORTED, "fold study modes take host inputs");
     const uint64_t n_cells = j.n_per * j.n_pdt;
     if (n_cells == 0) return PF_OK;
     std::vector<uint64_t> lengths(j.n_curves);
@@ -567,6 +605,7 @@ int run_dev(pf_ctx* ctx, const Job& j, const float* d_times, const float* d_mags
 }  // namespace
 
 size_t pfk::fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag) {
+    if (c.kind == KIND_BIN) return bin_smem_bytes(c.algo, c.cnt16, c.block, n_phase, n_mag);
     return fold_smem_bytes(c.algo, c.fold, c.acc, c.block, c.ovl, n_phase, n_mag);
 }
 
@@ -624,7 +663,7 @@ void pf_ctx_destroy(pf_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->done_recorded) cudaEventSynchronize(ctx->ev_done);
     for (DevBuf* b : {&ctx->d_in, &ctx->d_aux32, &ctx->d_aux64, &ctx->d_out, &ctx->d_pidx,
-                      &ctx->d_pval, &ctx->d_pack})
+                      &ctx->d_pval, &ctx->d_pack, &ctx->d_misc})
         if (b->p) cudaFree(b->p);
     if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -821,6 +860,22 @@ int pf_ls_dev(pf_ctx* ctx, const float* d_times, const float* d_mags, const int6
     j.n_pdt = n_pdt;
     j.out = d_out;
     return run_dev(ctx, j, d_times, d_mags, offsets, stream);
+}
+
+int pf_find_peaks_dev(pf_ctx* ctx, const float* d_data, uint64_t n_curves, uint64_t flat_len,
+                      uint32_t n_peaks, uint32_t min_distance, int use_max, int64_t* d_out_idx,
+                      float* d_out_val, void* stream) {
+    if (!ctx) return PF_EINVAL;
+    if (n_curves == 0 || n_peaks == 0) return PF_OK;
+    if (!d_data || !d_out_idx || !d_out_val) return fail(ctx, PF_EINVAL, "NULL argument");
+    if (n_curves > 0x7FFFFFFFull) return fail(ctx, PF_EINVAL, "too many curves");
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    PF_CUDA(launch_peaks(d_data, n_curves, flat_len, n_peaks, min_distance, use_max, d_out_idx,
+                         d_out_val, s),
+            "peak kernel launch");
+    ctx->launches++;
+    return PF_OK;
 }
 
 int pf_find_peaks(pf_ctx* ctx, const float* data, uint64_t n_curves, uint64_t flat_len,

@@ -1,0 +1,274 @@
+// pf_bin.cuh -- the chosen form's fused fold+bin kernel for CE and AOV.
+//
+// Included by the two semantics units after pf_fold.cuh (same namespace).
+//
+// Per (point, trial period) the reference computes
+//     q = RN(t_corr / P)                  (FP64 divide)
+//     folded = (float)(q - floor(q))      (FP64 floor, f64->f32 convert)
+//     bin = (size_t)(folded / bin_size)   (f32 divide)
+// which on B200 puts three instructions per evaluation on the narrow XU
+// pipe (floor, conversion, the divide's reciprocal), ~16 ops/clk/SM.
+// Here the bin comes from the FP64 and integer pipes only:
+//     q = RN(t_corr / P)                  exact, divide-free (fold_exact)
+//     r = RD(q + 1.5*2^52)                low word = floor(q)
+//     y = RD(q * n*2^20 + 1.5*2^52)       mantissa = 2^51 + floor(q*n*2^20)
+//     row = (y >> 20) - n*floor(q)        = floor(frac(q) * n)   (mod 2^32)
+// The 20 low bits of y are frac(q)*n's fractional bits.  The reference's
+// float rounding and f32 divide move its quotient by less than a bound
+// delta(n) (computed on the host); when frac(q)*n lies within that bound of
+// an integer the evaluation recomputes the reference's exact sequence, so
+// bin occupancies are identical by construction (about 2.5e-5 of
+// evaluations take that branch at n = 10).
+//
+// Valid while |q| * n < 2^30 (checked per CTA from the batch's max|t|;
+// otherwise the CTA runs the generic loop).
+//
+// CE counters are 16-bit halves of 32-bit words when every count fits
+// (curve length * overlaps < 65536), doubling the CTAs per SM; AOV keeps a
+// 32-bit count and a 32-bit fixed-point magnitude sum per bin.  Updates are
+// `red.shared.add.u32` (no return value, no dependency chain).
+#pragma once
+
+namespace pfk {
+namespace PF_KNS {
+
+__device__ __forceinline__ void red_shared_u32(uint32_t addr, uint32_t v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
+}
+
+constexpr double kMagic15 = 6755399441055744.0;  // 1.5 * 2^52
+
+template <int ALGO, bool CNT16, int BLOCK>
+struct BinLayout {
+    // Tile of points: double t[kBinTile]; aux[kBinTile] (uint2 for CE, u32 for AOV).
+    static constexpr uint32_t kAuxBytes = (ALGO == ALGO_CE) ? 8 : 4;
+};
+
+// One CTA: curve w.curve, period derivative w.pdt, periods p0 .. p0+np-1
+// (one per thread).  Shared memory: [tile t (double)][tile aux][counters].
+template <int ALGO, bool CNT16, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr uint32_t kAuxBytes = BinLayout<ALGO, CNT16, BLOCK>::kAuxBytes;
+    double* tile_t = reinterpret_cast<double*>(smem);
+    unsigned char* tile_aux = smem + kBinTile * 8;
+    unsigned char* cnt_raw = tile_aux + kBinTile * kAuxBytes;
+    const uint32_t cnt_base = (uint32_t)__cvta_generic_to_shared(cnt_raw);
+
+    const WorkItem w = p.work[blockIdx.x];
+    const CurveDesc cd = p.curves[w.curve];
+    const uint32_t n = cd.n;
+    const int tid = threadIdx.x;
+    const bool active = (uint32_t)tid < w.np;
+    const uint32_t pi = w.p0 + (active ? (uint32_t)tid : 0u);
+    const float period_dt = p.pdts[w.pdt];
+    const uint32_t nP = p.n_phase, nM = p.n_mag;
+
+    Cell s;
+    cell_setup<FOLD_EXACT>(s, p.periods[pi], period_dt);
+
+    // Counter layout: CE  [nP + 1 rows][W words][BLOCK] u32, W = nM or ceil(nM/2)
+    //                 AOV [2][nP + 1][BLOCK] u32 (count, fixed-point sum)
+    const uint32_t W = (ALGO == ALGO_CE) ? (CNT16 ? (nM + 1) / 2 : nM) : 1;
+    const uint32_t row_stride = W * BLOCK * 4;  // bytes per phase row
+    const uint32_t slots = (ALGO == ALGO_CE) ? (nP + 1) * W : 2 * (nP + 1);
+    for (uint32_t k = 0; k < slots; k++)
+        reinterpret_cast<uint32_t*>(cnt_raw)[k * BLOCK + tid] = 0u;
+    const uint32_t tbase = cnt_base + tid * 4;
+    const uint32_t sum_off = (nP + 1) * BLOCK * 4;  // AOV: sums after counts
+
+    // Range guard for y = q * n * 2^20 (uniform over the CTA).  Non-finite
+    // periods or derivatives (device-pointer callers are not checked on the
+    // host) also take the generic loop, whose bins are always clamped.
+    const double qb = cta_qbound<BLOCK>(p, pi, period_dt);
+    const bool fin = isfinite(s.yhi) && isfinite(s.ylo) && isfinite(s.c);
+    const bool fast = __syncthreads_and(fin ? 1 : 0) && qb * (double)nP < 1073741824.0;  // 2^30
+
+    const double nd20 = (double)nP * 1048576.0;
+    const uint32_t n_neg = 0u - nP;
+    const uint32_t edge_d = p.edge_d;
+
+    for (uint32_t base = 0; base < n; base += kBinTile) {
+        const uint32_t cnt = min(kBinTile, n - base);
+        __syncthreads();
+        {
+            const float4* gt = reinterpret_cast<const float4*>(p.t + cd.off + base);
+            const uint32_t n4 = (cnt + 3) >> 2;
+            for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
+                const float4 q = gt[i4];
+                tile_t[4 * i4 + 0] = (double)q.x;
+                tile_t[4 * i4 + 1] = (double)q.y;
+                tile_t[4 * i4 + 2] = (double)q.z;
+                tile_t[4 * i4 + 3] = (double)q.w;
+            }
+            if constexpr (ALGO == ALGO_CE) {
+                const uint4* ga = reinterpret_cast<const uint4*>(p.aux64 + cd.off + base);
+                uint4* sa = reinterpret_cast<uint4*>(tile_aux);
+                for (uint32_t i2 = tid; i2 < 2 * n4; i2 += BLOCK) sa[i2] = ga[i2];
+            } else {
+                const uint4* ga = reinterpret_cast<const uint4*>(p.aux32 + cd.off + base);
+                uint4* sa = reinterpret_cast<uint4*>(tile_aux);
+                for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) sa[i4] = ga[i4];
+            }
+        }
+        __syncthreads();
+        if (!active) continue;
+
+        auto body = [&](auto has_pdt_tag, auto fast_tag) {
+            constexpr bool HAS_PDT = decltype(has_pdt_tag)::value;
+            constexpr bool FAST = decltype(fast_tag)::value;
+#pragma unroll 4
+            for (uint32_t i = 0; i < cnt; i++) {
+                const double td = tile_t[i];
+                double a;
+                if constexpr (HAS_PDT) {
+                    a = td - s.c * td * td;  // reference expression and contraction
+                } else {
+                    a = td;
+                }
+                const double qh = __dmul_rn(a, s.yhi);
+                const double e = __fma_rn(a, s.yhi, -qh);
+                const double lo = __fma_rn(a, s.ylo, e);
+                const double q = __dadd_rn(qh, lo);
+                uint32_t row;  // phase bin + 2^31 (the bias vanishes in addresses)
+                if constexpr (FAST) {
+                    const double r = __dadd_rd(q, kMagic15);
+                    const double y = __fma_rd(q, nd20, kMagic15);
+                    const uint32_t ylo = (uint32_t)__double2loint(y);
+                    const uint32_t yhi = (uint32_t)__double2hiint(y);
+                    row = __funnelshift_r(ylo, yhi, 20) + (uint32_t)__double2loint(r) * n_neg;
+                    if (((ylo + edge_d) & 0xFFFFFu) < 2u * edge_d) {
+                        // Near a bin edge: the reference's exact sequence.
+                        const float folded = fabsf((float)(q - floor(q)));
+                        row = 0x80000000u + min(trunc_u(folded / p.phase_bin_size), nP);
+                    }
+                } else {
+                    const float folded = fabsf((float)(q - floor(q)));
+                    row = 0x80000000u + min(trunc_u(folded / p.phase_bin_size), nP);
+                }
+                if constexpr (ALGO == ALGO_CE) {
+                    const uint2 ax = reinterpret_cast<const uint2*>(tile_aux)[i];
+                    red_shared_u32(row * row_stride + ax.x + tbase, ax.y);
+                } else {
+                    const uint32_t qv = reinterpret_cast<const uint32_t*>(tile_aux)[i];
+                    const uint32_t a0 = row * (BLOCK * 4) + tbase;
+                    red_shared_u32(a0, 1u);
+                    red_shared_u32(a0 + sum_off, qv);
+                }
+            }
+        };
+        if (period_dt != 0.0f) {
+            if (fast) body(std::true_type{}, std::true_type{});
+            else body(std::true_type{}, std::false_type{});
+        } else {
+            if (fast) body(std::false_type{}, std::true_type{});
+            else body(std::false_type{}, std::false_type{});
+        }
+    }
+
+    if (!active) return;
+    __syncwarp();
+    const size_t out_idx =
+        (size_t)w.curve * ((size_t)p.n_per * p.n_pdt) + (size_t)pi * p.n_pdt + w.pdt;
+    uint32_t* cnt32 = reinterpret_cast<uint32_t*>(cnt_raw);
+
+    if constexpr (ALGO == ALGO_CE) {
+        auto count = [&](uint32_t j, uint32_t i) -> uint32_t {
+            // Row nP (folded == 1.0 in the reference) wraps to row 0.
+            auto get = [&](uint32_t jj) -> uint32_t {
+                if constexpr (CNT16) {
+                    const uint32_t wv = cnt32[(jj * W + (i >> 1)) * BLOCK + tid];
+                    return (i & 1u) ? (wv >> 16) : (wv & 0xFFFFu);
+                } else {
+                    return cnt32[(jj * W + i) * BLOCK + tid];
+                }
+            };
+            return j == 0 ? get(0) + get(nP) : get(j);
+        };
+        const float divf = (float)((unsigned long long)n * p.p_overlap * p.m_overlap);
+        float ce = 0.0f;
+        for (uint32_t j = 0; j < nP; j++) {
+            float p_j = 0.0f;
+            for (uint32_t i = 0; i < nM; i++) p_j += (float)count(j, i) / divf;
+#if PF_SEM_CPU_TU
+            for (uint32_t i = 0; i < nM; i++) {
+                const float p_ij = (float)count(j, i) / divf;
+                if (p_ij != 0.0f) ce += p_ij * logf(p_j / p_ij);
+            }
+#else
+            float ce_contrib = 0.0f;
+            for (uint32_t i = 0; i < nM; i++) {
+                const float p_ij = (float)count(j, i) / divf;
+                if (p_ij != 0) ce_contrib += p_ij * logf(p_j / p_ij);
+            }
+            ce += ce_contrib;
+#endif
+        }
+        p.out[out_idx] = ce;
+    } else {
+        const uint32_t* sums = cnt32 + (nP + 1) * BLOCK;
+        const double xbar = cd.fix_sumx / (double)n;
+        double s1 = 0.0, sbx = 0.0;
+        for (uint32_t b = 0; b < nP; b++) {
+            uint32_t c = cnt32[b * BLOCK + tid];
+            uint32_t X = sums[b * BLOCK + tid];
+            if (b == 0) {
+                c += cnt32[nP * BLOCK + tid];
+                X += sums[nP * BLOCK + tid];
+            }
+            if (c != 0u) {
+                const double nb = (double)c;
+                const double Xd = (double)X;
+                const double mu = Xd / nb;
+                const double r = mu - xbar;
+                s1 = __fma_rn(nb * r, r, s1);
+                sbx = __fma_rn(Xd, mu, sbx);
+            }
+        }
+        const double s2 = __dadd_rn(cd.fix_sumx2, -sbx);
+        const double scale = ((double)n - (double)nP) / ((double)nP - 1.0);
+#if PF_SEM_CPU_TU
+        p.out[out_idx] = (s2 <= 0.0) ? 0.0f : (float)(scale * (s1 / s2));
+#else
+        p.out[out_idx] = (float)(scale * (s1 / (s2 <= 0.0 ? 0.0 : s2)));
+#endif
+    }
+}
+
+// CE per-point bin data for bin_kernel: {byte offset of the magnitude
+// column within a phase row (without the thread term), increment}.
+__global__ void ce_binaux_kernel(const float* __restrict__ m, uint2* __restrict__ aux,
+                                 const CurveDesc* __restrict__ curves, uint32_t n_curves,
+                                 uint32_t n_mag, float mag_bin_size, int block, int cnt16) {
+    const uint32_t c = blockIdx.x;
+    if (c >= n_curves) return;
+    const CurveDesc cd = curves[c];
+    const uint32_t n4 = (cd.n + 3u) & ~3u;
+    for (uint32_t i = threadIdx.x; i < n4; i += blockDim.x) {
+        uint2 v = make_uint2(0u, 0u);
+        if (i < cd.n) {
+            const float mag_val = m[cd.off + i];
+            // MagBin (periodfind/cuda/ce.cu:70-72; rust/src/ce.rs:79).
+            const unsigned long long mb64 =
+                static_cast<unsigned long long>(mag_val / mag_bin_size);
+            const uint32_t mb = (uint32_t)(mb64 % n_mag);
+            if (cnt16) {
+                v.x = (mb >> 1) * (uint32_t)block * 4u;
+                v.y = (mb & 1u) ? 0x10000u : 1u;
+            } else {
+                v.x = mb * (uint32_t)block * 4u;
+                v.y = 1u;
+            }
+        }
+        aux[cd.off + i] = v;
+    }
+}
+
+}  // namespace PF_KNS
+}  // namespace pfk

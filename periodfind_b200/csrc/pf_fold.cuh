@@ -50,7 +50,7 @@ constexpr float kTwoPi = 6.283185307179586f;
 struct Cell {
     float period, pdt_corr;
     double Pd, yhi, ylo, c;
-    float fhi, flo;
+    float fhi, flo, ghi, glo;
 };
 
 template <int FOLD>
@@ -68,9 +68,12 @@ __device__ __forceinline__ void cell_setup(Cell& s, float period, float period_d
         s.c = (double)s.pdt_corr;
     }
     if (FOLD == FOLD_DF) {
-        // f = 1/P as an unevaluated float pair for the FP32 phase.
+        // f = 1/P and g = pdt_corr / P as unevaluated float pairs.
         s.fhi = __double2float_rn(s.yhi);
         s.flo = __double2float_rn(__dadd_rn(__dadd_rn(s.yhi, -(double)s.fhi), s.ylo));
+        const double g = __dmul_rn(s.c, s.yhi);
+        s.ghi = __double2float_rn(g);
+        s.glo = __double2float_rn(__dadd_rn(g, -(double)s.ghi));
     }
 }
 
@@ -111,14 +114,50 @@ __device__ __forceinline__ float fold_f32(float t, const Cell& s) {
     return fabsf(r - floorf(r));
 }
 
-// Split-precision FP32 phase frac(t * f), f = fhi + flo; result in turns in
-// [-0.5, 0.5] (pdt == 0 only; |t * fhi| < 2^22 checked on the host).
+// Split-precision FP32 phase of t_corr / P = t*f - t^2*g (f = 1/P,
+// g = pdt_corr / P as float pairs).  Each product is carried as a rounded
+// float plus its exact rounding error (fma), the integer part is removed
+// from the rounded float (exact for |x| < 2^22, checked per CTA), and the
+// small terms are added last: phase error ~1e-10 cycles at 6e4 cycles of
+// baseline.  Result in turns, within [-1, 1].
+__device__ __forceinline__ float rint_small(float x) {
+    return __fsub_rn(__fadd_rn(x, 12582912.0f), 12582912.0f);  // |x| < 2^22
+}
+
+template <bool HAS_PDT>
 __device__ __forceinline__ float fold_df(float t, const Cell& s) {
     const float p = __fmul_rn(t, s.fhi);
-    const float e = __fmaf_rn(t, s.fhi, -p);
-    const float e2 = __fmaf_rn(t, s.flo, e);
-    const float k = __fsub_rn(__fadd_rn(p, 12582912.0f), 12582912.0f);
-    return __fadd_rn(__fsub_rn(p, k), e2);
+    float e = __fmaf_rn(t, s.fhi, -p);
+    e = __fmaf_rn(t, s.flo, e);
+    float ph = __fsub_rn(p, rint_small(p));
+    if constexpr (HAS_PDT) {
+        const float t2 = __fmul_rn(t, t);
+        const float t2e = __fmaf_rn(t, t, -t2);
+        const float p2 = __fmul_rn(t2, s.ghi);
+        float e2 = __fmaf_rn(t2, s.ghi, -p2);
+        e2 = __fmaf_rn(t2, s.glo, e2);
+        e2 = __fmaf_rn(t2e, s.ghi, e2);
+        ph = __fsub_rn(ph, __fsub_rn(p2, rint_small(p2)));
+        e = __fsub_rn(e, e2);
+    }
+    return __fadd_rn(ph, e);
+}
+
+// Bound on |t_corr / P| over this CTA's cells: max|t| / min|P| +
+// |pdt| max|t|^2 / (2 min|P|^2).  All threads of the CTA must call it.
+template <int BLOCK>
+__device__ double cta_qbound(const FoldParams& p, uint32_t pi, float period_dt) {
+    __shared__ double warp_min[BLOCK / 32];
+    double mn = fabs((double)p.periods[pi]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    if ((threadIdx.x & 31) == 0) warp_min[threadIdx.x >> 5] = mn;
+    __syncthreads();
+    double pmin = warp_min[0];
+#pragma unroll
+    for (int k = 1; k < BLOCK / 32; k++) pmin = fmin(pmin, warp_min[k]);
+    const double tmax = (double)__uint_as_float(*p.tmax_bits);
+    return tmax / pmin + fabs((double)period_dt) * tmax * tmax / (2.0 * pmin * pmin);
 }
 
 // trunc(q) for finite q in [0, 2^23): identical to the reference's
@@ -148,7 +187,7 @@ struct LSAcc {
 };
 
 // Stream the curve through shared memory and accumulate this thread's cell.
-template <int ALGO, int FOLD, int ACC, int BLOCK, bool OVL, bool HAS_PDT>
+template <int ALGO, int FOLD, int ACC, int BLOCK, bool OVL, bool HAS_PDT, bool ALT>
 __device__ __forceinline__ void accumulate(const FoldParams& p, const Views& v, const Cell& s,
                                            int64_t off, uint32_t n, bool active, LSAcc& ls) {
     using TT = tile_t_type<FOLD>;
@@ -200,8 +239,11 @@ __device__ __forceinline__ void accumulate(const FoldParams& p, const Views& v, 
                 folded = fold_exact<HAS_PDT>(tile_t[i], s);
             } else if constexpr (FOLD == FOLD_F32) {
                 folded = fold_f32(tile_t[i], s);
+            } else if constexpr (ALT) {
+                // Outside the split-precision range: the exact fold.
+                folded = fold_exact<HAS_PDT>((double)tile_t[i], s);
             } else {
-                folded = fold_df(tile_t[i], s);
+                folded = fold_df<HAS_PDT>(tile_t[i], s);
             }
 
             if constexpr (ALGO == ALGO_LS) {
@@ -320,11 +362,17 @@ __global__ void __launch_bounds__(BLOCK) fold_kernel(const FoldParams p) {
     }
 
     LSAcc ls{0.0f, 0.0f, 0.0f, 0.0f};
+    // The split-precision fold needs |t_corr / P| < 2^21 (uniform per CTA).
+    bool alt = false;
+    if constexpr (FOLD == FOLD_DF) alt = !(cta_qbound<BLOCK>(p, pi, period_dt) < 2097152.0);
     // The period derivative is uniform over the CTA: pick the loop once.
-    if (period_dt != 0.0f)
-        accumulate<ALGO, FOLD, ACC, BLOCK, OVL, true>(p, v, s, cd.off, n, active, ls);
-    else
-        accumulate<ALGO, FOLD, ACC, BLOCK, OVL, false>(p, v, s, cd.off, n, active, ls);
+    if (period_dt != 0.0f) {
+        if (alt) accumulate<ALGO, FOLD, ACC, BLOCK, OVL, true, true>(p, v, s, cd.off, n, active, ls);
+        else accumulate<ALGO, FOLD, ACC, BLOCK, OVL, true, false>(p, v, s, cd.off, n, active, ls);
+    } else {
+        if (alt) accumulate<ALGO, FOLD, ACC, BLOCK, OVL, false, true>(p, v, s, cd.off, n, active, ls);
+        else accumulate<ALGO, FOLD, ACC, BLOCK, OVL, false, false>(p, v, s, cd.off, n, active, ls);
+    }
 
     if (!active) return;
     const size_t out_idx =

@@ -8,7 +8,11 @@
 
 namespace pfk {
 
+enum : int { KIND_FOLD = 0, KIND_BIN = 1 };
+
 struct FoldConfig {
+    int kind;   // KIND_FOLD: fold_kernel; KIND_BIN: the chosen CE/AOV bin_kernel
+    bool cnt16; // bin_kernel CE: 16-bit counters
     int algo;   // ALGO_*
     int fold;   // FOLD_*
     int acc;    // AOVACC_* (AOV only)
@@ -31,7 +35,19 @@ cudaError_t launch_magbin_cpusem(const float* m, uint32_t* aux, const CurveDesc*
                                  uint32_t n_curves, uint32_t n_mag, float mag_bin_size,
                                  int flag_saturated, cudaStream_t stream);
 
+cudaError_t launch_binaux_cudasem(const float* m, void* aux, const CurveDesc* curves,
+                                  uint32_t n_curves, uint32_t n_mag, float mag_bin_size,
+                                  int block, int cnt16, cudaStream_t s);
+cudaError_t launch_binaux_cpusem(const float* m, void* aux, const CurveDesc* curves,
+                                 uint32_t n_curves, uint32_t n_mag, float mag_bin_size,
+                                 int block, int cnt16, cudaStream_t s);
+
 // Preparation kernels (pf_prep.cu).
+// max |t| over n packed points into *tmax_bits (float bits; zeroed first).
+cudaError_t launch_tmax(const float* t, size_t n, unsigned* tmax_bits, cudaStream_t stream);
+// AOV bin kernel: 32-bit fixed-point magnitudes (k bits) and per-curve sums.
+cudaError_t launch_aov_fix32_prep(const float* m, uint32_t* aux32, CurveDesc* curves,
+                                  uint32_t n_curves, cudaStream_t stream);
 cudaError_t launch_aov_mean(const float* m, CurveDesc* curves, uint32_t n_curves,
                             cudaStream_t stream);
 cudaError_t launch_aov_fix_prep(const float* m, uint64_t* aux64, CurveDesc* curves,

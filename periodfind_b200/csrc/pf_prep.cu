@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "pf_launch.h"
 #include "pf_types.h"
 
@@ -124,7 +126,80 @@ __global__ void __launch_bounds__(kPrepThreads)
     }
 }
 
+// max |t| over the packed batch (padding is zero).  |t| as float bits is
+// monotone in the value, so an unsigned max is a float max.
+__global__ void tmax_kernel(const float* __restrict__ t, size_t n, unsigned* __restrict__ out) {
+    unsigned mx = 0u;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        mx = max(mx, __float_as_uint(fabsf(t[i])));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
+}
+
+// 32-bit fixed-point magnitudes for the bin kernel: k = min(24, 32 -
+// ceil(log2(n + 1))) bits so a bin's sum of up to n values fits in 32 bits.
+__global__ void __launch_bounds__(kPrepThreads)
+    aov_fix32_kernel(const float* __restrict__ m, uint32_t* __restrict__ aux32,
+                     CurveDesc* __restrict__ curves, uint32_t n_curves) {
+    __shared__ double dscr[kPrepThreads];
+    __shared__ float fscr[kPrepThreads];
+    __shared__ unsigned long long uscr[kPrepThreads];
+    const uint32_t c = blockIdx.x;
+    if (c >= n_curves) return;
+    const CurveDesc cd = curves[c];
+    const float* mc = m + cd.off;
+    float mn = __int_as_float(0x7f800000), mx = -__int_as_float(0x7f800000);
+    for (uint32_t i = threadIdx.x; i < cd.n; i += kPrepThreads) {
+        mn = fminf(mn, mc[i]);
+        mx = fmaxf(mx, mc[i]);
+    }
+    mn = block_reduce(mn, fscr, [](float a, float b) { return fminf(a, b); });
+    mx = block_reduce(mx, fscr, [](float a, float b) { return fmaxf(a, b); });
+    const unsigned long long tot = (unsigned long long)cd.n + 1ull;
+    const int need = 64 - __clzll(tot - 1ull);
+    const int kbits = min(24, 32 - need);
+    const double span = (double)mx - (double)mn;
+    const double scale = (span > 0.0 && kbits > 0) ? (double)((1u << kbits) - 1u) / span : 0.0;
+    unsigned long long sx = 0ull;
+    double sx2 = 0.0;
+    const uint32_t n4 = (cd.n + 3u) & ~3u;
+    for (uint32_t i = threadIdx.x; i < n4; i += kPrepThreads) {
+        uint32_t v = 0u;
+        if (i < cd.n) {
+            v = (uint32_t)rint(((double)mc[i] - (double)mn) * scale);
+            sx += v;
+            sx2 = __fma_rn((double)v, (double)v, sx2);
+        }
+        aux32[cd.off + i] = v;
+    }
+    sx = block_reduce(sx, uscr, [](unsigned long long a, unsigned long long b) { return a + b; });
+    sx2 = block_reduce(sx2, dscr, [](double a, double b) { return a + b; });
+    if (threadIdx.x == 0) {
+        curves[c].fix_mn = (double)mn;
+        curves[c].fix_scale = scale;
+        curves[c].fix_sumx = (double)sx;
+        curves[c].fix_sumx2 = sx2;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_tmax(const float* t, size_t n, unsigned* tmax_bits, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(tmax_bits, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess || n == 0) return e;
+    const int blocks = (int)std::min<size_t>((n + 255) / 256, 1184);
+    tmax_kernel<<<blocks, 256, 0, stream>>>(t, n, tmax_bits);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_aov_fix32_prep(const float* m, uint32_t* aux32, CurveDesc* curves,
+                                  uint32_t n_curves, cudaStream_t stream) {
+    if (n_curves == 0) return cudaSuccess;
+    aov_fix32_kernel<<<n_curves, kPrepThreads, 0, stream>>>(m, aux32, curves, n_curves);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_pack(const float* src_t, const float* src_m, const int64_t* src_off,
                         const CurveDesc* curves, uint32_t n_curves, float* dst_t, float* dst_m,

@@ -22,7 +22,8 @@ enum : int { AOVACC_F32 = 0, AOVACC_FIX = 1 };
 
 constexpr int kFixCountShift = 44;
 
-constexpr uint32_t kTile = 1024;  // points staged per tile (multiple of 4)
+constexpr uint32_t kTile = 1024;     // points staged per tile (multiple of 4)
+constexpr uint32_t kBinTile = 1024;  // points per tile in the chosen bin kernel
 
 // One light curve in the packed arrays.  Curves start on 16-byte
 // boundaries (offsets are multiples of 4 points).
@@ -59,7 +60,23 @@ struct FoldParams {
     uint32_t n_per, n_pdt;
     uint32_t n_phase, n_mag, p_overlap, m_overlap;
     float phase_bin_size, mag_bin_size;
+    const unsigned* tmax_bits;  // float bits of max |t| over the batch
+    uint32_t edge_d;            // bin-edge guard (units of 2^-20 of a bin)
 };
+
+// Shared-memory bytes of the chosen bin kernel (pf_bin.cuh).
+inline size_t bin_smem_bytes(int algo, bool cnt16, int block, uint32_t n_phase,
+                             uint32_t n_mag) {
+    const size_t aux = (algo == ALGO_CE) ? 8 : 4;
+    size_t bytes = (size_t)kBinTile * (8 + aux);
+    if (algo == ALGO_CE) {
+        const size_t w = cnt16 ? (n_mag + 1) / 2 : n_mag;
+        bytes += (size_t)(n_phase + 1) * w * block * 4;
+    } else {
+        bytes += (size_t)2 * (n_phase + 1) * block * 4;
+    }
+    return bytes;
+}
 
 // Shared-memory bytes for one CTA (host and device agree through this).
 inline size_t fold_smem_bytes(int algo, int fold, int acc, int block,

@@ -38,7 +38,9 @@ def _mode_flags(mode: str, semantics: str, fold: str | None = None) -> int:
         f |= nat.PF_FOLD_DF
     elif fold == "f32":
         f |= nat.PF_FOLD_F32
-    elif fold not in (None, "exact", "ref"):
+    elif fold == "exact":
+        f |= nat.PF_FOLD_EXACT
+    elif fold not in (None, "ref"):
         raise ValueError(f"unknown fold {fold!r}")
     return f
 
@@ -211,7 +213,8 @@ class LombScargle(_Periodogram):
     """Lomb-Scargle periodogram (maximum is best; magnitudes centred by
     default) (periodfind/ls.pyx:37-62).
 
-    fold='df' selects the split-precision FP32 phase (period_dt == 0 only);
+    The chosen form folds with a split-precision FP32 phase; fold='exact'
+    selects the divide-free exact fold (bit-identical to the plain form),
     fold='f32' the all-FP32 fold (precision studies).
     """
 
