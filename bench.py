@@ -433,9 +433,10 @@ def main():
         dist.destroy_process_group()
 
 
-# FP64-pipe operations per evaluation in the chosen CE fold: the exact
-# quotient (DMUL, 2 DFMA, DADD).  Updated with the kernel.
-FP64_OPS_PER_EVAL = 4
+# FP64-pipe operations per evaluation in the chosen CE fold (bin_kernel):
+# exact quotient (DMUL, 2 DFMA, DADD), floor (DADD.RD), bin (DFMA.RD), plus
+# DMUL + DFMA for t - c t^2 on the period-derivative cells (half the grid).
+FP64_OPS_PER_EVAL = 6 + 2 * sum(1 for d in PDTS if d != 0.0) / len(PDTS)
 
 if __name__ == "__main__":
     main()

@@ -139,7 +139,7 @@ int pf_find_peaks(pf_ctx* ctx, const float* data, uint64_t n_curves,
 /* ------------------------------------------------ device-resident callers */
 
 /* Same computations on device memory, enqueued on `stream` (a cudaStream_t;
- * NULL = the context stream).  Curves are packed: curve c occupies
+ * NULL = the CUDA default stream).  Curves are packed: curve c occupies
  * [offsets[c], offsets[c+1]) of d_times / d_mags; `offsets` is a HOST array
  * of n_curves + 1 entries (it drives the launch decomposition).  d_out is a
  * device array of n_curves * n_per * n_pdt floats.  The call returns once

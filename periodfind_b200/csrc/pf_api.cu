@@ -560,7 +560,8 @@ int run_dev(pf_ctx* ctx, const Job& j, const float* d_times, const float* d_mags
     if (offsets[j.n_curves] > 0 && (!d_times || !d_mags))
         return fail(ctx, PF_EINVAL, "d_times/d_mags is NULL");
     PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
-    cudaStream_t s = stream_v ? (cudaStream_t)stream_v : ctx->stream;
+    // NULL is the CUDA default stream, as for any CUDA API taking a stream.
+    cudaStream_t s = (cudaStream_t)stream_v;
 
     Layout L;
     FoldConfig cfg;
@@ -870,7 +871,7 @@ int pf_find_peaks_dev(pf_ctx* ctx, const float* d_data, uint64_t n_curves, uint6
     if (!d_data || !d_out_idx || !d_out_val) return fail(ctx, PF_EINVAL, "NULL argument");
     if (n_curves > 0x7FFFFFFFull) return fail(ctx, PF_EINVAL, "too many curves");
     PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
-    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    cudaStream_t s = (cudaStream_t)stream;  // NULL: the CUDA default stream
     PF_CUDA(launch_peaks(d_data, n_curves, flat_len, n_peaks, min_distance, use_max, d_out_idx,
                          d_out_val, s),
             "peak kernel launch");

@@ -374,10 +374,18 @@ def test_device_pointer_entry_points(gpu):
     dd = torch.from_numpy(D).cuda()
     out = torch.empty((len(ts), len(P), len(D)), dtype=torch.float32, device="cuda")
     ctx = nat.default_context(0)
-    stream = torch.cuda.current_stream().cuda_stream
-    with ctx.lock:
-        ctx.check(ctx.lib.pf_ls_dev(ctx.handle, dt.data_ptr(), dm.data_ptr(), off.ctypes.data,
-                                    len(ts), dp.data_ptr(), len(P), dd.data_ptr(), len(D),
-                                    nat.PF_MODE_CHOSEN, out.data_ptr(), stream))
-    torch.cuda.synchronize()
-    np.testing.assert_array_equal(out.cpu().numpy(), host)
+    # The work must be ordered on the caller's stream: the default stream
+    # (handle 0) and a side stream, each synchronised on its own.
+    side = torch.cuda.Stream()
+    for st in (torch.cuda.default_stream(), side):
+        out.fill_(-1.0)
+        torch.cuda.synchronize()
+        with ctx.lock:
+            ctx.check(ctx.lib.pf_ls_dev(ctx.handle, dt.data_ptr(), dm.data_ptr(),
+                                        off.ctypes.data, len(ts), dp.data_ptr(), len(P),
+                                        dd.data_ptr(), len(D), nat.PF_MODE_CHOSEN,
+                                        out.data_ptr(), st.cuda_stream))
+        done = torch.cuda.Event()
+        done.record(st)
+        done.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy(), host)
