@@ -253,13 +253,16 @@ FoldConfig choose_config(pf_ctx* ctx, const Job& j, uint32_t max_len, bool& ok) 
 }
 
 // Bin-edge guard of the bin kernel, in units of 2^-20 of a phase bin: the
-// reference's quotient folded / bin_size differs from frac(q) * n by less
+// reference's quotient folded / bin_size differs from frac(q') * n by less
 // than 2 ulp (f32 divide) + n * 2^-23 (bin width rounding) + n * 2^-25
-// (f64 -> f32 rounding of the phase), plus two units of margin.
+// (f64 -> f32 rounding of the phase) + 2^-20 (q' = t * RN(1/P) against
+// RN(t / P): 2 ulp(q) * n <= 2^-20 while |q| * n < 2^30), plus two units of
+// margin.
 uint32_t edge_guard(uint32_t n) {
     int cl = 0;
     while ((1u << cl) < n + 1u) cl++;
-    const double delta = ldexp(1.0, cl - 22) + n * ldexp(1.0, -23) + n * ldexp(1.0, -25);
+    const double delta =
+        ldexp(1.0, cl - 22) + n * ldexp(1.0, -23) + n * ldexp(1.0, -25) + ldexp(1.0, -20);
     return (uint32_t)ceil(delta * 1048576.0) + 2u;
 }
 

@@ -8,17 +8,19 @@
 //     bin = (size_t)(folded / bin_size)   (f32 divide)
 // which on B200 puts three instructions per evaluation on the narrow XU
 // pipe (floor, conversion, the divide's reciprocal), ~16 ops/clk/SM.
-// Here the bin comes from the FP64 and integer pipes only:
-//     q = RN(t_corr / P)                  exact, divide-free (fold_exact)
-//     r = RD(q + 1.5*2^52)                low word = floor(q)
-//     y = RD(q * n*2^20 + 1.5*2^52)       mantissa = 2^51 + floor(q*n*2^20)
-//     row = (y >> 20) - n*floor(q)        = floor(frac(q) * n)   (mod 2^32)
-// The 20 low bits of y are frac(q)*n's fractional bits.  The reference's
-// float rounding and f32 divide move its quotient by less than a bound
-// delta(n) (computed on the host); when frac(q)*n lies within that bound of
-// an integer the evaluation recomputes the reference's exact sequence, so
-// bin occupancies are identical by construction (about 2.5e-5 of
-// evaluations take that branch at n = 10).
+// Here the bin comes from three FP64 operations and integer arithmetic:
+//     q' = t_corr * RN(1/P)               within 2 ulp of RN(t_corr / P)
+//     r  = RD(q' + 1.5*2^52)              low word = floor(q')
+//     y  = RD(q' * n*2^20 + 1.5*2^52)     mantissa = 2^51 + floor(q'*n*2^20)
+//     row = (y >> 20) - n*floor(q')       = floor(frac(q') * n)  (mod 2^32)
+// The 20 low bits of y are frac(q')*n's fractional bits.  The reference's
+// quotient folded / bin_size differs from frac(q')*n by less than a bound
+// delta(n) (f32 divide, bin-width rounding, f64->f32 rounding of the phase,
+// and q' versus RN(t_corr/P); computed on the host).  When frac(q')*n lies
+// within that bound of an integer the evaluation recomputes the reference's
+// exact sequence (the correctly rounded quotient via fold_exact, then the
+// float fold and divide), so bin occupancies are identical by construction;
+// about 3e-5 of evaluations take that branch at n = 10.
 //
 // Valid while |q| * n < 2^30 (checked per CTA from the batch's max|t|;
 // otherwise the CTA runs the generic loop).
@@ -44,21 +46,21 @@ __device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
 
 constexpr double kMagic15 = 6755399441055744.0;  // 1.5 * 2^52
 
-template <int ALGO, bool CNT16, int BLOCK>
-struct BinLayout {
-    // Tile of points: double t[kBinTile]; aux[kBinTile] (uint2 for CE, u32 for AOV).
-    static constexpr uint32_t kAuxBytes = (ALGO == ALGO_CE) ? 8 : 4;
+// One CTA: curve w.curve, period derivative w.pdt, periods p0 .. p0+np-1
+// (one per thread).  Shared memory: [tile of 16-byte point records
+// {double t; u32 a; u32 b}][counters].  CE: a = byte offset of the
+// magnitude column within a phase row, b = increment (1 or 1 << 16).
+// AOV: a = fixed-point magnitude.
+struct BinPoint {
+    double t;
+    uint32_t a, b;
 };
 
-// One CTA: curve w.curve, period derivative w.pdt, periods p0 .. p0+np-1
-// (one per thread).  Shared memory: [tile t (double)][tile aux][counters].
 template <int ALGO, bool CNT16, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
-    constexpr uint32_t kAuxBytes = BinLayout<ALGO, CNT16, BLOCK>::kAuxBytes;
-    double* tile_t = reinterpret_cast<double*>(smem);
-    unsigned char* tile_aux = smem + kBinTile * 8;
-    unsigned char* cnt_raw = tile_aux + kBinTile * kAuxBytes;
+    BinPoint* tile = reinterpret_cast<BinPoint*>(smem);
+    unsigned char* cnt_raw = smem + kBinTile * sizeof(BinPoint);
     const uint32_t cnt_base = (uint32_t)__cvta_generic_to_shared(cnt_raw);
 
     const WorkItem w = p.work[blockIdx.x];
@@ -92,7 +94,10 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
 
     const double nd20 = (double)nP * 1048576.0;
     const uint32_t n_neg = 0u - nP;
-    const uint32_t edge_d = p.edge_d;
+    // Edge test: ((ylo + D) mod 2^20) < 2D, as one IMAD and one compare on
+    // the fraction bits moved to the top of the word.
+    const uint32_t edge_add = p.edge_d << 12;
+    const uint32_t edge_lim = (2u * p.edge_d) << 12;
 
     for (uint32_t base = 0; base < n; base += kBinTile) {
         const uint32_t cnt = min(kBinTile, n - base);
@@ -100,21 +105,26 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
         {
             const float4* gt = reinterpret_cast<const float4*>(p.t + cd.off + base);
             const uint32_t n4 = (cnt + 3) >> 2;
-            for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
-                const float4 q = gt[i4];
-                tile_t[4 * i4 + 0] = (double)q.x;
-                tile_t[4 * i4 + 1] = (double)q.y;
-                tile_t[4 * i4 + 2] = (double)q.z;
-                tile_t[4 * i4 + 3] = (double)q.w;
-            }
             if constexpr (ALGO == ALGO_CE) {
                 const uint4* ga = reinterpret_cast<const uint4*>(p.aux64 + cd.off + base);
-                uint4* sa = reinterpret_cast<uint4*>(tile_aux);
-                for (uint32_t i2 = tid; i2 < 2 * n4; i2 += BLOCK) sa[i2] = ga[i2];
+                for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
+                    const float4 q = gt[i4];
+                    const uint4 a01 = ga[2 * i4], a23 = ga[2 * i4 + 1];
+                    tile[4 * i4 + 0] = BinPoint{(double)q.x, a01.x, a01.y};
+                    tile[4 * i4 + 1] = BinPoint{(double)q.y, a01.z, a01.w};
+                    tile[4 * i4 + 2] = BinPoint{(double)q.z, a23.x, a23.y};
+                    tile[4 * i4 + 3] = BinPoint{(double)q.w, a23.z, a23.w};
+                }
             } else {
                 const uint4* ga = reinterpret_cast<const uint4*>(p.aux32 + cd.off + base);
-                uint4* sa = reinterpret_cast<uint4*>(tile_aux);
-                for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) sa[i4] = ga[i4];
+                for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
+                    const float4 q = gt[i4];
+                    const uint4 a = ga[i4];
+                    tile[4 * i4 + 0] = BinPoint{(double)q.x, a.x, 0u};
+                    tile[4 * i4 + 1] = BinPoint{(double)q.y, a.y, 0u};
+                    tile[4 * i4 + 2] = BinPoint{(double)q.z, a.z, 0u};
+                    tile[4 * i4 + 3] = BinPoint{(double)q.w, a.w, 0u};
+                }
             }
         }
         __syncthreads();
@@ -125,41 +135,38 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
             constexpr bool FAST = decltype(fast_tag)::value;
 #pragma unroll 4
             for (uint32_t i = 0; i < cnt; i++) {
-                const double td = tile_t[i];
-                double a;
-                if constexpr (HAS_PDT) {
-                    a = td - s.c * td * td;  // reference expression and contraction
-                } else {
-                    a = td;
-                }
-                const double qh = __dmul_rn(a, s.yhi);
-                const double e = __fma_rn(a, s.yhi, -qh);
-                const double lo = __fma_rn(a, s.ylo, e);
-                const double q = __dadd_rn(qh, lo);
+                const BinPoint pt = tile[i];
+                const double td = pt.t;
                 uint32_t row;  // phase bin + 2^31 (the bias vanishes in addresses)
                 if constexpr (FAST) {
-                    const double r = __dadd_rd(q, kMagic15);
-                    const double y = __fma_rd(q, nd20, kMagic15);
+                    double a;
+                    if constexpr (HAS_PDT) {
+                        a = td - s.c * td * td;
+                    } else {
+                        a = td;
+                    }
+                    const double qh = __dmul_rn(a, s.yhi);
+                    const double r = __dadd_rd(qh, kMagic15);
+                    const double y = __fma_rd(qh, nd20, kMagic15);
                     const uint32_t ylo = (uint32_t)__double2loint(y);
                     const uint32_t yhi = (uint32_t)__double2hiint(y);
                     row = __funnelshift_r(ylo, yhi, 20) + (uint32_t)__double2loint(r) * n_neg;
-                    if (((ylo + edge_d) & 0xFFFFFu) < 2u * edge_d) {
+                    if (ylo * 4096u + edge_add < edge_lim) {
                         // Near a bin edge: the reference's exact sequence.
-                        const float folded = fabsf((float)(q - floor(q)));
+                        const float folded = (HAS_PDT) ? fold_exact<true>(td, s)
+                                                       : fold_exact<false>(td, s);
                         row = 0x80000000u + min(trunc_u(folded / p.phase_bin_size), nP);
                     }
                 } else {
-                    const float folded = fabsf((float)(q - floor(q)));
+                    const float folded = fold_exact<HAS_PDT>(td, s);
                     row = 0x80000000u + min(trunc_u(folded / p.phase_bin_size), nP);
                 }
                 if constexpr (ALGO == ALGO_CE) {
-                    const uint2 ax = reinterpret_cast<const uint2*>(tile_aux)[i];
-                    red_shared_u32(row * row_stride + ax.x + tbase, ax.y);
+                    red_shared_u32(row * row_stride + pt.a + tbase, pt.b);
                 } else {
-                    const uint32_t qv = reinterpret_cast<const uint32_t*>(tile_aux)[i];
                     const uint32_t a0 = row * (BLOCK * 4) + tbase;
                     red_shared_u32(a0, 1u);
-                    red_shared_u32(a0 + sum_off, qv);
+                    red_shared_u32(a0 + sum_off, pt.a);
                 }
             }
         };
@@ -171,7 +178,6 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
             else body(std::false_type{}, std::false_type{});
         }
     }
-
     if (!active) return;
     __syncwarp();
     const size_t out_idx =

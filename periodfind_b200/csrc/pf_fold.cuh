@@ -230,6 +230,33 @@ __device__ __forceinline__ void accumulate(const FoldParams& p, const Views& v, 
         __syncthreads();
         if (!active) continue;
 
+        if constexpr (ALGO == ALGO_LS && FOLD == FOLD_DF && !ALT) {
+            // Four points per pair of 128-bit broadcast loads; the tail (not
+            // the zero padding) one point at a time.
+            auto ls_point = [&](float t, float mag) {
+                const float ph = fold_df<HAS_PDT>(t, s);
+                float sin_val, cos_val;
+                sincosf(kTwoPi * ph, &sin_val, &cos_val);
+                ls.mag_cos += mag * cos_val;
+                ls.mag_sin += mag * sin_val;
+                ls.cos_cos += cos_val * cos_val;
+                ls.cos_sin += cos_val * sin_val;
+            };
+            const float4* t4 = reinterpret_cast<const float4*>(tile_t);
+            const float4* m4 = reinterpret_cast<const float4*>(v.tile_a);
+            const uint32_t full = cnt & ~3u;
+#pragma unroll 2
+            for (uint32_t i = 0; i < full; i += 4) {
+                const float4 tt = t4[i >> 2], mm = m4[i >> 2];
+                ls_point(tt.x, mm.x);
+                ls_point(tt.y, mm.y);
+                ls_point(tt.z, mm.z);
+                ls_point(tt.w, mm.w);
+            }
+            for (uint32_t i = full; i < cnt; i++) ls_point(tile_t[i], __uint_as_float(v.tile_a[i]));
+            continue;
+        }
+
 #pragma unroll 4
         for (uint32_t i = 0; i < cnt; i++) {
             float folded;

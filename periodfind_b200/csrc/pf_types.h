@@ -67,8 +67,7 @@ struct FoldParams {
 // Shared-memory bytes of the chosen bin kernel (pf_bin.cuh).
 inline size_t bin_smem_bytes(int algo, bool cnt16, int block, uint32_t n_phase,
                              uint32_t n_mag) {
-    const size_t aux = (algo == ALGO_CE) ? 8 : 4;
-    size_t bytes = (size_t)kBinTile * (8 + aux);
+    size_t bytes = (size_t)kBinTile * 16;  // {double t; u32 a, b} per point
     if (algo == ALGO_CE) {
         const size_t w = cnt16 ? (n_mag + 1) / 2 : n_mag;
         bytes += (size_t)(n_phase + 1) * w * block * 4;
