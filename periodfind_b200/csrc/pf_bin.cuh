@@ -130,43 +130,80 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
         __syncthreads();
         if (!active) continue;
 
-        auto body = [&](auto has_pdt_tag, auto fast_tag) {
+        // Fast bin of one point: row (+2^31 bias) and the edge-test value
+        // ((fraction + D) << 12); the point is near an edge iff ev < edge_lim.
+        auto fast_bin = [&](double td, auto has_pdt_tag, uint32_t& ev) -> uint32_t {
             constexpr bool HAS_PDT = decltype(has_pdt_tag)::value;
+            double a;
+            if constexpr (HAS_PDT) {
+                a = td - s.c * td * td;
+            } else {
+                a = td;
+            }
+            const double qh = __dmul_rn(a, s.yhi);
+            const double r = __dadd_rd(qh, kMagic15);
+            const double y = __fma_rd(qh, nd20, kMagic15);
+            const uint32_t ylo = (uint32_t)__double2loint(y);
+            const uint32_t yhi = (uint32_t)__double2hiint(y);
+            ev = ylo * 4096u + edge_add;
+            return __funnelshift_r(ylo, yhi, 20) + (uint32_t)__double2loint(r) * n_neg;
+        };
+        // The reference's exact sequence (correctly rounded quotient, float
+        // fold, f32 divide): the bin (+2^31 bias).
+        auto exact_bin = [&](double td, auto has_pdt_tag) -> uint32_t {
+            constexpr bool HAS_PDT = decltype(has_pdt_tag)::value;
+            const float folded = fold_exact<HAS_PDT>(td, s);
+            return 0x80000000u + min(trunc_u(folded / p.phase_bin_size), nP);
+        };
+        auto add = [&](uint32_t row, const BinPoint& pt, uint32_t sign) {
+            // sign is 1 (add) or 0xFFFFFFFF (take back); u32 wraparound keeps
+            // packed 16-bit halves and sums exact.
+            if constexpr (ALGO == ALGO_CE) {
+                red_shared_u32(row * row_stride + pt.a + tbase, pt.b * sign);
+            } else {
+                const uint32_t a0 = row * (BLOCK * 4) + tbase;
+                red_shared_u32(a0, sign);
+                red_shared_u32(a0 + sum_off, pt.a * sign);
+            }
+        };
+
+        auto body = [&](auto has_pdt_tag, auto fast_tag) {
             constexpr bool FAST = decltype(fast_tag)::value;
+            if constexpr (FAST) {
+                // Groups of 32 points: no branch per point; a group whose
+                // smallest edge-test value is below the limit is revisited
+                // and its near-edge points are moved to the reference's bin.
+                for (uint32_t g = 0; g < cnt; g += 32) {
+                    const uint32_t gend = min(g + 32u, cnt);
+                    uint32_t emin = 0xFFFFFFFFu;
 #pragma unroll 4
-            for (uint32_t i = 0; i < cnt; i++) {
-                const BinPoint pt = tile[i];
-                const double td = pt.t;
-                uint32_t row;  // phase bin + 2^31 (the bias vanishes in addresses)
-                if constexpr (FAST) {
-                    double a;
-                    if constexpr (HAS_PDT) {
-                        a = td - s.c * td * td;
-                    } else {
-                        a = td;
+                    for (uint32_t i = g; i < gend; i++) {
+                        const BinPoint pt = tile[i];
+                        uint32_t ev;
+                        const uint32_t row = fast_bin(pt.t, has_pdt_tag, ev);
+                        emin = min(emin, ev);
+                        add(row, pt, 1u);
                     }
-                    const double qh = __dmul_rn(a, s.yhi);
-                    const double r = __dadd_rd(qh, kMagic15);
-                    const double y = __fma_rd(qh, nd20, kMagic15);
-                    const uint32_t ylo = (uint32_t)__double2loint(y);
-                    const uint32_t yhi = (uint32_t)__double2hiint(y);
-                    row = __funnelshift_r(ylo, yhi, 20) + (uint32_t)__double2loint(r) * n_neg;
-                    if (ylo * 4096u + edge_add < edge_lim) {
-                        // Near a bin edge: the reference's exact sequence.
-                        const float folded = (HAS_PDT) ? fold_exact<true>(td, s)
-                                                       : fold_exact<false>(td, s);
-                        row = 0x80000000u + min(trunc_u(folded / p.phase_bin_size), nP);
+                    if (emin < edge_lim) {
+                        for (uint32_t i = g; i < gend; i++) {
+                            const BinPoint pt = tile[i];
+                            uint32_t ev;
+                            const uint32_t row = fast_bin(pt.t, has_pdt_tag, ev);
+                            if (ev < edge_lim) {
+                                const uint32_t ex = exact_bin(pt.t, has_pdt_tag);
+                                if (ex != row) {
+                                    add(row, pt, 0xFFFFFFFFu);
+                                    add(ex, pt, 1u);
+                                }
+                            }
+                        }
                     }
-                } else {
-                    const float folded = fold_exact<HAS_PDT>(td, s);
-                    row = 0x80000000u + min(trunc_u(folded / p.phase_bin_size), nP);
                 }
-                if constexpr (ALGO == ALGO_CE) {
-                    red_shared_u32(row * row_stride + pt.a + tbase, pt.b);
-                } else {
-                    const uint32_t a0 = row * (BLOCK * 4) + tbase;
-                    red_shared_u32(a0, 1u);
-                    red_shared_u32(a0 + sum_off, pt.a);
+            } else {
+#pragma unroll 4
+                for (uint32_t i = 0; i < cnt; i++) {
+                    const BinPoint pt = tile[i];
+                    add(exact_bin(pt.t, has_pdt_tag), pt, 1u);
                 }
             }
         };
