@@ -34,9 +34,16 @@
 namespace pfk {
 namespace PF_KNS {
 
+// Fire-and-forget shared reduction.  No "memory" clobber: the counters it
+// updates are never read inside the point loop, so the compiler may hoist
+// the next points' shared loads above it (independent point chains overlap).
+// The epilogue's counter reads are ordered after the loop by an explicit
+// compiler barrier plus __syncwarp().
 __device__ __forceinline__ void red_shared_u32(uint32_t addr, uint32_t v) {
-    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(v));
 }
+
+__device__ __forceinline__ void compiler_fence() { asm volatile("" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
     uint32_t v;
@@ -130,6 +137,11 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
         __syncthreads();
         if (!active) continue;
 
+        // One 128-bit shared load per point record.
+        auto load_point = [&](uint32_t i) -> BinPoint {
+            const uint4 raw = reinterpret_cast<const uint4*>(tile)[i];
+            return BinPoint{__hiloint2double((int)raw.y, (int)raw.x), raw.z, raw.w};
+        };
         // Fast bin of one point: row (+2^31 bias) and the edge-test value
         // ((fraction + D) << 12); the point is near an edge iff ev < edge_lim.
         auto fast_bin = [&](double td, auto has_pdt_tag, uint32_t& ev) -> uint32_t {
@@ -178,7 +190,7 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
                     uint32_t emin = 0xFFFFFFFFu;
 #pragma unroll 4
                     for (uint32_t i = g; i < gend; i++) {
-                        const BinPoint pt = tile[i];
+                        const BinPoint pt = load_point(i);
                         uint32_t ev;
                         const uint32_t row = fast_bin(pt.t, has_pdt_tag, ev);
                         emin = min(emin, ev);
@@ -216,6 +228,7 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
         }
     }
     if (!active) return;
+    compiler_fence();
     __syncwarp();
     const size_t out_idx =
         (size_t)w.curve * ((size_t)p.n_per * p.n_pdt) + (size_t)pi * p.n_pdt + w.pdt;
