@@ -35,7 +35,6 @@ UNITS = {
     "pf_peaks.cu": [],
     "pf_api.cu": [],
 }
-HEADERS = ["pf_types.h", "pf_launch.h", "pf_fold.cuh", "pf_kern_dispatch.inc"]
 
 LIB = os.path.join(HERE, "libpfb200.so")
 PEAKS_LIB = os.path.join(HERE, "libpfpeaks.so")
@@ -53,7 +52,9 @@ def _mtime(p: str) -> float:
 
 
 def _dep_mtime() -> float:
-    deps = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "pf.h")]
+    """Newest header any unit may include (every .h/.cuh/.inc in csrc/)."""
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
+            if f.endswith((".h", ".cuh", ".inc"))] + [os.path.join(INCLUDE, "pf.h")]
     return max(_mtime(d) for d in deps)
 
 
