@@ -82,15 +82,15 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
     Cell s;
     cell_setup<FOLD_EXACT>(s, p.periods[pi], period_dt);
 
-    // Counter layout: CE  [nP + 1 rows][W words][BLOCK] u32, W = nM or ceil(nM/2)
-    //                 AOV [2][nP + 1][BLOCK] u32 (count, fixed-point sum)
+    // Counter layout: CE  [nP rows][W words][BLOCK] u32, W = nM or ceil(nM/2)
+    //                 AOV [2][nP][BLOCK] u32 (count, fixed-point sum)
     const uint32_t W = (ALGO == ALGO_CE) ? (CNT16 ? (nM + 1) / 2 : nM) : 1;
     const uint32_t row_stride = W * BLOCK * 4;  // bytes per phase row
-    const uint32_t slots = (ALGO == ALGO_CE) ? (nP + 1) * W : 2 * (nP + 1);
+    const uint32_t slots = (ALGO == ALGO_CE) ? nP * W : 2 * nP;
     for (uint32_t k = 0; k < slots; k++)
         reinterpret_cast<uint32_t*>(cnt_raw)[k * BLOCK + tid] = 0u;
     const uint32_t tbase = cnt_base + tid * 4;
-    const uint32_t sum_off = (nP + 1) * BLOCK * 4;  // AOV: sums after counts
+    const uint32_t sum_off = nP * BLOCK * 4;  // AOV: sums after counts
 
     // Range guard for y = q * n * 2^20 (uniform over the CTA).  Non-finite
     // periods or derivatives (device-pointer callers are not checked on the
@@ -161,11 +161,13 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
             return __funnelshift_r(ylo, yhi, 20) + (uint32_t)__double2loint(r) * n_neg;
         };
         // The reference's exact sequence (correctly rounded quotient, float
-        // fold, f32 divide): the bin (+2^31 bias).
+        // fold, f32 divide, then % n_phase: a folded phase of 1.0f gives bin
+        // n_phase, which wraps to 0): the bin (+2^31 bias).
         auto exact_bin = [&](double td, auto has_pdt_tag) -> uint32_t {
             constexpr bool HAS_PDT = decltype(has_pdt_tag)::value;
             const float folded = fold_exact<HAS_PDT>(td, s);
-            return 0x80000000u + min(trunc_u(folded / p.phase_bin_size), nP);
+            const uint32_t pb = min(trunc_u(folded / p.phase_bin_size), nP);
+            return 0x80000000u + (pb == nP ? 0u : pb);
         };
         auto add = [&](uint32_t row, const BinPoint& pt, uint32_t sign) {
             // sign is 1 (add) or 0xFFFFFFFF (take back); u32 wraparound keeps
@@ -236,16 +238,12 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
 
     if constexpr (ALGO == ALGO_CE) {
         auto count = [&](uint32_t j, uint32_t i) -> uint32_t {
-            // Row nP (folded == 1.0 in the reference) wraps to row 0.
-            auto get = [&](uint32_t jj) -> uint32_t {
-                if constexpr (CNT16) {
-                    const uint32_t wv = cnt32[(jj * W + (i >> 1)) * BLOCK + tid];
-                    return (i & 1u) ? (wv >> 16) : (wv & 0xFFFFu);
-                } else {
-                    return cnt32[(jj * W + i) * BLOCK + tid];
-                }
-            };
-            return j == 0 ? get(0) + get(nP) : get(j);
+            if constexpr (CNT16) {
+                const uint32_t wv = cnt32[(j * W + (i >> 1)) * BLOCK + tid];
+                return (i & 1u) ? (wv >> 16) : (wv & 0xFFFFu);
+            } else {
+                return cnt32[(j * W + i) * BLOCK + tid];
+            }
         };
         const float divf = (float)((unsigned long long)n * p.p_overlap * p.m_overlap);
         float ce = 0.0f;
@@ -268,16 +266,12 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
         }
         p.out[out_idx] = ce;
     } else {
-        const uint32_t* sums = cnt32 + (nP + 1) * BLOCK;
+        const uint32_t* sums = cnt32 + nP * BLOCK;
         const double xbar = cd.fix_sumx / (double)n;
         double s1 = 0.0, sbx = 0.0;
         for (uint32_t b = 0; b < nP; b++) {
-            uint32_t c = cnt32[b * BLOCK + tid];
-            uint32_t X = sums[b * BLOCK + tid];
-            if (b == 0) {
-                c += cnt32[nP * BLOCK + tid];
-                X += sums[nP * BLOCK + tid];
-            }
+            const uint32_t c = cnt32[b * BLOCK + tid];
+            const uint32_t X = sums[b * BLOCK + tid];
             if (c != 0u) {
                 const double nb = (double)c;
                 const double Xd = (double)X;

@@ -23,7 +23,7 @@ enum : int { AOVACC_F32 = 0, AOVACC_FIX = 1 };
 constexpr int kFixCountShift = 44;
 
 constexpr uint32_t kTile = 1024;     // points staged per tile (multiple of 4)
-constexpr uint32_t kBinTile = 1024;  // points per tile in the chosen bin kernel
+constexpr uint32_t kBinTile = 256;   // points per tile in the chosen bin kernel
 
 // One light curve in the packed arrays.  Curves start on 16-byte
 // boundaries (offsets are multiples of 4 points).
@@ -70,9 +70,9 @@ inline size_t bin_smem_bytes(int algo, bool cnt16, int block, uint32_t n_phase,
     size_t bytes = (size_t)kBinTile * 16;  // {double t; u32 a, b} per point
     if (algo == ALGO_CE) {
         const size_t w = cnt16 ? (n_mag + 1) / 2 : n_mag;
-        bytes += (size_t)(n_phase + 1) * w * block * 4;
+        bytes += (size_t)n_phase * w * block * 4;
     } else {
-        bytes += (size_t)2 * (n_phase + 1) * block * 4;
+        bytes += (size_t)2 * n_phase * block * 4;
     }
     return bytes;
 }
