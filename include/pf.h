@@ -167,6 +167,29 @@ int pf_find_peaks_dev(pf_ctx* ctx, const float* d_data, uint64_t n_curves,
                       int use_max, int64_t* d_out_idx, float* d_out_val,
                       void* stream);
 
+/* LS periodograms and their top-N peaks on device pointers, allocating
+ * nothing.  No counterpart in the reference: it exists for callers that may
+ * not call cudaMalloc where they need peaks -- code whose device memory is
+ * owned by another allocator's pool, latency-critical paths that cannot
+ * take cudaMalloc's implicit synchronisation, or fixed memory budgets.
+ * Arguments are those of pf_ls_dev plus pf_find_peaks_dev's outputs (device
+ * arrays [n_curves][n_peaks]); no context is used.  All scratch lives in one
+ * 32 MiB device array inside the library (held by every GPU that loads it
+ * until exit); a batch whose packed curves, work list and periodograms need
+ * more is rejected with PF_EINVAL and a message in `err` (a caller buffer of
+ * err_len bytes, may be NULL).  The first call on a device looks up the
+ * array's address with that device current: make it before any stream
+ * capture.  Calls share the array, so calls whose GPU work overlaps race on
+ * it; order them on one stream.  Work is enqueued on `stream` (NULL = the
+ * CUDA default stream) and the call returns without synchronising. */
+int pf_ls_peaks_dev_noalloc(const float* d_times, const float* d_mags,
+                            const int64_t* offsets, uint64_t n_curves,
+                            const float* d_periods, uint64_t n_per,
+                            const float* d_pdts, uint64_t n_pdt,
+                            uint32_t n_peaks, uint32_t min_distance, int mode,
+                            int64_t* d_out_idx, float* d_out_val, void* stream,
+                            char* err, uint64_t err_len);
+
 /* Number of kernels this context has launched since creation (telemetry
  * for benchmarks: launches of the library's own kernels only). */
 uint64_t pf_launch_count(const pf_ctx* ctx);

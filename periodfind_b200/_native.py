@@ -57,6 +57,8 @@ SIGNATURES = {
                    _int),
     "pf_ls_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _int, _vp, _vp], _int),
     "pf_find_peaks_dev": ([_vp, _vp, _u64, _u64, _u32, _u32, _int, _vp, _vp, _vp], _int),
+    "pf_ls_peaks_dev_noalloc": ([_vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int,
+                                 _vp, _vp, _vp, ctypes.c_char_p, _u64], _int),
     "pf_launch_count": ([_vp], _u64),
     "pf_last_kernel_ms": ([_vp], ctypes.c_double),
 }

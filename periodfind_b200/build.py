@@ -34,6 +34,7 @@ UNITS = {
     "pf_prep.cu": ["-fmad=false"],
     "pf_peaks.cu": [],
     "pf_api.cu": [],
+    "pf_noalloc.cu": [],
 }
 
 LIB = os.path.join(HERE, "libpfb200.so")
