@@ -419,7 +419,11 @@ def main():
                          "frac": achieved / peak if peak == peak else None,
                          "ops_per_eval": fp64_per_eval, "kernel_ms": ce_ms,
                          "peak_source": "measured DFMA rate (periodfind_b200/csrc/pipe_peaks.cu)",
-                         "traffic": None,
+                         "traffic": CE_TRAFFIC_BYTES,
+                         "shared_atomic_view": {
+                             "achieved_gops": evals_ce / (ce_ms * 1e-3) / 1e9,
+                             "peak_gops": pipes.get("atoms_u32_private", {}).get("per_s", float("nan")) / 1e9,
+                             "ops_per_eval": 1},
                          "hbm_view": {"achieved_gbs": hbm_gbs, "peak_gbs": 6453.7,
                                       "frac": hbm_gbs / 6453.7}},
             "kernels_ms": {"ce_fold": ce_ms, "aov_fold": aov_ms},
@@ -433,10 +437,13 @@ def main():
         dist.destroy_process_group()
 
 
-# FP64-pipe operations per evaluation in the chosen CE fold (bin_kernel):
-# exact quotient (DMUL, 2 DFMA, DADD), floor (DADD.RD), bin (DFMA.RD), plus
-# DMUL + DFMA for t - c t^2 on the period-derivative cells (half the grid).
-FP64_OPS_PER_EVAL = 6 + 2 * sum(1 for d in PDTS if d != 0.0) / len(PDTS)
+# FP64-pipe operations per evaluation in the chosen CE bin kernel's fast
+# path: t * RN(1/P) (DMUL), floor (DADD.RD), bin with fraction bits
+# (DFMA.RD), plus DMUL + DFMA for t - c t^2 on the period-derivative cells.
+FP64_OPS_PER_EVAL = 3 + 2 * sum(1 for d in PDTS if d != 0.0) / len(PDTS)
+# DRAM bytes (read + write) of one full-size CE bin_kernel launch, from the
+# ncu capture summarised in profiles/bin_kernel_ce_aov_10x4096.md.
+CE_TRAFFIC_BYTES = 52514048 + 28131328
 
 if __name__ == "__main__":
     main()
