@@ -351,6 +351,7 @@ def main():
     # Each rank processes its own batch of curves (weak scaling, no exchange).
     ts, ms, periods, pdts = make_workload(args.curves, SEED + rank)
     from periodfind_b200 import _native as nat
+    from periodfind_b200.distributed import max_over_ranks
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -364,26 +365,18 @@ def main():
     clocks.start()
     ms_step, launches = time_device(chosen, args.steps, args.warmup, torch, flush)
     clock_info = clocks.stop()
-    t_max = torch.tensor([ms_step], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms_step = float(t_max.item())
+    ms_step = max_over_ranks(ms_step, device="cuda")
     ce_ms, aov_ms = time_kernels(chosen, torch)
 
     plain = DeviceStep(ts, ms, periods, pdts, nat.PF_MODE_PLAIN, torch, local)
     plain_ms, _ = time_device(plain, max(1, min(args.steps, 3)), 1, torch, flush)
-    pt = torch.tensor([plain_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(pt, op=dist.ReduceOp.MAX)
-    plain_ms = float(pt.item())
+    plain_ms = max_over_ranks(plain_ms, device="cuda")
     del plain
 
     e2e_s = time_e2e(ts, ms, periods, pdts, max(1, min(args.steps, 3)), 1, local)
-    et = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    e2e_s = max_over_ranks(e2e_s, device="cuda")
     if dist:
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
         dist.barrier()
-    e2e_s = float(et.item())
 
     n_eval = evals_per_step(args.curves) * world
     value = n_eval / (ms_step * 1e-3)
