@@ -318,6 +318,121 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------ ragged batch
+
+
+def make_ragged(n_curves=100000, seed=SEED + 5, n_periods=20000):
+    """Mixed ragged batch: lengths lognormal (median 300, sigma 0.8) clipped to
+    [20, 2000]; seasonal cadence over 2500 days (125-day seasons); 1/3
+    sinusoids, 1/3 box eclipses (depth 0.5, duty 0.05), 1/3 pure noise; noise
+    sigma U[0.02, 0.1]; 20000 periods log-spaced in [0.05, 500] days."""
+    rng = np.random.default_rng(seed)
+    lens = np.clip(np.round(rng.lognormal(np.log(300.0), 0.8, n_curves)), 20, 2000).astype(np.int64)
+    cid = np.repeat(np.arange(n_curves), lens)
+    n_years = int(np.ceil(2500.0 / 365.25))
+    t = rng.integers(0, n_years, cid.size) * 365.25 + rng.uniform(0.0, 125.25, cid.size)
+    t = np.minimum(t, 2500.0)
+    order = np.lexsort((t, cid))
+    t = t[order].astype(np.float32)
+    period = np.exp(rng.uniform(np.log(0.05), np.log(500.0), n_curves))[cid]
+    phase = rng.uniform(0, 1, n_curves)[cid]
+    kind = (np.arange(n_curves) % 3)[cid]
+    sigma = rng.uniform(0.02, 0.1, n_curves)[cid]
+    ph = np.mod(t / period + phase, 1.0)
+    y = np.where(kind == 0, 0.3 * np.sin(2 * np.pi * ph),
+                 np.where(kind == 1, np.where(ph < 0.05, -0.5, 0.0), 0.0))
+    m = (15.0 + y + rng.normal(0.0, 1.0, cid.size) * sigma).astype(np.float32)
+    off = np.zeros(n_curves + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    periods = np.exp(np.linspace(np.log(0.05), np.log(500.0), n_periods)).astype(np.float32)
+    return t, m, off, periods, np.zeros(1, np.float32)
+
+
+def ragged_arm(args):
+    import torch
+
+    from periodfind_b200 import _native as nat
+
+    torch.cuda.set_device(0)
+    n_curves = args.curves if args.curves != N_CURVES else 100000
+    t, m, off, periods, pdts = make_ragged(n_curves)
+    lens = np.diff(off)
+    ctx = nat.default_context(0)
+    dev = "cuda"
+    d_t = torch.from_numpy(t).to(dev)
+    # Per-curve magnitude preparation as the reference does it: normalise for
+    # CE (periodfind/_utils.py:39-45), centre for LS, raw for AOV.
+    seg_min = np.minimum.reduceat(m, off[:-1])
+    seg_max = np.maximum.reduceat(m, off[:-1])
+    cid = np.repeat(np.arange(n_curves), lens)
+    m_ce = (((m - seg_min[cid]) / (seg_max[cid] - seg_min[cid])) * np.float32(0.999)
+            + np.float32(5e-4)).astype(np.float32)
+    seg_mean = (np.add.reduceat(m.astype(np.float64), off[:-1]) / lens).astype(np.float32)
+    m_ls = (m - seg_mean[cid]).astype(np.float32)
+    mags = {"ce": torch.from_numpy(m_ce).to(dev), "aov": torch.from_numpy(m).to(dev),
+            "ls": torch.from_numpy(m_ls).to(dev)}
+    d_p = torch.from_numpy(periods).to(dev)
+    d_d = torch.from_numpy(pdts).to(dev)
+    cells = len(periods) * len(pdts)
+    pg = torch.empty((n_curves, cells), dtype=torch.float32, device=dev)
+    pk_i = torch.empty((n_curves, N_PEAKS), dtype=torch.int64, device=dev)
+    pk_v = torch.empty((n_curves, N_PEAKS), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    s = stream.cuda_stream
+    evals = int(lens.sum()) * cells
+
+    def step(algo, flags):
+        h, lib = ctx.handle, ctx.lib
+        common = (h, d_t.data_ptr(), mags[algo].data_ptr(), off.ctypes.data, n_curves,
+                  d_p.data_ptr(), len(periods), d_d.data_ptr(), len(pdts))
+        if algo == "ce":
+            ctx.check(lib.pf_ce_dev(*common, 10, 10, 1, 1, flags, pg.data_ptr(), s))
+        elif algo == "aov":
+            ctx.check(lib.pf_aov_dev(*common, 15, 1, flags, pg.data_ptr(), s))
+        else:
+            ctx.check(lib.pf_ls_dev(*common, flags, pg.data_ptr(), s))
+        ctx.check(lib.pf_find_peaks_dev(h, pg.data_ptr(), n_curves, cells, N_PEAKS, 1,
+                                        0 if algo == "ce" else 1, pk_i.data_ptr(),
+                                        pk_v.data_ptr(), s))
+
+    out = {"workload": f"ragged: {n_curves} curves, lengths lognormal(median 300, sigma 0.8) "
+                       f"in [20, 2000] (mean {lens.mean():.0f}), seasonal cadence 2500 d, "
+                       f"{len(periods)} log periods [0.05, 500] d, top-{N_PEAKS} peaks",
+           "evals_per_algo": evals, "algos": {}}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for algo in ("ce", "aov", "ls"):
+        row = {}
+        for mode, flags in (("chosen", nat.PF_MODE_CHOSEN), ("plain", nat.PF_MODE_PLAIN)):
+            step(algo, flags)
+            torch.cuda.synchronize()
+            ts_ = []
+            for _ in range(max(1, args.steps)):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                step(algo, flags)
+                e1.record(stream)
+                e1.synchronize()
+                ts_.append(e0.elapsed_time(e1))
+            ms_ = float(np.median(ts_))
+            # Per-curve device latency from a separate, stamped run.
+            step(algo, flags | nat.PF_TIMING)
+            lat = np.zeros(n_curves)
+            ctx.check(ctx.lib.pf_curve_latency(ctx.handle, n_curves, lat.ctypes.data))
+            row[mode] = {"ms": ms_, "evals_per_s": evals / (ms_ * 1e-3),
+                         "curve_latency_ms_p50": float(np.percentile(lat, 50)) / 1e6,
+                         "curve_latency_ms_p99": float(np.percentile(lat, 99)) / 1e6}
+        row["chosen_over_plain"] = row["plain"]["ms"] / row["chosen"]["ms"]
+        out["algos"][algo] = row
+    tc = sum(out["algos"][a]["chosen"]["ms"] for a in out["algos"])
+    tp = sum(out["algos"][a]["plain"]["ms"] for a in out["algos"])
+    out["all_three"] = {"chosen_evals_per_s": 3 * evals / (tc * 1e-3),
+                        "plain_evals_per_s": 3 * evals / (tp * 1e-3),
+                        "chosen_over_plain": tp / tc}
+    print(json.dumps(out), flush=True)
+
+
 # ------------------------------------------------------------------- main
 
 
@@ -329,9 +444,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--curves", type=int, default=N_CURVES)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--workload", default="batch", choices=["batch", "ragged"],
+                    help="'ragged': the mixed ragged batch (separate report, 1 GPU)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.workload == "ragged":
+        ragged_arm(args)
         return
 
     import torch

@@ -38,6 +38,8 @@
  *                  frequency as an unevaluated float pair; no FP64 per point.
  *  PF_FOLD_EXACT   (LS, chosen) the divide-free exact fold instead of the
  *                  split-precision phase: bit-identical to the plain form.
+ *  PF_TIMING       record device timestamps per work item (CTA start and
+ *                  end, %globaltimer) for pf_curve_latency.
  */
 #ifndef PERIODFIND_B200_PF_H
 #define PERIODFIND_B200_PF_H
@@ -61,6 +63,7 @@ extern "C" {
 #define PF_FOLD_F32 0x100
 #define PF_FOLD_DF 0x200
 #define PF_FOLD_EXACT 0x400
+#define PF_TIMING 0x1000
 
 typedef struct pf_ctx pf_ctx;
 
@@ -189,6 +192,12 @@ int pf_ls_peaks_dev_noalloc(const float* d_times, const float* d_mags,
                             uint32_t n_peaks, uint32_t min_distance, int mode,
                             int64_t* d_out_idx, float* d_out_val, void* stream,
                             char* err, uint64_t err_len);
+
+/* Per-curve device latency of the last PF_TIMING launch on this context:
+ * out_ns[c] = last end - first start (ns) over the CTAs that computed curve
+ * c's periodogram; n_curves must be that launch's.  Synchronises the
+ * stream that launch ran on. */
+int pf_curve_latency(pf_ctx* ctx, uint64_t n_curves, double* out_ns);
 
 /* Number of kernels this context has launched since creation (telemetry
  * for benchmarks: launches of the library's own kernels only). */

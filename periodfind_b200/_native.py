@@ -28,6 +28,7 @@ PF_SEM_CPU = 0x10
 PF_FOLD_F32 = 0x100
 PF_FOLD_DF = 0x200
 PF_FOLD_EXACT = 0x400
+PF_TIMING = 0x1000
 
 _vp = ctypes.c_void_p
 _u64 = ctypes.c_uint64
@@ -59,6 +60,7 @@ SIGNATURES = {
     "pf_find_peaks_dev": ([_vp, _vp, _u64, _u64, _u32, _u32, _int, _vp, _vp, _vp], _int),
     "pf_ls_peaks_dev_noalloc": ([_vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int,
                                  _vp, _vp, _vp, ctypes.c_char_p, _u64], _int),
+    "pf_curve_latency": ([_vp, _u64, _vp], _int),
     "pf_launch_count": ([_vp], _u64),
     "pf_last_kernel_ms": ([_vp], ctypes.c_double),
 }

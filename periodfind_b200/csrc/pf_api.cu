@@ -54,7 +54,12 @@ struct pf_ctx {
     cudaEvent_t ev_done = nullptr;              // last device-pointer call done
     bool staged_pending = false, done_recorded = false, timed_pending = false;
     std::string err;
-    DevBuf d_in, d_aux32, d_aux64, d_out, d_pidx, d_pval, d_pack, d_misc;
+    DevBuf d_in, d_aux32, d_aux64, d_out, d_pidx, d_pval, d_pack, d_misc, d_stamps;
+    // PF_TIMING: the curve of each work item of the last timed launch, and
+    // the stream it ran on.
+    std::vector<uint32_t> stamp_curves;   // curve of each stamped work item
+    uint64_t stamp_n_curves = 0;
+    cudaStream_t stamp_stream = nullptr;
     PinnedBuf h_in;
     uint64_t launches = 0;
     double last_ms = -1.0;
@@ -362,7 +367,7 @@ int staging_ready(pf_ctx* ctx) {
     return PF_OK;
 }
 
-void fill_meta(const Job& j, const Layout& L, const FoldConfig& cfg, char* hb) {
+void fill_meta(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig& cfg, char* hb) {
     CurveDesc* hc = (CurveDesc*)(hb + L.o_curves);
     for (uint64_t c = 0; c < j.n_curves; c++) {
         CurveDesc d{};
@@ -370,7 +375,13 @@ void fill_meta(const Job& j, const Layout& L, const FoldConfig& cfg, char* hb) {
         d.n = L.len[c];
         hc[c] = d;
     }
-    build_work(j, L, cfg.block, (WorkItem*)(hb + L.o_work));
+    WorkItem* w = (WorkItem*)(hb + L.o_work);
+    build_work(j, L, cfg.block, w);
+    if (j.mode & PF_TIMING) {
+        ctx->stamp_curves.resize(L.n_work);
+        for (uint32_t k = 0; k < L.n_work; k++) ctx->stamp_curves[k] = w[k].curve;
+        ctx->stamp_n_curves = j.n_curves;
+    }
 }
 
 // Device pipeline shared by both entry styles: preparation kernel, fused
@@ -430,6 +441,13 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
             PF_CUDA(launch_aov_mean(p.m, dcurves, ncur, s), "AOV mean kernel");
         }
         ctx->launches++;
+    }
+    p.stamps = nullptr;
+    if (j.mode & PF_TIMING) {
+        if ((rc = ensure_dev(ctx, ctx->d_stamps, (size_t)L.n_work * 16)) != PF_OK) return rc;
+        PF_CUDA(cudaMemsetAsync(ctx->d_stamps.p, 0, (size_t)L.n_work * 16, s), "memset");
+        p.stamps = (unsigned long long*)ctx->d_stamps.p;
+        ctx->stamp_stream = s;
     }
     PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
     cudaError_t e = cpu ? launch_fold_cpusem(cfg, p, L.n_work, s)
@@ -507,7 +525,7 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
         for (int b : bad)
             if (b) return fail(ctx, PF_EINVAL, "times must be finite");
     }
-    fill_meta(j, L, cfg, hb);
+    fill_meta(ctx, j, L, cfg, hb);
     memcpy(hb + L.o_periods, j.periods, j.n_per * 4);
     memcpy(hb + L.o_pdts, j.pdts, j.n_pdt * 4);
 
@@ -574,7 +592,7 @@ int run_dev(pf_ctx* ctx, const Job& j, const float* d_times, const float* d_mags
     if ((rc = ensure_dev(ctx, ctx->d_in, L.bytes)) != PF_OK) return rc;
     if ((rc = ensure_dev(ctx, ctx->d_pack, L.total_pts * 8 + 64)) != PF_OK) return rc;
     char* hb = (char*)ctx->h_in.p;
-    fill_meta(j, L, cfg, hb);
+    fill_meta(ctx, j, L, cfg, hb);
     memcpy(hb + L.o_srcoff, offsets, j.n_curves * 8);
 
     // Order this call after the previous one on this context (its buffers
@@ -667,7 +685,7 @@ void pf_ctx_destroy(pf_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->done_recorded) cudaEventSynchronize(ctx->ev_done);
     for (DevBuf* b : {&ctx->d_in, &ctx->d_aux32, &ctx->d_aux64, &ctx->d_out, &ctx->d_pidx,
-                      &ctx->d_pval, &ctx->d_pack, &ctx->d_misc})
+                      &ctx->d_pval, &ctx->d_pack, &ctx->d_misc, &ctx->d_stamps})
         if (b->p) cudaFree(b->p);
     if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -684,6 +702,30 @@ const char* pf_last_error(const pf_ctx* ctx) {
 }
 
 uint64_t pf_launch_count(const pf_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int pf_curve_latency(pf_ctx* ctx, uint64_t n_curves, double* out_ns) {
+    if (!ctx || (!out_ns && n_curves)) return PF_EINVAL;
+    const size_t nw = ctx->stamp_curves.size();
+    if (nw == 0) return fail(ctx, PF_EINVAL, "no launch with PF_TIMING on this context");
+    if (n_curves != ctx->stamp_n_curves)
+        return fail(ctx, PF_EINVAL, "n_curves differs from the last PF_TIMING launch");
+    std::vector<unsigned long long> st(2 * nw);
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    PF_CUDA(cudaMemcpyAsync(st.data(), ctx->d_stamps.p, nw * 16, cudaMemcpyDeviceToHost,
+                            ctx->stamp_stream),
+            "D2H stamps");
+    PF_CUDA(cudaStreamSynchronize(ctx->stamp_stream), "stream synchronize");
+    std::vector<unsigned long long> lo(n_curves, ~0ull), hi(n_curves, 0ull);
+    for (size_t k = 0; k < nw; k++) {
+        const uint32_t c = ctx->stamp_curves[k];
+        if (c >= n_curves) continue;
+        lo[c] = std::min(lo[c], st[2 * k]);
+        hi[c] = std::max(hi[c], st[2 * k + 1]);
+    }
+    for (uint64_t c = 0; c < n_curves; c++)
+        out_ns[c] = (hi[c] > lo[c] && lo[c] != ~0ull) ? (double)(hi[c] - lo[c]) : 0.0;
+    return PF_OK;
+}
 
 double pf_last_kernel_ms(const pf_ctx* ctx) {
     if (!ctx) return -1.0;

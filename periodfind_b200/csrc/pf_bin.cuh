@@ -70,6 +70,7 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
     unsigned char* cnt_raw = smem + kBinTile * sizeof(BinPoint);
     const uint32_t cnt_base = (uint32_t)__cvta_generic_to_shared(cnt_raw);
 
+    stamp_start(p);
     const WorkItem w = p.work[blockIdx.x];
     const CurveDesc cd = p.curves[w.curve];
     const uint32_t n = cd.n;
@@ -229,7 +230,10 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
             else body(std::false_type{}, std::false_type{});
         }
     }
-    if (!active) return;
+    if (!active) {
+        stamp_end(p);
+        return;
+    }
     compiler_fence();
     __syncwarp();
     const size_t out_idx =
@@ -289,6 +293,7 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
         p.out[out_idx] = (float)(scale * (s1 / (s2 <= 0.0 ? 0.0 : s2)));
 #endif
     }
+    stamp_end(p);
 }
 
 // CE per-point bin data for bin_kernel: {byte offset of the magnitude

@@ -160,6 +160,20 @@ __device__ double cta_qbound(const FoldParams& p, uint32_t pi, float period_dt) 
     return tmax / pmin + fabs((double)period_dt) * tmax * tmax / (2.0 * pmin * pmin);
 }
 
+// Optional per-work-item timing (%globaltimer, ns): the CTA's first thread
+// stamps the start; every thread raises the end stamp when it finishes.
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void stamp_start(const FoldParams& p) {
+    if (p.stamps && threadIdx.x == 0) p.stamps[2 * blockIdx.x] = global_ns();
+}
+__device__ __forceinline__ void stamp_end(const FoldParams& p) {
+    if (p.stamps) atomicMax(&p.stamps[2 * blockIdx.x + 1], global_ns());
+}
+
 // trunc(q) for finite q in [0, 2^23): identical to the reference's
 // (size_t) conversion on that range, without a conversion instruction.
 __device__ __forceinline__ unsigned trunc_u(float q) {
@@ -360,6 +374,7 @@ __global__ void __launch_bounds__(BLOCK) fold_kernel(const FoldParams p) {
     v.a_sum = reinterpret_cast<float*>(hist_raw) + (size_t)nP * BLOCK;
     v.a_sq = reinterpret_cast<float*>(hist_raw) + (size_t)2 * nP * BLOCK;
 
+    stamp_start(p);
     const WorkItem w = p.work[blockIdx.x];
     const CurveDesc cd = p.curves[w.curve];
     const uint32_t n = cd.n;
@@ -401,7 +416,10 @@ __global__ void __launch_bounds__(BLOCK) fold_kernel(const FoldParams p) {
         else accumulate<ALGO, FOLD, ACC, BLOCK, OVL, false, false>(p, v, s, cd.off, n, active, ls);
     }
 
-    if (!active) return;
+    if (!active) {
+        stamp_end(p);
+        return;
+    }
     const size_t out_idx =
         (size_t)w.curve * ((size_t)p.n_per * p.n_pdt) + (size_t)pi * p.n_pdt + w.pdt;
 
@@ -511,6 +529,7 @@ __global__ void __launch_bounds__(BLOCK) fold_kernel(const FoldParams p) {
         p.out[out_idx] = 0.5f * ((numerator_l / denominator_l) + (numerator_r / denominator_r));
 #endif
     }
+    stamp_end(p);
 }
 
 // ------------------------------------------------------------- preparation

@@ -16,7 +16,8 @@
 //     c + min_distance - 1 (after that index's own peak test), or at the
 //     end if no such index is fed;
 //   - a better extremum fed before that replaces it.
-// The sorted top-N list lives in the caller's output rows.
+// The sorted top-N list lives in shared memory (threshold in a register)
+// and is written to the caller's rows at the end.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -32,22 +33,18 @@ constexpr int kPerThread = 8;
 constexpr uint32_t kChunk = kPeakThreads * kPerThread;
 
 struct PeakState {
-    int64_t* idx;
+    int64_t* idx;   // shared memory, n_peaks entries
     float* val;
     uint32_t count, n_peaks;
     bool use_max;
     bool has_cand;
     int64_t cand_idx;
     float cand_val;
+    float thr;      // threshold(): the worst kept value once the list is full
 };
 
 __device__ __forceinline__ bool better(bool use_max, float a, float b) {
     return use_max ? (a > b) : (a < b);
-}
-
-__device__ __forceinline__ float threshold(const PeakState& s) {
-    if (s.count < s.n_peaks) return s.use_max ? -INFINITY : INFINITY;
-    return s.val[s.count - 1];
 }
 
 // peaks.rs:104-130: append (or replace the worst) and bubble toward the front.
@@ -71,38 +68,43 @@ __device__ void insert(PeakState& s, int64_t idx, float v) {
         s.idx[i - 1] = ti;
         i--;
     }
+    if (s.count == s.n_peaks) s.thr = s.val[s.count - 1];
 }
 
 // peaks.rs:134-140.
 __device__ __forceinline__ void promote(PeakState& s) {
-    if (s.has_cand && better(s.use_max, s.cand_val, threshold(s))) insert(s, s.cand_idx, s.cand_val);
+    if (s.has_cand && better(s.use_max, s.cand_val, s.thr)) insert(s, s.cand_idx, s.cand_val);
     s.has_cand = false;
 }
 
+// Dynamic shared memory: [kChunk int64 extrema indices][kChunk f32 values]
+// [n_peaks int64][n_peaks f32] (the best-first list).
 __global__ void __launch_bounds__(kPeakThreads)
     peaks_kernel(const float* __restrict__ pg, uint64_t flat_len, uint32_t n_peaks,
                  uint32_t min_distance, int use_max_i, int64_t* __restrict__ out_idx,
                  float* __restrict__ out_val) {
-    __shared__ int64_t ext_idx[kChunk];
-    __shared__ float ext_val[kChunk];
+    extern __shared__ __align__(16) unsigned char psmem[];
+    int64_t* ext_idx = reinterpret_cast<int64_t*>(psmem);
+    float* ext_val = reinterpret_cast<float*>(psmem + kChunk * 8);
+    int64_t* top_idx = reinterpret_cast<int64_t*>(psmem + kChunk * 12);
+    float* top_val = reinterpret_cast<float*>(psmem + kChunk * 12 + (size_t)n_peaks * 8);
     __shared__ uint32_t warp_tot[kPeakThreads / 32];
     __shared__ uint32_t chunk_count;
 
     const uint64_t c = blockIdx.x;
     const float* d = pg + c * flat_len;
     const bool use_max = use_max_i != 0;
-    int64_t* row_idx = out_idx + c * n_peaks;
-    float* row_val = out_val + c * n_peaks;
 
     PeakState s;
-    s.idx = row_idx;
-    s.val = row_val;
+    s.idx = top_idx;
+    s.val = top_val;
     s.count = 0;
     s.n_peaks = n_peaks;
     s.use_max = use_max;
     s.has_cand = false;
     s.cand_idx = -1;
     s.cand_val = use_max ? -INFINITY : INFINITY;
+    s.thr = use_max ? -INFINITY : INFINITY;
     const uint64_t md = min_distance;
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(kPeakThreads)
             }
         }
         __syncthreads();
-        // (3) replay.
+        // (3) replay (one thread; state in registers and shared memory).
         if (tid == 0) {
             const uint32_t ne = chunk_count;
             for (uint32_t e = 0; e < ne; e++) {
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(kPeakThreads)
                 if (s.has_cand && (uint64_t)s.cand_idx + (md > 0 ? md - 1 : 0) < (uint64_t)i)
                     promote(s);
                 // feed(i): peak test against the current threshold.
-                if (better(use_max, v, threshold(s)) &&
+                if (better(use_max, v, s.thr) &&
                     (!s.has_cand || better(use_max, v, s.cand_val))) {
                     s.cand_idx = i;
                     s.cand_val = v;
@@ -173,11 +175,14 @@ __global__ void __launch_bounds__(kPeakThreads)
         }
         __syncthreads();
     }
-    if (tid == 0) {
-        promote(s);  // finalize (peaks.rs:207-209)
-        for (uint32_t k = s.count; k < n_peaks; k++) {
-            row_idx[k] = -1;
-            row_val[k] = 0.0f;
+    if (tid == 0) promote(s);  // finalize (peaks.rs:207-209)
+    __syncthreads();
+    const uint32_t count = __shfl_sync(0xffffffffu, s.count, 0);
+    if (wid == 0) {
+        for (uint32_t k = lane; k < n_peaks; k += 32) {
+            const bool have = k < count;
+            out_idx[c * n_peaks + k] = have ? top_idx[k] : -1;
+            out_val[c * n_peaks + k] = have ? top_val[k] : 0.0f;
         }
     }
 }
@@ -188,7 +193,12 @@ cudaError_t launch_peaks(const float* pg, uint64_t n_curves, uint64_t flat_len,
                          uint32_t n_peaks, uint32_t min_distance, int use_max,
                          int64_t* out_idx, float* out_val, cudaStream_t stream) {
     if (n_curves == 0 || n_peaks == 0) return cudaSuccess;
-    peaks_kernel<<<(unsigned)n_curves, kPeakThreads, 0, stream>>>(
+    const size_t smem = (size_t)kChunk * 12 + (size_t)n_peaks * 12;
+    if (smem > 227u * 1024u) return cudaErrorInvalidValue;  // n_peaks > ~18000
+    cudaError_t e = cudaFuncSetAttribute(peaks_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    peaks_kernel<<<(unsigned)n_curves, kPeakThreads, smem, stream>>>(
         pg, flat_len, n_peaks, min_distance, use_max, out_idx, out_val);
     return cudaGetLastError();
 }

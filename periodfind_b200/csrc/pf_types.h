@@ -62,6 +62,7 @@ struct FoldParams {
     float phase_bin_size, mag_bin_size;
     const unsigned* tmax_bits;  // float bits of max |t| over the batch
     uint32_t edge_d;            // bin-edge guard (units of 2^-20 of a bin)
+    unsigned long long* stamps; // optional: [work item][start, end] globaltimer ns
 };
 
 // Shared-memory bytes of the chosen bin kernel (pf_bin.cuh).

@@ -389,3 +389,51 @@ def test_device_pointer_entry_points(gpu):
         done.record(st)
         done.synchronize()
         np.testing.assert_array_equal(out.cpu().numpy(), host)
+
+
+@pytest.mark.parametrize("algo,mode", [("ce", "chosen"), ("ce", "plain"), ("ls", "chosen")])
+def test_per_curve_device_timestamps(gpu, algo, mode):
+    """PF_TIMING records a start and end stamp per work item; the results are
+    unchanged and every curve gets a positive latency no longer than the
+    whole launch."""
+    torch = pytest.importorskip("torch")
+    import time
+
+    from periodfind_b200 import _native as nat
+
+    ts, ms = _ragged(seed=33, lengths=(20, 700, 64, 2000, 5))
+    if algo == "ce":
+        ms = [lc.normalize(m) for m in ms]
+    P, D = _grid(300, pdts=(0.0, 1e-4))
+    off = np.zeros(len(ts) + 1, np.int64)
+    np.cumsum([len(t) for t in ts], out=off[1:])
+    dt = torch.from_numpy(np.concatenate(ts)).cuda()
+    dm = torch.from_numpy(np.concatenate(ms)).cuda()
+    dp = torch.from_numpy(P).cuda()
+    dd = torch.from_numpy(D).cuda()
+    ctx = nat.default_context(0)
+    flags = nat.PF_MODE_CHOSEN if mode == "chosen" else nat.PF_MODE_PLAIN
+    outs = []
+    for extra in (0, nat.PF_TIMING):
+        out = torch.empty((len(ts), len(P), len(D)), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with ctx.lock:
+            args = (ctx.handle, dt.data_ptr(), dm.data_ptr(), off.ctypes.data, len(ts),
+                    dp.data_ptr(), len(P), dd.data_ptr(), len(D))
+            if algo == "ce":
+                ctx.check(ctx.lib.pf_ce_dev(*args, 10, 10, 1, 1, flags | extra,
+                                            out.data_ptr(), 0))
+            else:
+                ctx.check(ctx.lib.pf_ls_dev(*args, flags | extra, out.data_ptr(), 0))
+            torch.cuda.synchronize()
+            wall_ns = (time.perf_counter() - t0) * 1e9
+            if extra:
+                lat = np.zeros(len(ts))
+                ctx.check(ctx.lib.pf_curve_latency(ctx.handle, len(ts), lat.ctypes.data))
+                bad = np.zeros(len(ts) + 1)
+                assert ctx.lib.pf_curve_latency(ctx.handle, len(ts) + 1,
+                                                bad.ctypes.data) == nat.PF_EINVAL
+        outs.append(out.cpu().numpy())
+    np.testing.assert_array_equal(outs[0], outs[1])
+    assert np.all(lat > 0) and np.all(lat <= wall_ns), lat
