@@ -433,6 +433,175 @@ def ragged_arm(args):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------- LS derivatives and study
+
+
+def _seasonal_ls_batch(lengths, seed, baseline=3000.0):
+    """LS study curves: seasonal cadence over `baseline` days (240-day annual
+    gap), 15 + A sin(2 pi f t) + N(0, sigma^2) with A ~ U[0.01, 0.5],
+    sigma ~ U[0.01, 0.1], f ~ U[0.01, 20] / day; magnitudes centred.
+    Returns CSR (times, mags, offsets)."""
+    rng = np.random.default_rng(seed)
+    lengths = np.asarray(lengths, np.int64)
+    n_curves = len(lengths)
+    cid = np.repeat(np.arange(n_curves), lengths)
+    n_years = int(np.ceil(baseline / 365.25))
+    t = rng.integers(0, n_years, cid.size) * 365.25 + rng.uniform(0.0, 125.25, cid.size)
+    t = np.minimum(t, baseline)
+    t = t[np.lexsort((t, cid))].astype(np.float32)
+    amp = rng.uniform(0.01, 0.5, n_curves)[cid]
+    sig = rng.uniform(0.01, 0.1, n_curves)[cid]
+    f = rng.uniform(0.01, 20.0, n_curves)[cid]
+    ph = rng.uniform(0, 2 * np.pi, n_curves)[cid]
+    m = 15.0 + amp * np.sin(2 * np.pi * f * t.astype(np.float64) + ph)
+    m = m + rng.normal(0.0, 1.0, cid.size) * sig
+    off = np.zeros(n_curves + 1, np.int64)
+    np.cumsum(lengths, out=off[1:])
+    mean = np.add.reduceat(m, off[:-1]) / lengths
+    return t, (m - mean[cid]).astype(np.float32), off
+
+
+def _event_ms(torch, fn, reps, flush):
+    ts_ = []
+    for _ in range(reps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        ts_.append(e0.elapsed_time(e1))
+    return float(np.median(ts_))
+
+
+def lsgrad_arm(args):
+    """2000 curves x 2048 points over 3000 days; 20000 log-spaced frequencies
+    in [0.01, 20] / day.  Times the LS grid periodogram + top-32 peaks, the
+    autograd forward (power, dP/domega, coefficients) and backward
+    (dP/dy and dL/domega) over the grid, and 5 Newton steps on the top-32
+    peaks of every curve."""
+    import torch
+
+    from periodfind_b200 import _native as nat
+    from periodfind_b200 import ls_grad
+
+    torch.cuda.set_device(0)
+    n_curves, n_pts, n_freq = 2000, 2048, 20000
+    t, m, off = _seasonal_ls_batch(np.full(n_curves, n_pts), SEED + 4)
+    freqs = np.exp(np.linspace(np.log(0.01), np.log(20.0), n_freq))
+    periods = (1.0 / freqs[::-1]).astype(np.float32)
+    dev = "cuda"
+    d_t, d_m = torch.from_numpy(t).to(dev), torch.from_numpy(m).to(dev)
+    d_p = torch.from_numpy(periods).to(dev)
+    d_d = torch.zeros(1, dtype=torch.float32, device=dev)
+    pg = torch.empty((n_curves, n_freq), dtype=torch.float32, device=dev)
+    pk_i = torch.empty((n_curves, N_PEAKS), dtype=torch.int64, device=dev)
+    pk_v = torch.empty((n_curves, N_PEAKS), dtype=torch.float32, device=dev)
+    ctx = nat.default_context(0)
+    s = torch.cuda.current_stream().cuda_stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    reps = max(1, args.steps)
+
+    def grid_peaks():
+        ctx.check(ctx.lib.pf_ls_dev(ctx.handle, d_t.data_ptr(), d_m.data_ptr(), off.ctypes.data,
+                                    n_curves, d_p.data_ptr(), n_freq, d_d.data_ptr(), 1,
+                                    nat.PF_MODE_CHOSEN, pg.data_ptr(), s))
+        ctx.check(ctx.lib.pf_find_peaks_dev(ctx.handle, pg.data_ptr(), n_curves, n_freq, N_PEAKS,
+                                            1, 1, pk_i.data_ptr(), pk_v.data_ptr(), s))
+
+    w_grid = torch.from_numpy(2 * np.pi / periods.astype(np.float64)).to(dev)
+    y = d_m.clone().requires_grad_(True)
+    w = w_grid.clone().requires_grad_(True)
+    holder = {}
+
+    def forward():
+        holder["P"] = ls_grad.ls_power(d_t, y, w, off)
+
+    def backward():
+        holder["P"].backward(holder["g"])
+
+    grid_peaks()
+    forward()
+    holder["g"] = torch.ones_like(holder["P"])
+    backward()
+    torch.cuda.synchronize()
+    out = {"workload": f"LS derivatives: {n_curves} curves x {n_pts} points, seasonal cadence "
+                       f"3000 d, {n_freq} log-spaced frequencies [0.01, 20] / d, top-{N_PEAKS} "
+                       "peaks refined by 5 Newton steps"}
+    ev = n_curves * n_pts * n_freq
+    ms_grid = _event_ms(torch, grid_peaks, reps, flush)
+    ms_fwd = _event_ms(torch, forward, reps, flush)
+    ms_bwd = []
+    for _ in range(reps):
+        forward()
+        torch.cuda.synchronize()
+        ms_bwd.append(_event_ms(torch, backward, 1, flush))
+    ms_bwd = float(np.median(ms_bwd))
+    # Newton refinement of the grid peaks.
+    idx = pk_i.clamp(min=0)
+    wg = w_grid
+    w0 = wg[idx]
+    hw = torch.maximum((wg[(idx - 1).clamp(min=0)] - w0).abs(),
+                       (wg[(idx + 1).clamp(max=n_freq - 1)] - w0).abs()).contiguous()
+    w0 = w0.contiguous()
+
+    def refine():
+        holder["ref"] = ls_grad.refine_peaks(d_t, d_m, w0, hw, off, n_steps=5)
+
+    refine()
+    ms_ref = _event_ms(torch, refine, reps, flush)
+    ev_ref = n_curves * n_pts * N_PEAKS * 6
+    out["grid_periodogram_peaks"] = {"ms": ms_grid, "evals_per_s": ev / (ms_grid * 1e-3)}
+    out["autograd_forward"] = {"ms": ms_fwd, "evals_per_s": ev / (ms_fwd * 1e-3)}
+    out["autograd_backward"] = {"ms": ms_bwd, "evals_per_s": ev / (ms_bwd * 1e-3)}
+    out["newton_refine_5_steps"] = {"ms": ms_ref, "evals_per_s": ev_ref / (ms_ref * 1e-3),
+                                    "peaks": n_curves * N_PEAKS}
+    print(json.dumps(out), flush=True)
+
+
+def precision_arm(args):
+    """10000 curves, lengths log-uniform in [64, 16384], seasonal cadence over
+    3000 days; 50000 frequencies uniform in [0.01, 20] / day.  Times the LS
+    periodogram with each fold: plain (the reference's FP64-divide fold),
+    chosen split-precision, chosen exact, and the all-FP32 fold."""
+    import torch
+
+    from periodfind_b200 import _native as nat
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(SEED + 3)
+    n_curves = args.curves if args.curves != N_CURVES else 10000
+    lengths = np.exp(rng.uniform(np.log(64), np.log(16384), n_curves)).astype(np.int64)
+    t, m, off = _seasonal_ls_batch(lengths, SEED + 3)
+    n_freq = 50000
+    periods = (1.0 / np.linspace(0.01, 20.0, n_freq)[::-1]).astype(np.float32)
+    dev = "cuda"
+    d_t, d_m = torch.from_numpy(t).to(dev), torch.from_numpy(m).to(dev)
+    d_p = torch.from_numpy(periods).to(dev)
+    d_d = torch.zeros(1, dtype=torch.float32, device=dev)
+    pg = torch.empty((n_curves, n_freq), dtype=torch.float32, device=dev)
+    ctx = nat.default_context(0)
+    s = torch.cuda.current_stream().cuda_stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ev = int(lengths.sum()) * n_freq
+    out = {"workload": f"LS precision study: {n_curves} curves, lengths log-uniform [64, 16384] "
+                       f"(mean {lengths.mean():.0f}), seasonal cadence 3000 d, {n_freq} "
+                       "frequencies uniform in [0.01, 20] / d", "evals": ev, "folds": {}}
+    for name, flags in (("plain (reference fold)", nat.PF_MODE_PLAIN),
+                        ("chosen split-precision", nat.PF_MODE_CHOSEN),
+                        ("chosen exact", nat.PF_MODE_CHOSEN | nat.PF_FOLD_EXACT),
+                        ("all-FP32", nat.PF_MODE_CHOSEN | nat.PF_FOLD_F32)):
+        def run(flags=flags):
+            ctx.check(ctx.lib.pf_ls_dev(ctx.handle, d_t.data_ptr(), d_m.data_ptr(),
+                                        off.ctypes.data, n_curves, d_p.data_ptr(), n_freq,
+                                        d_d.data_ptr(), 1, flags, pg.data_ptr(), s))
+        run()
+        ms_ = _event_ms(torch, run, max(1, args.steps), flush)
+        out["folds"][name] = {"ms": ms_, "evals_per_s": ev / (ms_ * 1e-3)}
+    print(json.dumps(out), flush=True)
+
+
 # ------------------------------------------------------------------- main
 
 
@@ -444,14 +613,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--curves", type=int, default=N_CURVES)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--workload", default="batch", choices=["batch", "ragged"],
-                    help="'ragged': the mixed ragged batch (separate report, 1 GPU)")
+    ap.add_argument("--workload", default="batch",
+                    choices=["batch", "ragged", "lsgrad", "precision"],
+                    help="'ragged': the mixed ragged batch; 'lsgrad': LS derivatives and "
+                         "Newton refinement; 'precision': LS folds on the precision-study "
+                         "batch (separate reports, 1 GPU)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
         return
-    if args.workload == "ragged":
-        ragged_arm(args)
+    if args.workload != "batch":
+        {"ragged": ragged_arm, "lsgrad": lsgrad_arm, "precision": precision_arm}[args.workload](args)
         return
 
     import torch

@@ -27,8 +27,9 @@
  *                  a divide (bit-identical), bins from FP64/integer ops with
  *                  the reference's exact sequence near bin edges (identical
  *                  bin occupancies), 16-bit CE counters, exact fixed-point
- *                  AOV sums.  LS: split-precision FP32 phase (more accurate
- *                  than the reference's f32-rounded phase).
+ *                  AOV sums.  LS: split-precision FP32 phase, no FP64 per
+ *                  point, with the error bound of the reference's FP64 fold
+ *                  (the f32 rounding of the phase, <= 2^-25 turns).
  *  PF_SEM_CPU      arithmetic of the reference's CPU (Rust) path: IEEE
  *                  divides, no multiply-add contraction, accurate libm-style
  *                  log/sin/cos.  Without it the arithmetic follows the
@@ -198,6 +199,56 @@ int pf_ls_peaks_dev_noalloc(const float* d_times, const float* d_mags,
  * c's periodogram; n_curves must be that launch's.  Synchronises the
  * stream that launch ran on. */
 int pf_curve_latency(pf_ctx* ctx, uint64_t n_curves, double* out_ns);
+
+/* Folded phase of every (period, time) pair as the fold kernels compute it,
+ * for precision studies (no counterpart in the reference):
+ * d_out[p * n + i] for device arrays d_times[n], d_periods[n_per].  mode
+ * selects the fold: 0 = the reference's expression (periodfind/cuda/
+ * ce.cu:140-143), PF_FOLD_EXACT, PF_FOLD_DF (turns in [-1, 1]) or PF_FOLD_F32;
+ * PF_SEM_CPU selects the CPU-semantics build of it. */
+int pf_fold_phase_dev(pf_ctx* ctx, int mode, const float* d_times, uint64_t n,
+                      const float* d_periods, uint64_t n_per, float period_dt, float* d_out,
+                      void* stream);
+
+/* ---- Lomb-Scargle derivatives (no counterpart in the reference) ----------
+ * The reference evaluates the LS power on the trial grid only
+ * (periodfind/cuda/ls.cu:75-136).  These calls evaluate the same power at
+ * arbitrary ANGULAR frequencies omega (radians per time unit; omega = 2 pi /
+ * period) with its derivatives, for gradient-based use and for refining
+ * peaks off the grid.  Inputs are CSR device arrays as in pf_ls_dev (host
+ * offsets, device times / magnitudes); omega[c * omega_stride + k] (FP64,
+ * stride 0 = one grid for all curves).  Outputs are [n_curves][n_freq].
+ * Work is enqueued on `stream` (NULL = default stream).
+ *
+ * pf_ls_eval_dev: power, and where non-NULL dP/domega, d2P/domega2 and the
+ * least-squares coefficients coef[2 * cell + {0, 1}] = (alpha, beta), with
+ * dP/dy_i = alpha cos(omega (t_i - t0)) + beta sin(omega (t_i - t0)) and t0
+ * the midpoint of the curve's time span. */
+int pf_ls_eval_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
+                   const int64_t* offsets, uint64_t n_curves, const double* d_omega,
+                   uint64_t omega_stride, uint64_t n_freq, float* d_power, float* d_dpdw,
+                   float* d_d2pdw2, float* d_coef, void* stream);
+
+/* Backward of pf_ls_eval_dev for an upstream gradient g = dL/dpower
+ * ([n_curves][n_freq]), from the forward's d_dpdw and d_coef:
+ * d_grad_omega[cell] = g * dP/domega (NULL: skipped; needs d_dpdw) and
+ * d_grad_mags[i] = sum_k g_k dP_k/dy_i over the curve's frequencies (NULL:
+ * skipped). */
+int pf_ls_backward_dev(pf_ctx* ctx, const float* d_times, const int64_t* offsets,
+                       uint64_t n_curves, const double* d_omega, uint64_t omega_stride,
+                       uint64_t n_freq, const float* d_grad_power, const float* d_dpdw,
+                       const float* d_coef, double* d_grad_omega, float* d_grad_mags,
+                       void* stream);
+
+/* Newton refinement of LS maxima: for each (curve, k), starting at
+ * d_omega0[c * n_freq + k], up to n_steps (<= 64) safeguarded Newton steps on
+ * dP/domega inside [omega0 - h, omega0 + h] (h = d_half_width[cell]); writes
+ * the best evaluated frequency to d_omega (may alias d_omega0) and its power
+ * to d_power. */
+int pf_ls_refine_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
+                     const int64_t* offsets, uint64_t n_curves, const double* d_omega0,
+                     const double* d_half_width, uint64_t n_freq, uint32_t n_steps,
+                     double* d_omega, float* d_power, void* stream);
 
 /* Number of kernels this context has launched since creation (telemetry
  * for benchmarks: launches of the library's own kernels only). */

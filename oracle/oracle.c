@@ -465,6 +465,166 @@ ORC_API void orc_phase_f64(const float* times, int64_t n, const double* periods,
     }
 }
 
+/* ------------------------------------------------------ LS derivatives */
+
+/* The LS power as a function of angular frequency w, with its first and
+ * second w-derivatives, in FP64.  No counterpart in the reference (which
+ * evaluates the power on the trial grid only, rust/src/ls.rs:231-276); the
+ * power itself equals orc_ls_cell_f64 (the reference's tau expression,
+ * ls.rs:253-275) because tau only diagonalises the 2x2 normal matrix:
+ *   P = 0.5 v^T M^-1 v,  v = (C, S),  M = [[CC, CS], [CS, SS]],  w = M^-1 v.
+ * Times are measured from the midpoint t0 of the curve's time span, the
+ * convention under which (alpha, beta) = M^-1 v are reported. */
+static double ls_t0(const float* t, uint64_t n) {
+    if (n == 0) return 0.0;
+    float lo = t[0], hi = t[0];
+    for (uint64_t i = 1; i < n; i++) {
+        if (t[i] < lo) lo = t[i];
+        if (t[i] > hi) hi = t[i];
+    }
+    return 0.5 * ((double)lo + (double)hi);
+}
+
+static void ls_deriv_cell_f64(const float* t, const float* y, uint64_t n, double w,
+                              double out[5]) {
+    const double t0 = ls_t0(t, n);
+    double C = 0, S = 0, CC = 0, CS = 0, C1 = 0, S1 = 0, CC1 = 0, CS1 = 0;
+    double C2 = 0, S2 = 0, CC2 = 0, CS2 = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        const double x = (double)t[i] - t0, yy = (double)y[i];
+        const double th = w * x;
+        const double s = sin(th), c = cos(th);
+        const double s2 = sin(2.0 * th), c2 = cos(2.0 * th);
+        C += yy * c;
+        S += yy * s;
+        CC += c * c;
+        CS += c * s;
+        C1 -= yy * x * s;
+        S1 += yy * x * c;
+        CC1 -= x * s2;
+        CS1 += x * c2;
+        C2 -= yy * x * x * c;
+        S2 -= yy * x * x * s;
+        CC2 -= 2.0 * x * x * c2;
+        CS2 -= 2.0 * x * x * s2;
+    }
+    const double SS = (double)n - CC;
+    const double det = CC * SS - CS * CS;
+    for (int k = 0; k < 5; k++) out[k] = 0.0;
+    if (!(det > 1e-6 * CC * SS)) return; /* singular M: power 0, as the device */
+    const double al = (SS * C - CS * S) / det, be = (CC * S - CS * C) / det;
+    const double u0 = C1 - (CC1 * al + CS1 * be), u1 = S1 - (CS1 * al - CC1 * be);
+    out[0] = 0.5 * (al * C + be * S);
+    out[1] = al * C1 + be * S1 - 0.5 * ((al * al - be * be) * CC1 + 2.0 * al * be * CS1);
+    out[2] = (SS * u0 * u0 - 2.0 * CS * u0 * u1 + CC * u1 * u1) / det + al * C2 + be * S2 -
+             0.5 * ((al * al - be * be) * CC2 + 2.0 * al * be * CS2);
+    out[3] = al;
+    out[4] = be;
+}
+
+/* out[cell * 5 + {0..4}] = (P, dP/dw, d2P/dw2, alpha, beta) for
+ * w = omega[c * omega_stride + k]. */
+ORC_API void orc_ls_derivs_f64(const float* times, const float* mags, const int64_t* offsets,
+                               int64_t n_curves, const double* omega, int64_t omega_stride,
+                               int64_t n_freq, int n_threads, double* out) {
+    set_threads(n_threads);
+    const int64_t total = n_curves * n_freq;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t cell = 0; cell < total; cell++) {
+        const int64_t c = cell / n_freq, k = cell % n_freq;
+        const int64_t o = offsets[c];
+        ls_deriv_cell_f64(times + o, mags + o, (uint64_t)(offsets[c + 1] - o),
+                          omega[c * omega_stride + k], out + 5 * cell);
+    }
+}
+
+/* dL/dy_i = sum_k (g alpha)_k cos(w_k (t_i - t0)) + (g beta)_k sin(...),
+ * gcoef[cell * 2 + {0, 1}] = upstream gradient times (alpha, beta). */
+ORC_API void orc_ls_grad_mags_f64(const float* times, const int64_t* offsets, int64_t n_curves,
+                                  const double* omega, int64_t omega_stride, int64_t n_freq,
+                                  const double* gcoef, int n_threads, double* out) {
+    set_threads(n_threads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t c = 0; c < n_curves; c++) {
+        const int64_t o = offsets[c];
+        const uint64_t n = (uint64_t)(offsets[c + 1] - o);
+        const double t0 = ls_t0(times + o, n);
+        for (uint64_t i = 0; i < n; i++) {
+            const double x = (double)times[o + i] - t0;
+            double acc = 0.0;
+            for (int64_t k = 0; k < n_freq; k++) {
+                const double th = omega[c * omega_stride + k] * x;
+                acc += gcoef[2 * (c * n_freq + k)] * cos(th) +
+                       gcoef[2 * (c * n_freq + k) + 1] * sin(th);
+            }
+            out[o + i] = acc;
+        }
+    }
+}
+
+/* Safeguarded Newton toward the LS maximum, the control flow the device
+ * refinement follows: n_steps updates inside [w0 - h, w0 + h]; Newton where
+ * d2P/dw2 < 0, else a quarter-bracket step uphill; n_steps + 1 evaluations.
+ * The last iterate is returned unless its power is more than 1e-5 (relative)
+ * below the best evaluated one, which is returned then. */
+ORC_API void orc_ls_refine_f64(const float* times, const float* mags, const int64_t* offsets,
+                               int64_t n_curves, const double* omega0,
+                               const double* half_width, int64_t n_freq, int n_steps,
+                               int n_threads, double* omega_out, double* power_out) {
+    set_threads(n_threads);
+    const int64_t total = n_curves * n_freq;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t cell = 0; cell < total; cell++) {
+        const int64_t c = cell / n_freq;
+        const int64_t o = offsets[c];
+        const uint64_t n = (uint64_t)(offsets[c + 1] - o);
+        double w = omega0[cell];
+        const double hw = half_width[cell], lo = w - hw, hi = w + hw;
+        double best_w = w, best_p = -1.0, last_w = w, last_p = -1.0;
+        for (int e = 0; e <= n_steps; e++) {
+            double d[5];
+            ls_deriv_cell_f64(times + o, mags + o, n, w, d);
+            last_p = d[0];
+            last_w = w;
+            if (d[0] > best_p) {
+                best_p = d[0];
+                best_w = w;
+            }
+            if (e < n_steps) {
+                double step = (d[2] < 0.0) ? -d[1] / d[2] : ((d[1] > 0.0) ? 0.25 * hw : -0.25 * hw);
+                w = fmin(fmax(w + step, lo), hi);
+            }
+        }
+        /* the last iterate unless its power is clearly below the best */
+        const int keep_last = last_p >= best_p * (1.0 - 1e-5);
+        omega_out[cell] = keep_last ? last_w : best_w;
+        const double pw = keep_last ? last_p : best_p;
+        power_out[cell] = pw > 0.0 ? pw : 0.0;
+    }
+}
+
+/* The reference's tau expression (rust/src/ls.rs:253-275) in FP64 with FP64
+ * magnitudes, at angular frequency w: the target of finite-difference
+ * gradient checks. */
+ORC_API double orc_ls_power_tau_f64(const double* t, const double* y, int64_t n, double w) {
+    double mc = 0, ms = 0, cc = 0, cs = 0;
+    for (int64_t i = 0; i < n; i++) {
+        const double s = sin(w * t[i]), c = cos(w * t[i]);
+        mc += y[i] * c;
+        ms += y[i] * s;
+        cc += c * c;
+        cs += c * s;
+    }
+    const double ss = (double)n - cc;
+    const double tau = 0.5 * atan2(2.0 * cs, cc - ss);
+    const double st = sin(tau), ct = cos(tau);
+    const double a = ct * mc + st * ms, b = ct * ms - st * mc;
+    const double dl = ct * ct * cc + 2.0 * ct * st * cs + st * st * ss;
+    const double dr = ct * ct * ss - 2.0 * ct * st * cs + st * st * cc;
+    if (dl == 0.0 || dr == 0.0) return 0.0;
+    return 0.5 * (a * a / dl + b * b / dr);
+}
+
 /* ---------------------------------------------------------------- peaks */
 
 /* Streaming greedy top-N peak finder, rust/src/peaks.rs:18-218, applied in

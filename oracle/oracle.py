@@ -70,6 +70,13 @@ def _load():
     lib.orc_find_top_peaks.restype = i64
     lib.orc_find_top_peaks_batched.argtypes = [_f32p, i64, i64, i64, i64, c_int, c_int,
                                                _i64p, _f32p]
+    lib.orc_ls_derivs_f64.argtypes = [_f32p, _f32p, _i64p, i64, _f64p, i64, i64, c_int, _f64p]
+    lib.orc_ls_grad_mags_f64.argtypes = [_f32p, _i64p, i64, _f64p, i64, i64, _f64p, c_int,
+                                         _f64p]
+    lib.orc_ls_refine_f64.argtypes = [_f32p, _f32p, _i64p, i64, _f64p, _f64p, i64, c_int,
+                                      c_int, _f64p, _f64p]
+    lib.orc_ls_power_tau_f64.argtypes = [_f64p, _f64p, i64, ctypes.c_double]
+    lib.orc_ls_power_tau_f64.restype = ctypes.c_double
     _lib = lib
     return lib
 
@@ -172,6 +179,69 @@ def phase_f64(times, periods, period_dt=0.0, n_threads=0):
     lib.orc_phase_f64(_ptr(t, _f32p), len(t), _ptr(p, _f64p), len(p), float(period_dt),
                       n_threads, _ptr(out, _f64p))
     return out
+
+
+def _omega_arg(omega, n_curves):
+    """(contiguous float64 omega, stride): [n_freq] -> stride 0, [n_curves, n_freq] -> n_freq."""
+    w = np.ascontiguousarray(omega, dtype=np.float64)
+    if w.ndim == 1:
+        return w, 0, len(w)
+    if w.ndim != 2 or w.shape[0] != n_curves:
+        raise ValueError("omega must be [n_freq] or [n_curves, n_freq]")
+    return w, w.shape[1], w.shape[1]
+
+
+def ls_derivs_f64(times, mags, omega, n_threads=0):
+    """FP64 LS power and omega-derivatives at angular frequencies `omega`
+    ([n_freq] shared, or [n_curves, n_freq]).  Returns an array
+    [n_curves, n_freq, 5] of (P, dP/dw, d2P/dw2, alpha, beta), times measured
+    from the midpoint of each curve's time span."""
+    lib = _load()
+    t, m, off = pack(times, mags)
+    n_curves = len(off) - 1
+    w, stride, K = _omega_arg(omega, n_curves)
+    out = np.zeros((n_curves, K, 5), np.float64)
+    lib.orc_ls_derivs_f64(_ptr(t, _f32p), _ptr(m, _f32p), _ptr(off, _i64p), n_curves,
+                          _ptr(w, _f64p), stride, K, n_threads, _ptr(out, _f64p))
+    return out
+
+
+def ls_grad_mags_f64(times, omega, gcoef, n_threads=0):
+    """dL/dy for upstream-weighted coefficients gcoef [n_curves, n_freq, 2]
+    (g * alpha, g * beta); returns the concatenated per-point gradient."""
+    lib = _load()
+    t, _, off = pack(times, times)
+    n_curves = len(off) - 1
+    w, stride, K = _omega_arg(omega, n_curves)
+    g = np.ascontiguousarray(gcoef, dtype=np.float64)
+    out = np.zeros(len(t), np.float64)
+    lib.orc_ls_grad_mags_f64(_ptr(t, _f32p), _ptr(off, _i64p), n_curves, _ptr(w, _f64p),
+                             stride, K, _ptr(g, _f64p), n_threads, _ptr(out, _f64p))
+    return out
+
+
+def ls_refine_f64(times, mags, omega0, half_width, n_steps=5, n_threads=0):
+    """FP64 safeguarded Newton refinement of LS maxima from omega0
+    [n_curves, K] within +-half_width; returns (omega, power), each [n_curves, K]."""
+    lib = _load()
+    t, m, off = pack(times, mags)
+    n_curves = len(off) - 1
+    w0 = np.ascontiguousarray(omega0, dtype=np.float64).reshape(n_curves, -1)
+    hw = np.ascontiguousarray(half_width, dtype=np.float64).reshape(w0.shape)
+    w = np.zeros_like(w0)
+    p = np.zeros_like(w0)
+    lib.orc_ls_refine_f64(_ptr(t, _f32p), _ptr(m, _f32p), _ptr(off, _i64p), n_curves,
+                          _ptr(w0, _f64p), _ptr(hw, _f64p), w0.shape[1], int(n_steps),
+                          n_threads, _ptr(w, _f64p), _ptr(p, _f64p))
+    return w, p
+
+
+def ls_power_tau_f64(t, y, omega):
+    """The reference's tau expression in FP64 (FP64 times and magnitudes)."""
+    lib = _load()
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    return lib.orc_ls_power_tau_f64(_ptr(t, _f64p), _ptr(y, _f64p), len(t), float(omega))
 
 
 def ce_counts(t, m, period, pdt, n_phase=10, n_mag=10, po=1, mo=1, fused_tcorr=False):

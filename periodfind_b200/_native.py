@@ -61,6 +61,12 @@ SIGNATURES = {
     "pf_ls_peaks_dev_noalloc": ([_vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int,
                                  _vp, _vp, _vp, ctypes.c_char_p, _u64], _int),
     "pf_curve_latency": ([_vp, _u64, _vp], _int),
+    "pf_fold_phase_dev": ([_vp, _int, _vp, _u64, _vp, _u64, ctypes.c_float, _vp, _vp], _int),
+    "pf_ls_eval_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _u64, _vp, _vp, _vp, _vp, _vp],
+                       _int),
+    "pf_ls_backward_dev": ([_vp, _vp, _vp, _u64, _vp, _u64, _u64, _vp, _vp, _vp, _vp, _vp,
+                            _vp], _int),
+    "pf_ls_refine_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _vp, _u64, _u32, _vp, _vp, _vp], _int),
     "pf_launch_count": ([_vp], _u64),
     "pf_last_kernel_ms": ([_vp], ctypes.c_double),
 }

@@ -35,6 +35,7 @@ UNITS = {
     "pf_peaks.cu": [],
     "pf_api.cu": [],
     "pf_noalloc.cu": [],
+    "pf_lsgrad.cu": [],
 }
 
 LIB = os.path.join(HERE, "libpfb200.so")

@@ -624,6 +624,45 @@ int run_dev(pf_ctx* ctx, const Job& j, const float* d_times, const float* d_mags
     return PF_OK;
 }
 
+// Copy a host CSR offsets array into the context's device metadata block,
+// ordered after the previous device-pointer call on this context, on stream
+// s.  Returns the device copy and the longest curve.
+int stage_offsets(pf_ctx* ctx, const int64_t* offsets, uint64_t n_curves, cudaStream_t s,
+                  const int64_t** d_off, uint32_t* max_len) {
+    if (!offsets) return fail(ctx, PF_EINVAL, "offsets is NULL");
+    uint64_t mx = 0;
+    for (uint64_t c = 0; c < n_curves; c++) {
+        if (offsets[c + 1] < offsets[c] || offsets[c] < 0)
+            return fail(ctx, PF_EINVAL, "offsets must be non-decreasing and non-negative");
+        mx = std::max(mx, (uint64_t)(offsets[c + 1] - offsets[c]));
+    }
+    if (mx > 0xFFFFFFFFull) return fail(ctx, PF_EINVAL, "a curve has more than 2^32-1 points");
+    const size_t bytes = (size_t)(n_curves + 1) * 8;
+    int rc;
+    if ((rc = staging_ready(ctx)) != PF_OK) return rc;
+    if ((rc = ensure_pinned(ctx, ctx->h_in, bytes)) != PF_OK) return rc;
+    if (ctx->done_recorded) PF_CUDA(cudaStreamWaitEvent(s, ctx->ev_done, 0), "stream wait");
+    if ((rc = ensure_dev(ctx, ctx->d_in, bytes)) != PF_OK) return rc;
+    memcpy(ctx->h_in.p, offsets, bytes);
+    PF_CUDA(cudaMemcpyAsync(ctx->d_in.p, ctx->h_in.p, bytes, cudaMemcpyHostToDevice, s),
+            "H2D offsets");
+    PF_CUDA(cudaEventRecord(ctx->ev_staged, s), "event");
+    ctx->staged_pending = true;
+    *d_off = (const int64_t*)ctx->d_in.p;
+    *max_len = (uint32_t)mx;
+    return PF_OK;
+}
+
+int ls_common_checks(pf_ctx* ctx, const float* d_times, const int64_t* offsets,
+                     uint64_t n_curves, const void* d_omega, uint64_t n_freq) {
+    if (!ctx) return PF_EINVAL;
+    if (n_curves == 0 || n_freq == 0) return PF_OK;
+    if (!offsets) return fail(ctx, PF_EINVAL, "offsets is NULL");
+    if (!d_omega) return fail(ctx, PF_EINVAL, "omega is NULL");
+    if (offsets[n_curves] > offsets[0] && !d_times) return fail(ctx, PF_EINVAL, "d_times is NULL");
+    return PF_OK;
+}
+
 }  // namespace
 
 size_t pfk::fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag) {
@@ -724,6 +763,129 @@ int pf_curve_latency(pf_ctx* ctx, uint64_t n_curves, double* out_ns) {
     }
     for (uint64_t c = 0; c < n_curves; c++)
         out_ns[c] = (hi[c] > lo[c] && lo[c] != ~0ull) ? (double)(hi[c] - lo[c]) : 0.0;
+    return PF_OK;
+}
+
+int pf_ls_eval_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
+                   const int64_t* offsets, uint64_t n_curves, const double* d_omega,
+                   uint64_t omega_stride, uint64_t n_freq, float* d_power, float* d_dpdw,
+                   float* d_d2pdw2, float* d_coef, void* stream) {
+    int rc = ls_common_checks(ctx, d_times, offsets, n_curves, d_omega, n_freq);
+    if (rc != PF_OK || n_curves == 0 || n_freq == 0) return rc;
+    if (!d_power) return fail(ctx, PF_EINVAL, "d_power is NULL");
+    if (offsets[n_curves] > offsets[0] && !d_mags) return fail(ctx, PF_EINVAL, "d_mags is NULL");
+    if (omega_stride != 0 && omega_stride < n_freq)
+        return fail(ctx, PF_EINVAL, "omega_stride must be 0 or >= n_freq");
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    LsEvalParams p;
+    uint32_t max_len = 0;
+    if ((rc = stage_offsets(ctx, offsets, n_curves, s, &p.off, &max_len)) != PF_OK) return rc;
+    p.t = d_times;
+    p.y = d_mags;
+    p.n_curves = n_curves;
+    p.omega = d_omega;
+    p.omega_stride = omega_stride;
+    p.n_freq = n_freq;
+    p.power = d_power;
+    p.dpdw = d_dpdw;
+    p.d2pdw2 = d_d2pdw2;
+    p.coef = d_coef;
+    const int order = d_d2pdw2 ? 2 : (d_dpdw ? 1 : 0);
+    PF_CUDA(launch_ls_eval(p, order, s), "LS derivative kernel");
+    ctx->launches++;
+    PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
+    ctx->done_recorded = true;
+    return PF_OK;
+}
+
+int pf_ls_backward_dev(pf_ctx* ctx, const float* d_times, const int64_t* offsets,
+                       uint64_t n_curves, const double* d_omega, uint64_t omega_stride,
+                       uint64_t n_freq, const float* d_grad_power, const float* d_dpdw,
+                       const float* d_coef, double* d_grad_omega, float* d_grad_mags,
+                       void* stream) {
+    int rc = ls_common_checks(ctx, d_times, offsets, n_curves, d_omega, n_freq);
+    if (rc != PF_OK || n_curves == 0 || n_freq == 0) return rc;
+    if (!d_grad_power || !d_coef) return fail(ctx, PF_EINVAL, "d_grad_power/d_coef is NULL");
+    if (d_grad_omega && !d_dpdw) return fail(ctx, PF_EINVAL, "d_grad_omega needs d_dpdw");
+    if (omega_stride != 0 && omega_stride < n_freq)
+        return fail(ctx, PF_EINVAL, "omega_stride must be 0 or >= n_freq");
+    if (!d_grad_omega && !d_grad_mags) return PF_OK;
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    LsGradParams p;
+    uint32_t max_len = 0;
+    if ((rc = stage_offsets(ctx, offsets, n_curves, s, &p.off, &max_len)) != PF_OK) return rc;
+    p.t = d_times;
+    p.n_curves = n_curves;
+    p.omega = d_omega;
+    p.omega_stride = omega_stride;
+    p.n_freq = n_freq;
+    p.grad_power = d_grad_power;
+    p.dpdw = d_dpdw;
+    p.coef = d_coef;
+    p.grad_omega = d_grad_omega;
+    p.grad_mags = d_grad_mags;
+    PF_CUDA(launch_ls_grad(p, max_len, s), "LS backward kernel");
+    ctx->launches++;
+    PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
+    ctx->done_recorded = true;
+    return PF_OK;
+}
+
+int pf_ls_refine_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
+                     const int64_t* offsets, uint64_t n_curves, const double* d_omega0,
+                     const double* d_half_width, uint64_t n_freq, uint32_t n_steps,
+                     double* d_omega, float* d_power, void* stream) {
+    int rc = ls_common_checks(ctx, d_times, offsets, n_curves, d_omega0, n_freq);
+    if (rc != PF_OK || n_curves == 0 || n_freq == 0) return rc;
+    if (!d_half_width || !d_omega || !d_power)
+        return fail(ctx, PF_EINVAL, "d_half_width/d_omega/d_power is NULL");
+    if (offsets[n_curves] > offsets[0] && !d_mags) return fail(ctx, PF_EINVAL, "d_mags is NULL");
+    if (n_steps > 64) return fail(ctx, PF_EINVAL, "n_steps must be <= 64");
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    LsEvalParams p;
+    uint32_t max_len = 0;
+    if ((rc = stage_offsets(ctx, offsets, n_curves, s, &p.off, &max_len)) != PF_OK) return rc;
+    p.t = d_times;
+    p.y = d_mags;
+    p.n_curves = n_curves;
+    p.omega = d_omega0;
+    p.omega_stride = n_freq;
+    p.n_freq = n_freq;
+    p.power = d_power;
+    p.half_width = d_half_width;
+    p.n_steps = n_steps;
+    p.omega_out = d_omega;
+    PF_CUDA(launch_ls_refine(p, s), "LS Newton refinement kernel");
+    ctx->launches++;
+    PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
+    ctx->done_recorded = true;
+    return PF_OK;
+}
+
+int pf_fold_phase_dev(pf_ctx* ctx, int mode, const float* d_times, uint64_t n,
+                      const float* d_periods, uint64_t n_per, float period_dt, float* d_out,
+                      void* stream) {
+    if (!ctx) return PF_EINVAL;
+    if (n == 0 || n_per == 0) return PF_OK;
+    if (!d_times || !d_periods || !d_out) return fail(ctx, PF_EINVAL, "NULL pointer argument");
+    const int f = mode & (PF_FOLD_F32 | PF_FOLD_DF | PF_FOLD_EXACT);
+    int fold;
+    if (f == 0) fold = FOLD_REF;
+    else if (f == PF_FOLD_F32) fold = FOLD_F32;
+    else if (f == PF_FOLD_DF) fold = FOLD_DF;
+    else if (f == PF_FOLD_EXACT) fold = FOLD_EXACT;
+    else return fail(ctx, PF_EINVAL, "at most one of PF_FOLD_F32 / PF_FOLD_DF / PF_FOLD_EXACT");
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    PF_CUDA(use_cpu_semantics(mode)
+                ? launch_phase_probe_cpusem(fold, d_times, n, d_periods, n_per, period_dt, d_out, s)
+                : launch_phase_probe_cudasem(fold, d_times, n, d_periods, n_per, period_dt, d_out,
+                                             s),
+            "phase probe kernel");
+    ctx->launches++;
     return PF_OK;
 }
 

@@ -118,8 +118,10 @@ __device__ __forceinline__ float fold_f32(float t, const Cell& s) {
 // g = pdt_corr / P as float pairs).  Each product is carried as a rounded
 // float plus its exact rounding error (fma), the integer part is removed
 // from the rounded float (exact for |x| < 2^22, checked per CTA), and the
-// small terms are added last: phase error ~1e-10 cycles at 6e4 cycles of
-// baseline.  Result in turns, within [-1, 1].
+// small terms are added last.  Before the final rounding the phase is good
+// to ~1e-10 turns at 6e4 cycles of baseline; the f32 result is then within
+// half an ulp of it (at most 2^-25 turns), the same bound as the reference's
+// FP64 fold rounded to f32.  Result in turns, within [-1, 1].
 __device__ __forceinline__ float rint_small(float x) {
     return __fsub_rn(__fadd_rn(x, 12582912.0f), 12582912.0f);  // |x| < 2^22
 }
@@ -554,6 +556,35 @@ __global__ void ce_magbin_kernel(const float* __restrict__ m, uint32_t* __restri
             if (flag_saturated && mb == ~0ull) v |= 0x80000000u;
         }
         aux[cd.off + i] = v;
+    }
+}
+
+// Folded phase of each (period, time) pair with one fold variant, as the
+// fold kernels compute it (precision studies): out[p * n + i].  FOLD_DF
+// returns turns in [-1, 1]; the others [0, 1].
+template <int FOLD>
+__global__ void phase_probe_kernel(const float* __restrict__ t, uint64_t n,
+                                   const float* __restrict__ periods, uint64_t n_per,
+                                   float period_dt, float* __restrict__ out) {
+    const uint64_t total = n * n_per;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t pi = k / n, i = k % n;
+        Cell s;
+        cell_setup<FOLD>(s, periods[pi], period_dt);
+        const float ti = t[i];
+        float ph;
+        if constexpr (FOLD == FOLD_REF) {
+            ph = fold_ref(ti, s);
+        } else if constexpr (FOLD == FOLD_EXACT) {
+            ph = (period_dt != 0.0f) ? fold_exact<true>((double)ti, s)
+                                     : fold_exact<false>((double)ti, s);
+        } else if constexpr (FOLD == FOLD_F32) {
+            ph = fold_f32(ti, s);
+        } else {
+            ph = (period_dt != 0.0f) ? fold_df<true>(ti, s) : fold_df<false>(ti, s);
+        }
+        out[k] = ph;
     }
 }
 

@@ -42,6 +42,15 @@ cudaError_t launch_binaux_cpusem(const float* m, void* aux, const CurveDesc* cur
                                  uint32_t n_curves, uint32_t n_mag, float mag_bin_size,
                                  int block, int cnt16, cudaStream_t s);
 
+// Folded phase of every (period, time) pair with one fold variant
+// (FOLD_REF / FOLD_EXACT / FOLD_F32 / FOLD_DF), out[p * n + i].
+cudaError_t launch_phase_probe_cudasem(int fold, const float* t, uint64_t n,
+                                       const float* periods, uint64_t n_per, float period_dt,
+                                       float* out, cudaStream_t s);
+cudaError_t launch_phase_probe_cpusem(int fold, const float* t, uint64_t n,
+                                      const float* periods, uint64_t n_per, float period_dt,
+                                      float* out, cudaStream_t s);
+
 // Preparation kernels (pf_prep.cu).
 // max |t| over n packed points into *tmax_bits (float bits; zeroed first).
 cudaError_t launch_tmax(const float* t, size_t n, unsigned* tmax_bits, cudaStream_t stream);
@@ -56,6 +65,44 @@ cudaError_t launch_aov_fix_prep(const float* m, uint64_t* aux64, CurveDesc* curv
 cudaError_t launch_pack(const float* src_t, const float* src_m, const int64_t* src_off,
                         const CurveDesc* curves, uint32_t n_curves, float* dst_t, float* dst_m,
                         cudaStream_t stream);
+
+// Lomb-Scargle derivatives (pf_lsgrad.cu).  Times and magnitudes are CSR
+// arrays with device offsets; omega is angular frequency (rad / time unit),
+// omega[c * omega_stride + k] (stride 0: one grid for every curve).
+// Outputs are [n_curves][n_freq]; coef holds (alpha, beta) pairs.
+struct LsEvalParams {
+    const float* t = nullptr;
+    const float* y = nullptr;
+    const int64_t* off = nullptr;
+    uint64_t n_curves = 0;
+    const double* omega = nullptr;
+    uint64_t omega_stride = 0;
+    uint64_t n_freq = 0;
+    float* power = nullptr;
+    float* dpdw = nullptr;
+    float* d2pdw2 = nullptr;
+    float* coef = nullptr;
+    // Newton refinement only
+    const double* half_width = nullptr;  // [n_curves][n_freq] bracket half-width
+    uint32_t n_steps = 0;
+    double* omega_out = nullptr;
+};
+struct LsGradParams {
+    const float* t = nullptr;
+    const int64_t* off = nullptr;
+    uint64_t n_curves = 0;
+    const double* omega = nullptr;
+    uint64_t omega_stride = 0;
+    uint64_t n_freq = 0;
+    const float* grad_power = nullptr;
+    const float* dpdw = nullptr;
+    const float* coef = nullptr;
+    double* grad_omega = nullptr;
+    float* grad_mags = nullptr;
+};
+cudaError_t launch_ls_eval(const LsEvalParams& p, int order, cudaStream_t stream);
+cudaError_t launch_ls_refine(const LsEvalParams& p, cudaStream_t stream);
+cudaError_t launch_ls_grad(const LsGradParams& p, uint32_t max_len, cudaStream_t stream);
 
 // Peak search (pf_peaks.cu): one CTA per curve over a [n_curves][flat]
 // periodogram; rust/src/peaks.rs semantics.

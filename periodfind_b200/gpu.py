@@ -234,6 +234,51 @@ class LombScargle(_Periodogram):
                                    nat.ptr(pdts), len(pdts), n_peaks, min_distance,
                                    self._flags, nat.ptr(idx), nat.ptr(val))
 
+    def refine_peaks(self, times, mags, periods, peak_indices, n_steps=5, center=None):
+        """Refine grid peaks off the trial grid by Newton steps on dP/domega
+        (no counterpart in the reference, whose peaks are grid points).
+
+        peak_indices: [n_curves, K] indices into `periods` (-1 = no peak), as
+        peaks() returns them for period_dts=[0].  Each peak is refined inside
+        the bracket reaching its farther grid neighbour.  Returns (periods
+        float64 [n_curves, K], NaN where no peak; powers float32, 0 there).
+        """
+        import torch
+
+        from . import ls_grad
+
+        if center is None:
+            center = self._center_default
+        validate_inputs(times, mags)
+        ensure_float32(times, "times")
+        ensure_float32(mags, "mags")
+        mags_use = prepare_magnitudes(mags, center, False)
+        grid = np.asarray(_grid(periods, "periods"), dtype=np.float64)
+        idx = np.asarray(peak_indices, dtype=np.int64)
+        if idx.ndim != 2 or idx.shape[0] != len(times):
+            raise ValueError("peak_indices must be [n_curves, K]")
+        if np.any(idx >= len(grid)):
+            raise ValueError("peak index out of range of periods")
+        valid = idx >= 0
+        i = np.where(valid, idx, 0)
+        w_grid = 2.0 * np.pi / grid
+        w0 = w_grid[i]
+        hw = np.maximum(np.abs(w_grid[np.maximum(i - 1, 0)] - w0),
+                        np.abs(w_grid[np.minimum(i + 1, len(grid) - 1)] - w0))
+        lens = np.array([len(t) for t in times], dtype=np.int64)
+        off = np.zeros(len(times) + 1, dtype=np.int64)
+        np.cumsum(lens, out=off[1:])
+        dev = torch.device("cuda", self.device)
+        cat = lambda xs: torch.from_numpy(
+            np.concatenate(xs) if len(xs) else np.zeros(0, np.float32)).to(dev)
+        w, pw = ls_grad.refine_peaks(cat(list(times)), cat(list(mags_use)),
+                                     torch.from_numpy(w0).to(dev), torch.from_numpy(hw).to(dev),
+                                     off, n_steps)
+        w = w.cpu().numpy()
+        pw = pw.cpu().numpy()
+        return (np.where(valid, 2.0 * np.pi / np.where(valid, w, 1.0), np.nan),
+                np.where(valid, pw, np.float32(0.0)).astype(np.float32))
+
 
 def find_top_peaks_batched(data, n_peaks, min_distance, use_max, device=0):
     """Top peaks of precomputed periodograms [n_curves, n_periods, n_pdts]

@@ -105,3 +105,25 @@ def batch_config2(n_curves, n_points, seed, t_span=2000.0):
         times.append(t)
         mags.append(noisy(rng, y, 0.05))
     return times, mags
+
+
+def ls_study_curves(n_curves, seed, lengths=None, baseline=3000.0):
+    """Lomb-Scargle study curves: lengths log-uniform in [64, 16384] unless
+    given; seasonal cadence over `baseline` days with a 240-day annual gap;
+    15 + A sin(2 pi f t) + N(0, sigma^2), A ~ U[0.01, 0.5], sigma ~ U[0.01,
+    0.1], f ~ U[0.01, 20] per day.  Returns (times, mags, freqs, sigmas)
+    with float32 times / mags and the magnitudes centred."""
+    rng = np.random.default_rng(seed)
+    if lengths is None:
+        lengths = np.exp(rng.uniform(np.log(64), np.log(16384), n_curves)).astype(np.int64)
+    ts, ms, fs, ss = [], [], [], []
+    for n in lengths:
+        t = seasonal_times(rng, int(n), baseline)
+        a, s, f = rng.uniform(0.01, 0.5), rng.uniform(0.01, 0.1), rng.uniform(0.01, 20.0)
+        m = 15.0 + a * np.sin(2 * np.pi * f * t.astype(np.float64) + rng.uniform(0, 2 * np.pi))
+        m = (m + rng.normal(0.0, s, len(t))).astype(np.float32)
+        ts.append(t)
+        ms.append(center(m))
+        fs.append(f)
+        ss.append(s)
+    return ts, ms, np.array(fs), np.array(ss)

@@ -1,0 +1,146 @@
+"""Precision study of the LS folds on the GPU against the FP64 oracle:
+phase error of each fold variant (the reference's expression, the exact
+divide-free fold, the split-precision fold, the all-FP32 fold) and the power
+and peak error of the periodograms they give, on samples of the study batch
+(seasonal cadence over 3000 days, up to 6e4 cycles of baseline at 20 / day).
+
+Bounds asserted:
+  reference / exact fold phase  |err| <= 2^-24 turns (the f32 rounding of
+                                the result; exact fold == reference bit for bit)
+  split-precision phase         |err| <= 1.5 * 2^-24 turns
+  split-precision LS power      |err| <= max(2e-5, 1.1 x the plain fold's) x
+                                max power of the curve, and the same grid
+                                argmax as the FP64 oracle
+  all-FP32 fold                 reported only (errors ~1e-3 turns)
+Set PF_REPORT_DIR to also write precision.json there.
+"""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests import lightcurves as lc
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+FOLDS = {"reference": 0, "exact": 0x400, "split": 0x200, "f32": 0x100}
+
+
+def _circ(a, b):
+    d = np.asarray(a, np.float64) - np.asarray(b, np.float64)
+    return np.abs(d - np.round(d))
+
+
+@pytest.fixture(scope="module")
+def report():
+    rep = {}
+    yield rep
+    d = os.environ.get("PF_REPORT_DIR")
+    if d:
+        os.makedirs(d, exist_ok=True)
+        with open(os.path.join(d, "precision.json"), "w") as fh:
+            json.dump(rep, fh, indent=1)
+
+
+def test_phase_error_per_fold(oracle, report):
+    from periodfind_b200 import _native as nat
+
+    rng = np.random.default_rng(3)
+    t = lc.seasonal_times(rng, 4096, 3000.0)
+    freqs = np.linspace(0.01, 20.0, 2000)
+    periods = (1.0 / freqs).astype(np.float32)
+    ref = oracle.phase_f64(t, periods.astype(np.float64))
+    ctx = nat.default_context(0)
+    dt = torch.from_numpy(t).cuda()
+    dp = torch.from_numpy(periods).cuda()
+    out = torch.empty(len(periods) * len(t), dtype=torch.float32, device="cuda")
+    res = {}
+    phases = {}
+    for name, mode in FOLDS.items():
+        with ctx.lock:
+            ctx.check(ctx.lib.pf_fold_phase_dev(ctx.handle, mode, dt.data_ptr(), len(t),
+                                                dp.data_ptr(), len(periods), 0.0,
+                                                out.data_ptr(), None))
+        torch.cuda.synchronize()
+        ph = out.cpu().numpy().reshape(len(periods), len(t))
+        phases[name] = ph
+        e = _circ(ph, ref)
+        res[name] = {"max_turns": float(e.max()), "rms_turns": float(np.sqrt(np.mean(e ** 2)))}
+    print("phase error vs FP64 (turns):",
+          {k: f"max {v['max_turns']:.2e} rms {v['rms_turns']:.2e}" for k, v in res.items()})
+    report["phase"] = {"sample": f"{len(t)} seasonal times over 3000 d x {len(periods)} "
+                                 "frequencies in [0.01, 20] / d (up to 6e4 cycles)",
+                       "folds": res}
+    np.testing.assert_array_equal(phases["exact"], phases["reference"])
+    assert res["reference"]["max_turns"] <= 2.0 ** -24
+    assert res["split"]["max_turns"] <= 1.5 * 2.0 ** -24
+
+
+def test_power_error_per_fold(oracle, report):
+    from periodfind_b200 import gpu
+
+    lengths = [64, 300, 1500, 4000, 16384]
+    ts, ms, fs, _ = lc.ls_study_curves(len(lengths), seed=21, lengths=lengths)
+    freqs = np.linspace(0.01, 20.0, 50000)
+    periods = (1.0 / freqs[::-1]).astype(np.float32)
+    pdts = np.zeros(1, np.float32)
+    ref = oracle.ls_f64(ts, ms, periods.astype(np.float64), [0.0])[:, :, 0]
+    res = {}
+    for name, kw in (("plain (reference fold)", dict(mode="plain")),
+                     ("chosen split-precision", dict(mode="chosen")),
+                     ("chosen exact", dict(mode="chosen", fold="exact")),
+                     ("all-FP32", dict(mode="chosen", fold="f32"))):
+        pg = gpu.LombScargle(**kw).periodograms(ts, ms, periods, pdts)[:, :, 0]
+        scale = ref.max(axis=1, keepdims=True)
+        err = np.abs(pg - ref) / scale
+        same_peak = np.argmax(pg, axis=1) == np.argmax(ref, axis=1)
+        res[name] = {"max_rel_to_peak": float(err.max()),
+                     "median_rel_to_peak": float(np.median(err)),
+                     "argmax_agrees": int(same_peak.sum()), "curves": len(ts)}
+    print("power error vs FP64 (relative to each curve's peak):",
+          {k: f"max {v['max_rel_to_peak']:.2e} argmax {v['argmax_agrees']}/{v['curves']}"
+           for k, v in res.items()})
+    report["power"] = {"sample": f"curves of {lengths} points, 50000 frequencies "
+                                 "uniform in [0.01, 20] / d", "folds": res}
+    s = res["chosen split-precision"]
+    # The FP32 sums dominate the power error of both folds; the phase adds
+    # nothing measurable.
+    bound = max(2e-5, 1.1 * res["plain (reference fold)"]["max_rel_to_peak"])
+    assert s["max_rel_to_peak"] <= bound and s["argmax_agrees"] == len(ts)
+    assert res["plain (reference fold)"]["argmax_agrees"] == len(ts)
+
+
+def test_refined_peak_frequency_error(oracle, report):
+    """Top-32 peaks of 2048-point curves (grid of 20000 log-spaced
+    frequencies), refined by 5 Newton steps, against the FP64 oracle's
+    refinement: the relative frequency error is reported and bounded by
+    1e-7."""
+    from periodfind_b200 import gpu
+
+    ts, ms, fs, _ = lc.ls_study_curves(48, seed=22, lengths=[2048] * 48)
+    freqs = np.exp(np.linspace(np.log(0.01), np.log(20.0), 20000))
+    periods = (1.0 / freqs[::-1]).astype(np.float32)
+    ls = gpu.LombScargle()
+    idx, _ = ls.peaks(ts, ms, periods, np.zeros(1, np.float32), 32, 1)
+    got_p, got_pw = ls.refine_peaks(ts, ms, periods, idx, n_steps=5, center=False)
+    wg = 2 * np.pi / periods.astype(np.float64)
+    valid = idx >= 0
+    i = np.where(valid, idx, 0)
+    w0 = wg[i]
+    hw = np.maximum(np.abs(wg[np.maximum(i - 1, 0)] - w0),
+                    np.abs(wg[np.minimum(i + 1, len(wg) - 1)] - w0))
+    ref_w, _ = oracle.ls_refine_f64(ts, ms, w0, hw, n_steps=5)
+    ref_p = 2 * np.pi / ref_w
+    rel = (np.abs(got_p - ref_p) / ref_p)[valid]
+    grid_rel = (np.abs(periods.astype(np.float64)[i] - ref_p) / ref_p)[valid]
+    res = {"peaks": int(valid.sum()), "median": float(np.median(rel)),
+           "p99": float(np.percentile(rel, 99)), "max": float(rel.max()),
+           "grid_point_error_median": float(np.median(grid_rel))}
+    print("refined peak frequency relative error:", res)
+    report["refined_peaks"] = {"sample": "48 curves x 2048 points, top-32 peaks, 5 steps",
+                               **res}
+    assert rel.max() <= 1e-7
