@@ -41,6 +41,11 @@
  *                  split-precision phase: bit-identical to the plain form.
  *  PF_TIMING       record device timestamps per work item (CTA start and
  *                  end, %globaltimer) for pf_curve_latency.
+ *  PF_REF_STATS    (CE/AOV, chosen) compute the statistic from the bins with
+ *                  the reference's operation sequence instead of the chosen
+ *                  form's divide-free one (agreeing to ~1e-6): values are then
+ *                  bit-identical to the plain form exactly when the bin
+ *                  occupancies are, which is how occupancy parity is tested.
  */
 #ifndef PERIODFIND_B200_PF_H
 #define PERIODFIND_B200_PF_H
@@ -65,6 +70,7 @@ extern "C" {
 #define PF_FOLD_DF 0x200
 #define PF_FOLD_EXACT 0x400
 #define PF_TIMING 0x1000
+#define PF_REF_STATS 0x2000
 
 typedef struct pf_ctx pf_ctx;
 

@@ -29,6 +29,7 @@ PF_FOLD_F32 = 0x100
 PF_FOLD_DF = 0x200
 PF_FOLD_EXACT = 0x400
 PF_TIMING = 0x1000
+PF_REF_STATS = 0x2000
 
 _vp = ctypes.c_void_p
 _u64 = ctypes.c_uint64

@@ -235,6 +235,7 @@ FoldConfig choose_config(pf_ctx* ctx, const Job& j, uint32_t max_len, bool& ok) 
     if (chosen && !c.ovl && (j.algo == ALGO_CE || j.algo == ALGO_AOV) && max_len < 65536u) {
         c.kind = KIND_BIN;
         c.cnt16 = (j.algo == ALGO_CE);
+        c.ref_stats = (j.mode & PF_REF_STATS) != 0;
     } else if (j.algo == ALGO_AOV && chosen &&
                (uint64_t)max_len * j.po < (1ull << (64 - kFixCountShift)) - 1ull) {
         c.acc = AOVACC_FIX;

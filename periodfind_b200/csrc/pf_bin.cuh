@@ -63,7 +63,63 @@ struct BinPoint {
     uint32_t a, b;
 };
 
-template <int ALGO, bool CNT16, int BLOCK>
+// The chosen form's CE statistic.  Counters are read through 32-bit shared
+// addresses (tbase = this thread's column).  Each row term
+// C_j ln C_j - sum_i c_ij ln c_ij is non-negative, so FP32 accumulation keeps
+// the relative error near 1e-7 (FP64 here costs registers in the binning
+// loop, measured slower).
+template <bool CNT16>
+__device__ __forceinline__ float ce_stat_fast(uint32_t tbase, uint32_t nP, uint32_t W,
+                                              uint32_t block, uint32_t n) {
+    // c ln c, zero for c = 0 and 1: one log per bin, no divide.
+    auto xlx = [](uint32_t c) -> float {
+        const float f = (float)max(c, 1u);
+        return f * logf(f);
+    };
+    float acc = 0.0f;
+    for (uint32_t j = 0; j < nP; j++) {
+        uint32_t col = 0;
+        float row = 0.0f;
+        for (uint32_t wi = 0; wi < W; wi++) {
+            const uint32_t wv = lds_u32(tbase + (j * W + wi) * block * 4u);
+            if constexpr (CNT16) {
+                const uint32_t c0 = wv & 0xFFFFu, c1 = wv >> 16;
+                col += c0 + c1;
+                row += xlx(c0) + xlx(c1);
+            } else {
+                col += wv;
+                row += xlx(wv);
+            }
+        }
+        acc += xlx(col) - row;
+    }
+    return acc / (float)n;
+}
+
+// The chosen form's AOV sum_b X_b^2 / c_b over the fixed-point bin sums X_b
+// (empty bins have X_b = 0 and contribute nothing).
+__device__ __forceinline__ double aov_sbx_fast(uint32_t tbase, uint32_t nP, uint32_t block) {
+    double sbx = 0.0;
+    const uint32_t sum_off = nP * block * 4u;
+    for (uint32_t b = 0; b < nP; b++) {
+        const uint32_t c = lds_u32(tbase + b * block * 4u);
+        const double Xd = (double)lds_u32(tbase + sum_off + b * block * 4u);
+        sbx = __fma_rn(Xd * Xd, __drcp_rn((double)max(c, 1u)), sbx);
+    }
+    return sbx;
+}
+
+// Statistic forms.  REF_STATS: the reference's operation sequence
+// (periodfind/cuda/ce.cu:160-178, aov.cu:84-121), so identical bins give
+// values bit-identical to the plain form.  Otherwise the same statistic
+// computed from the integer bins with one log (CE) or one reciprocal (AOV)
+// per bin and no divide:
+//   CE  = (sum_j C_j ln C_j - sum_ij c_ij ln c_ij) / n,  C_j = sum_i c_ij
+//         (the bin counts c over n points; the reference's p_ij ln(p_j/p_ij)
+//         summed, with the 1/n scale taken out of the logs);
+//   AOV = (n - nP)/(nP - 1) * s1 / s2, s1 = sum_b X_b^2 / c_b - X^2 / n,
+//         s2 = sum x^2 - sum_b X_b^2 / c_b (X_b the fixed-point bin sums).
+template <int ALGO, bool CNT16, int BLOCK, bool REF_STATS>
 __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
     BinPoint* tile = reinterpret_cast<BinPoint*>(smem);
@@ -240,7 +296,19 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
         (size_t)w.curve * ((size_t)p.n_per * p.n_pdt) + (size_t)pi * p.n_pdt + w.pdt;
     uint32_t* cnt32 = reinterpret_cast<uint32_t*>(cnt_raw);
 
-    if constexpr (ALGO == ALGO_CE) {
+    if constexpr (ALGO == ALGO_CE && !REF_STATS) {
+        p.out[out_idx] = ce_stat_fast<CNT16>(tbase, nP, W, BLOCK, n);
+    } else if constexpr (ALGO == ALGO_AOV && !REF_STATS) {
+        const double sbx = aov_sbx_fast(tbase, nP, BLOCK);
+        const double s1 = fmax(sbx - cd.fix_sumx * cd.fix_sumx / (double)n, 0.0);
+        const double s2 = __dadd_rn(cd.fix_sumx2, -sbx);
+        const double scale = ((double)n - (double)nP) / ((double)nP - 1.0);
+#if PF_SEM_CPU_TU
+        p.out[out_idx] = (s2 <= 0.0) ? 0.0f : (float)(scale * (s1 / s2));
+#else
+        p.out[out_idx] = (float)(scale * (s1 / (s2 <= 0.0 ? 0.0 : s2)));
+#endif
+    } else if constexpr (ALGO == ALGO_CE) {
         auto count = [&](uint32_t j, uint32_t i) -> uint32_t {
             if constexpr (CNT16) {
                 const uint32_t wv = cnt32[(j * W + (i >> 1)) * BLOCK + tid];

@@ -18,6 +18,7 @@ struct FoldConfig {
     int acc;    // AOVACC_* (AOV only)
     int block;  // threads per CTA: 64, 128 or 256
     bool ovl;   // general bin-overlap path
+    bool ref_stats; // bin_kernel: the reference's statistic operation sequence
 };
 
 size_t fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag);

@@ -7,10 +7,13 @@ classes (periodfind/cpu/__init__.py:73-397): `output` may also be 'peaks'
 (with `n_peaks`, `min_distance`), and `errs` is accepted and ignored, as
 CE, AOV and LS do not use uncertainties.
 
-Two keyword-only additions select the implementation:
+Keyword-only additions select the implementation:
   mode       'chosen' (default) or 'plain' (the reference's fold, op for op)
   semantics  'cuda' (default: the reference CUDA build's arithmetic) or
              'cpu' (the reference CPU path's IEEE arithmetic)
+  reference_stats  (CE, AOV) True: the chosen form computes the statistic
+             from its bins with the reference's operation sequence, so its
+             values equal the plain form's exactly when the bins do
 """
 
 from __future__ import annotations
@@ -26,7 +29,8 @@ MIN_DISTANCE_DEFAULT = 1
 _OUTPUTS = ("stats", "periodogram", "peaks")
 
 
-def _mode_flags(mode: str, semantics: str, fold: str | None = None) -> int:
+def _mode_flags(mode: str, semantics: str, fold: str | None = None,
+                reference_stats: bool = False) -> int:
     if mode not in ("chosen", "plain"):
         raise ValueError(f"mode must be 'chosen' or 'plain', got {mode!r}")
     if semantics not in ("cuda", "cpu"):
@@ -42,6 +46,8 @@ def _mode_flags(mode: str, semantics: str, fold: str | None = None) -> int:
         f |= nat.PF_FOLD_EXACT
     elif fold not in (None, "ref"):
         raise ValueError(f"unknown fold {fold!r}")
+    if reference_stats:
+        f |= nat.PF_REF_STATS
     return f
 
 
@@ -84,7 +90,8 @@ class _Periodogram:
         self.mode = mode
         self.semantics = semantics
         self.device = device
-        self._flags = _mode_flags(mode, semantics, getattr(self, "_fold", None))
+        self._flags = _mode_flags(mode, semantics, getattr(self, "_fold", None),
+                                  getattr(self, "_reference_stats", False))
 
     # -- native calls, implemented per algorithm
     def _native_pgram(self, ctx, b, periods, pdts, out):
@@ -165,7 +172,8 @@ class ConditionalEntropy(_Periodogram):
     _normalize_default = True
 
     def __init__(self, n_phase=10, n_mag=10, phase_bin_extent=1, mag_bin_extent=1, *,
-                 mode="chosen", semantics="cuda", device=0):
+                 mode="chosen", semantics="cuda", device=0, reference_stats=False):
+        self._reference_stats = bool(reference_stats)
         super().__init__(mode=mode, semantics=semantics, device=device)
         self.n_phase = int(n_phase)
         self.n_mag = int(n_mag)
@@ -192,7 +200,8 @@ class AOV(_Periodogram):
     _use_max = True
 
     def __init__(self, n_phase=10, phase_bin_extent=1, *, mode="chosen", semantics="cuda",
-                 device=0):
+                 device=0, reference_stats=False):
+        self._reference_stats = bool(reference_stats)
         super().__init__(mode=mode, semantics=semantics, device=device)
         self.n_phase = int(n_phase)
         self.phase_bin_extent = int(phase_bin_extent)

@@ -138,7 +138,8 @@ def test_chosen_equals_plain_ce_ls(gpu, sem):
     msn = [lc.normalize(m) if len(m) > 1 else np.full(1, 0.5, np.float32) for m in ms]
     P, D = _grid(500, pdts=(0.0, 2e-4))
     a = gpu.ConditionalEntropy(mode="plain", semantics=sem).periodograms(ts, msn, P, D)
-    b = gpu.ConditionalEntropy(mode="chosen", semantics=sem).periodograms(ts, msn, P, D)
+    b = gpu.ConditionalEntropy(mode="chosen", semantics=sem,
+                               reference_stats=True).periodograms(ts, msn, P, D)
     np.testing.assert_array_equal(a, b)
     msc = [lc.center(m) for m in ms]
     a = gpu.LombScargle(mode="plain", semantics=sem).periodograms(ts, msc, P, D)
@@ -165,11 +166,41 @@ def test_bin_kernel_occupancy_exact_at_scale(gpu, pdts):
     D = np.array(pdts, np.float32)
     for sem in ("cuda", "cpu"):
         a = gpu.ConditionalEntropy(mode="plain", semantics=sem).periodograms(ts, msn, P, D)
-        b = gpu.ConditionalEntropy(mode="chosen", semantics=sem).periodograms(ts, msn, P, D)
+        b = gpu.ConditionalEntropy(mode="chosen", semantics=sem,
+                                   reference_stats=True).periodograms(ts, msn, P, D)
         np.testing.assert_array_equal(a, b)
+        # the chosen form's own statistic from the same bins: within 1e-5
+        f = gpu.ConditionalEntropy(mode="chosen", semantics=sem).periodograms(ts, msn, P, D)
+        np.testing.assert_allclose(f, a, rtol=1e-5)
         a = gpu.ConditionalEntropy(15, 7, mode="plain", semantics=sem).periodograms(ts[:8], msn[:8], P, D)
-        b = gpu.ConditionalEntropy(15, 7, mode="chosen", semantics=sem).periodograms(ts[:8], msn[:8], P, D)
+        b = gpu.ConditionalEntropy(15, 7, mode="chosen", semantics=sem,
+                                   reference_stats=True).periodograms(ts[:8], msn[:8], P, D)
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("sem", ["cuda", "cpu"])
+def test_chosen_statistics_from_same_bins(gpu, sem):
+    """The chosen form's divide-free CE / AOV statistics from the same bins:
+    CE within 1e-5 of the plain form; AOV within 1e-9 of the chosen form's
+    reference-sequence statistic (both FP64 over exact fixed-point sums; the
+    plain AOV keeps the reference's f32 sums, which cancel for raw
+    magnitudes near 15)."""
+    ts, ms = _ragged(seed=8)
+    msn = [lc.normalize(m) if len(m) > 1 else np.full(1, 0.5, np.float32) for m in ms]
+    P, D = _grid(700, pdts=(0.0, 3e-5))
+    for n_phase, n_mag in ((10, 10), (12, 7), (5, 20)):
+        a = gpu.ConditionalEntropy(n_phase, n_mag, mode="plain", semantics=sem).periodograms(
+            ts, msn, P, D)
+        b = gpu.ConditionalEntropy(n_phase, n_mag, mode="chosen", semantics=sem).periodograms(
+            ts, msn, P, D)
+        np.testing.assert_allclose(b, a, rtol=1e-5)
+    keep = [i for i, t in enumerate(ts) if len(t) >= 16]
+    tk, mk = [ts[i] for i in keep], [ms[i] for i in keep]
+    for n_phase in (15, 10, 3):
+        a = gpu.AOV(n_phase, mode="chosen", semantics=sem,
+                    reference_stats=True).periodograms(tk, mk, P, D)
+        b = gpu.AOV(n_phase, mode="chosen", semantics=sem).periodograms(tk, mk, P, D)
+        np.testing.assert_allclose(b, a, rtol=1e-9, atol=1e-9 * np.abs(a).max())
 
 
 def test_ls_split_precision_phase_is_more_accurate(gpu, oracle):
@@ -204,9 +235,12 @@ def test_exact_fold_long_baseline(gpu, oracle):
     P = np.exp(np.linspace(np.log(0.01), np.log(0.1), 700)).astype(np.float32)
     D = np.array([0.0, 1e-7], np.float32)
     a = gpu.ConditionalEntropy(mode="plain", semantics="cpu").periodograms([t], [m], P, D)
-    b = gpu.ConditionalEntropy(mode="chosen", semantics="cpu").periodograms([t], [m], P, D)
+    b = gpu.ConditionalEntropy(mode="chosen", semantics="cpu",
+                               reference_stats=True).periodograms([t], [m], P, D)
     np.testing.assert_array_equal(a, b)
     np.testing.assert_allclose(b, oracle.ce([t], [m], P, D), rtol=2e-6)
+    f = gpu.ConditionalEntropy(mode="chosen", semantics="cpu").periodograms([t], [m], P, D)
+    np.testing.assert_allclose(f, a, rtol=1e-5)
 
 
 # ----------------------------------------------------- peaks on the device
