@@ -41,6 +41,14 @@
  *                  split-precision phase: bit-identical to the plain form.
  *  PF_TIMING       record device timestamps per work item (CTA start and
  *                  end, %globaltimer) for pf_curve_latency.
+ *  PF_NO_TUNE      (chosen) skip the launch-shape autotuner and use the
+ *                  default shape for every length class.  The chosen kernels
+ *                  take their work from a device queue split by curve length
+ *                  ([0,64), [64,256), [256,1024), [1024,4096), [4096,...));
+ *                  the first call that meets a (computation, class) pair
+ *                  times the candidate shapes on a sample of that class and
+ *                  synchronises the stream once; the result is cached in the
+ *                  context.  Results do not depend on the shape.
  *  PF_REF_STATS    (CE/AOV, chosen) compute the statistic from the bins with
  *                  the reference's operation sequence instead of the chosen
  *                  form's divide-free one (agreeing to ~1e-6): values are then
@@ -71,6 +79,7 @@ extern "C" {
 #define PF_FOLD_EXACT 0x400
 #define PF_TIMING 0x1000
 #define PF_REF_STATS 0x2000
+#define PF_NO_TUNE 0x4000
 
 typedef struct pf_ctx pf_ctx;
 
@@ -255,6 +264,12 @@ int pf_ls_refine_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
                      const int64_t* offsets, uint64_t n_curves, const double* d_omega0,
                      const double* d_half_width, uint64_t n_freq, uint32_t n_steps,
                      double* d_omega, float* d_power, void* stream);
+
+/* The autotuner's decisions on this context, one line per (computation,
+ * length class): the launch shape kept and the sample times of the fastest
+ * and slowest candidates.  Writes at most len bytes (NUL-terminated) and
+ * returns the number of entries. */
+int pf_tuning_report(const pf_ctx* ctx, char* buf, uint64_t len);
 
 /* Number of kernels this context has launched since creation (telemetry
  * for benchmarks: launches of the library's own kernels only). */

@@ -30,6 +30,7 @@ PF_FOLD_DF = 0x200
 PF_FOLD_EXACT = 0x400
 PF_TIMING = 0x1000
 PF_REF_STATS = 0x2000
+PF_NO_TUNE = 0x4000
 
 _vp = ctypes.c_void_p
 _u64 = ctypes.c_uint64
@@ -68,6 +69,7 @@ SIGNATURES = {
     "pf_ls_backward_dev": ([_vp, _vp, _vp, _u64, _vp, _u64, _u64, _vp, _vp, _vp, _vp, _vp,
                             _vp], _int),
     "pf_ls_refine_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _vp, _u64, _u32, _vp, _vp, _vp], _int),
+    "pf_tuning_report": ([_vp, ctypes.c_char_p, _u64], _int),
     "pf_launch_count": ([_vp], _u64),
     "pf_last_kernel_ms": ([_vp], ctypes.c_double),
 }
@@ -130,6 +132,12 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def tuning_report(self) -> str:
+        """The autotuner's choices on this context (pf_tuning_report)."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        self.check(min(0, self.lib.pf_tuning_report(self.handle, buf, len(buf))))
+        return buf.value.decode()
 
     def check(self, rc):
         if rc != PF_OK:

@@ -19,6 +19,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -65,6 +66,16 @@ struct pf_ctx {
     double last_ms = -1.0;
     int n_sm = 0;
     size_t smem_optin = 0;
+    // Autotuner: launch shape per (computation, length class), measured on
+    // the device the first time the key is met (see tuned_config).
+    struct Tuned {
+        int block;
+        bool persist;
+        float ms;        // sample time of the winner
+        float ms_worst;  // and of the slowest candidate
+        uint32_t candidates;
+    };
+    std::map<std::string, Tuned> tuned;
 };
 
 namespace {
@@ -147,6 +158,7 @@ struct Job {
 struct Layout {
     std::vector<int64_t> off;  // per curve, in points (multiple of 4)
     std::vector<uint32_t> len;
+    std::vector<uint32_t> order;  // queue kernels: curves longest first
     size_t total_pts = 0;      // padded
     size_t o_t = 0, o_m = 0, o_curves = 0, o_work = 0, o_periods = 0, o_pdts = 0, o_srcoff = 0;
     size_t bytes = 0;
@@ -231,11 +243,13 @@ FoldConfig choose_config(pf_ctx* ctx, const Job& j, uint32_t max_len, bool& ok) 
         if (j.mode & PF_FOLD_F32) c.fold = FOLD_F32;
     }
     c.acc = AOVACC_F32;
+    c.n_sm = ctx->n_sm;
     c.ovl = (j.algo == ALGO_CE) ? (j.po > 1 || j.mo > 1) : (j.algo == ALGO_AOV && j.po > 1);
     if (chosen && !c.ovl && (j.algo == ALGO_CE || j.algo == ALGO_AOV) && max_len < 65536u) {
         c.kind = KIND_BIN;
         c.cnt16 = (j.algo == ALGO_CE);
         c.ref_stats = (j.mode & PF_REF_STATS) != 0;
+        c.persist = true;  // measured: the bin kernel gains from the persistent queue
     } else if (j.algo == ALGO_AOV && chosen &&
                (uint64_t)max_len * j.po < (1ull << (64 - kFixCountShift)) - 1ull) {
         c.acc = AOVACC_FIX;
@@ -293,6 +307,22 @@ void build_work(const Job& j, const Layout& L, int block, WorkItem* w) {
     }
 }
 
+// Curve order of the persistent kernels' queue: longest first, ties in
+// input order (a counting sort on the lengths, or a stable sort when the
+// longest curve is very long).
+void build_order(const Layout& L, uint64_t n_curves, uint32_t* order) {
+    if (L.max_len <= (1u << 20)) {
+        std::vector<uint32_t> start((size_t)L.max_len + 2, 0u);
+        for (uint64_t c = 0; c < n_curves; c++) start[(size_t)(L.max_len - L.len[c]) + 1]++;
+        for (size_t k = 1; k < start.size(); k++) start[k] += start[k - 1];
+        for (uint64_t c = 0; c < n_curves; c++) order[start[L.max_len - L.len[c]]++] = (uint32_t)c;
+        return;
+    }
+    std::iota(order, order + n_curves, 0u);
+    std::stable_sort(order, order + n_curves,
+                     [&](uint32_t a, uint32_t b) { return L.len[a] > L.len[b]; });
+}
+
 // Copy one curve into the packed staging area, checking times are finite.
 bool copy_curve(const float* t, const float* m, uint32_t n, float* dt, float* dm, uint32_t pad) {
     bool ok = true;
@@ -347,7 +377,12 @@ int plan(pf_ctx* ctx, const Job& j, const uint64_t* lengths, bool with_points, b
     L.o_curves = o;
     o = align_up(o + j.n_curves * sizeof(CurveDesc), 256);
     L.o_work = o;
-    o = align_up(o + (size_t)L.n_work * sizeof(WorkItem), 256);
+    // Queue kernels take a curve order (the device derives the items);
+    // the others a host-built work list.
+    if (uses_queue(cfg.kind, cfg.fold))
+        o = align_up(o + (size_t)j.n_curves * sizeof(uint32_t), 256);
+    else
+        o = align_up(o + (size_t)L.n_work * sizeof(WorkItem), 256);
     L.o_periods = o;
     if (with_grid) o = align_up(o + j.n_per * 4, 256);
     L.o_pdts = o;
@@ -368,13 +403,20 @@ int staging_ready(pf_ctx* ctx) {
     return PF_OK;
 }
 
-void fill_meta(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig& cfg, char* hb) {
+void fill_meta(pf_ctx* ctx, const Job& j, Layout& L, const FoldConfig& cfg, char* hb) {
     CurveDesc* hc = (CurveDesc*)(hb + L.o_curves);
     for (uint64_t c = 0; c < j.n_curves; c++) {
         CurveDesc d{};
         d.off = L.off[c];
         d.n = L.len[c];
         hc[c] = d;
+    }
+    if (uses_queue(cfg.kind, cfg.fold)) {
+        // Item-to-curve map for PF_TIMING is made per class at launch time.
+        L.order.resize(j.n_curves);
+        build_order(L, j.n_curves, L.order.data());
+        memcpy(hb + L.o_work, L.order.data(), j.n_curves * sizeof(uint32_t));
+        return;
     }
     WorkItem* w = (WorkItem*)(hb + L.o_work);
     build_work(j, L, cfg.block, w);
@@ -383,6 +425,174 @@ void fill_meta(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig& cfg
         for (uint32_t k = 0; k < L.n_work; k++) ctx->stamp_curves[k] = w[k].curve;
         ctx->stamp_n_curves = j.n_curves;
     }
+}
+
+// Length classes of the queue kernels: [0,64), [64,256), [256,1024),
+// [1024,4096), [4096,...).  Each class runs as its own launch with the
+// launch shape the autotuner picked for it.
+constexpr uint32_t kClassEdges[] = {64, 256, 1024, 4096};
+constexpr int kClasses = 5;
+int length_class(uint32_t len) {
+    int c = 0;
+    for (uint32_t e : kClassEdges) c += (len >= e) ? 1 : 0;
+    return c;
+}
+const char* class_name(int c) {
+    static const char* names[kClasses] = {"[0,64)", "[64,256)", "[256,1024)", "[1024,4096)",
+                                          "[4096,inf)"};
+    return names[c];
+}
+// Queue counters in the context's misc block: one per class, one for tuning.
+constexpr size_t kCounterOffset = 64;
+constexpr int kTuneCounter = kClasses;
+
+uint64_t queue_items(const Job& j, uint64_t n_curves, int block) {
+    return n_curves * j.n_pdt * ((j.n_per + block - 1) / block);
+}
+
+std::string tune_key(const Job& j, const FoldConfig& c, int cls) {
+    char b[160];
+    snprintf(b, sizeof(b), "%s %s%s%s ph=%u mag=%u pdt=%s sem=%s class=%s",
+             c.algo == ALGO_CE ? "ce" : c.algo == ALGO_AOV ? "aov" : "ls",
+             c.kind == KIND_BIN ? "bin" : (c.fold == FOLD_DF ? "fold-split" : "fold-exact"),
+             c.cnt16 ? "-cnt16" : "", c.ref_stats ? "-refstats" : "", j.n_phase,
+             c.algo == ALGO_CE ? j.n_mag : 0u, j.n_pdt > 1 ? "many" : "one",
+             use_cpu_semantics(j.mode) ? "cpu" : "cuda", class_name(cls));
+    return b;
+}
+
+cudaError_t launch_fold_sem(const Job& j, const FoldConfig& c, const FoldParams& p,
+                            uint32_t n_work, cudaStream_t s) {
+    return use_cpu_semantics(j.mode) ? launch_fold_cpusem(c, p, n_work, s)
+                                     : launch_fold_cudasem(c, p, n_work, s);
+}
+
+// Launch shape of one length class.  Cached per context; the first time a
+// key is met, every candidate (block 64 / 128 / 256 where shared memory
+// allows, persistent or one CTA per item) is timed with CUDA events on a
+// sample of the class (a contiguous run of its curves from the middle of
+// the class, about 2e9 point evaluations) and the fastest kept.  The sample
+// writes cells of the real output, which the class launch rewrites.  Every
+// candidate computes the same values; only the time differs.  No tuning
+// (the base shape) with PF_NO_TUNE or while the stream is being captured.
+int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uint64_t c0,
+                 uint64_t nc, uint64_t cls_points, const FoldParams& p, cudaStream_t s,
+                 FoldConfig& out) {
+    out = base;
+    const std::string key = tune_key(j, base, cls);
+    auto it = ctx->tuned.find(key);
+    if (it != ctx->tuned.end()) {
+        out.block = it->second.block;
+        out.persist = it->second.persist;
+        return PF_OK;
+    }
+    if (j.mode & PF_NO_TUNE) return PF_OK;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PF_CUDA(cudaStreamIsCapturing(s, &cap), "capture query");
+    if (cap != cudaStreamCaptureStatusNone) return PF_OK;
+
+    const double per_curve = (double)cls_points / (double)nc * (double)j.n_per * (double)j.n_pdt;
+    uint64_t k = (uint64_t)std::max(1.0, std::ceil(2e9 / std::max(per_curve, 1.0)));
+    k = std::min(k, nc);
+    const uint64_t s0 = c0 + (nc - k) / 2;
+    FoldParams ps = p;
+    ps.stamps = nullptr;
+    ps.q.order = p.q.order + s0;
+    ps.q.next = reinterpret_cast<unsigned*>((char*)ctx->d_misc.p + kCounterOffset) + kTuneCounter;
+    pf_ctx::Tuned best{base.block, base.persist, 1e30f, 0.0f, 0};
+    for (int block : {64, 128, 256}) {
+        FoldConfig t = base;
+        t.block = block;
+        if (fold_smem(t, j.n_phase, j.n_mag) > ctx->smem_optin) continue;
+        for (bool persist : {false, true}) {
+            t.persist = persist;
+            const uint64_t nw = queue_items(j, k, block);
+            if (nw == 0 || nw > 0x7FFFFFFFull) continue;
+            ps.q.n_work = (uint32_t)nw;
+            float ms = 0.0f;
+            for (int rep = 0; rep < 2; rep++) {  // the first launch warms up
+                PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
+                PF_CUDA(launch_fold_sem(j, t, ps, (uint32_t)nw, s), "tuning launch");
+                PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
+                PF_CUDA(cudaEventSynchronize(ctx->ev1), "tuning sync");
+                PF_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1), "event time");
+            }
+            ctx->launches += 2;
+            best.candidates++;
+            best.ms_worst = std::max(best.ms_worst, ms);
+            if (ms < best.ms) {
+                best.ms = ms;
+                best.block = block;
+                best.persist = persist;
+            }
+        }
+    }
+    if (best.candidates == 0) return PF_OK;
+    ctx->tuned[key] = best;
+    out.block = best.block;
+    out.persist = best.persist;
+    return PF_OK;
+}
+
+// One launch per length class of a queue kernel (curves longest first, so
+// each class is a contiguous run of the order array), after tuning.
+int launch_classes(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig& cfg,
+                   const FoldParams& p, cudaStream_t s) {
+    struct Range {
+        uint64_t c0, n, points;
+    };
+    Range r[kClasses] = {};
+    bool seen[kClasses] = {};
+    for (uint64_t i = 0; i < j.n_curves; i++) {
+        const int c = length_class(L.len[L.order[i]]);
+        if (!seen[c]) {
+            seen[c] = true;
+            r[c].c0 = i;
+        }
+        r[c].n++;
+        r[c].points += L.len[L.order[i]];
+    }
+    FoldConfig cc[kClasses];
+    uint64_t total_items = 0;
+    int rc;
+    for (int c = 0; c < kClasses; c++) {
+        if (!r[c].n) continue;
+        if ((rc = tuned_config(ctx, j, cfg, c, r[c].c0, r[c].n, r[c].points, p, s, cc[c])) !=
+            PF_OK)
+            return rc;
+        total_items += queue_items(j, r[c].n, cc[c].block);
+    }
+    if (total_items > 0x7FFFFFFFull) return fail(ctx, PF_EINVAL, "too much work for one launch");
+    if (j.mode & PF_TIMING) {
+        if ((rc = ensure_dev(ctx, ctx->d_stamps, (size_t)total_items * 16)) != PF_OK) return rc;
+        PF_CUDA(cudaMemsetAsync(ctx->d_stamps.p, 0, (size_t)total_items * 16, s), "memset");
+        ctx->stamp_curves.resize(total_items);
+        ctx->stamp_n_curves = j.n_curves;
+        ctx->stamp_stream = s;
+    }
+    PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
+    uint64_t base = 0;
+    for (int c = 0; c < kClasses; c++) {
+        if (!r[c].n) continue;
+        const uint64_t nw = queue_items(j, r[c].n, cc[c].block);
+        FoldParams pc = p;
+        pc.q.order = p.q.order + r[c].c0;
+        pc.q.n_work = (uint32_t)nw;
+        pc.q.next = reinterpret_cast<unsigned*>((char*)ctx->d_misc.p + kCounterOffset) + c;
+        pc.stamps = nullptr;
+        if (j.mode & PF_TIMING) {
+            pc.stamps = (unsigned long long*)ctx->d_stamps.p + 2 * base;
+            const uint64_t tpc = queue_items(j, 1, cc[c].block);
+            for (uint64_t k = 0; k < nw; k++)
+                ctx->stamp_curves[base + k] = L.order[r[c].c0 + k / tpc];
+        }
+        PF_CUDA(launch_fold_sem(j, cc[c], pc, (uint32_t)nw, s), "fold kernel launch");
+        ctx->launches++;
+        base += nw;
+    }
+    PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
+    ctx->timed_pending = true;
+    return PF_OK;
 }
 
 // Device pipeline shared by both entry styles: preparation kernel, fused
@@ -403,6 +613,7 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
     const uint32_t ncur = (uint32_t)j.n_curves;
     int rc;
     if ((rc = ensure_dev(ctx, ctx->d_misc, 256)) != PF_OK) return rc;
+    static_assert(kCounterOffset + 4 * (kClasses + 1) <= 256, "counters fit the misc block");
     p.tmax_bits = (const unsigned*)ctx->d_misc.p;
     PF_CUDA(launch_tmax(p.t, L.total_pts, (unsigned*)ctx->d_misc.p, s), "max|t| kernel");
     ctx->launches++;
@@ -444,19 +655,24 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
         ctx->launches++;
     }
     p.stamps = nullptr;
-    if (j.mode & PF_TIMING) {
-        if ((rc = ensure_dev(ctx, ctx->d_stamps, (size_t)L.n_work * 16)) != PF_OK) return rc;
-        PF_CUDA(cudaMemsetAsync(ctx->d_stamps.p, 0, (size_t)L.n_work * 16, s), "memset");
-        p.stamps = (unsigned long long*)ctx->d_stamps.p;
-        ctx->stamp_stream = s;
+    if (uses_queue(cfg.kind, cfg.fold)) {
+        // The staged work section holds the curve order (fill_meta).
+        p.q.order = reinterpret_cast<const uint32_t*>(p.work);
+        p.work = nullptr;
+        if ((rc = launch_classes(ctx, j, L, cfg, p, s)) != PF_OK) return rc;
+    } else {
+        if (j.mode & PF_TIMING) {
+            if ((rc = ensure_dev(ctx, ctx->d_stamps, (size_t)L.n_work * 16)) != PF_OK) return rc;
+            PF_CUDA(cudaMemsetAsync(ctx->d_stamps.p, 0, (size_t)L.n_work * 16, s), "memset");
+            p.stamps = (unsigned long long*)ctx->d_stamps.p;
+            ctx->stamp_stream = s;
+        }
+        PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
+        PF_CUDA(launch_fold_sem(j, cfg, p, L.n_work, s), "fold kernel launch");
+        ctx->launches++;
+        PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
+        ctx->timed_pending = true;
     }
-    PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
-    cudaError_t e = cpu ? launch_fold_cpusem(cfg, p, L.n_work, s)
-                        : launch_fold_cudasem(cfg, p, L.n_work, s);
-    PF_CUDA(e, "fold kernel launch");
-    ctx->launches++;
-    PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
-    ctx->timed_pending = true;
     if (j.peaks && j.n_peaks > 0) {
         const size_t pk = (size_t)j.n_curves * j.n_peaks;
         if ((rc = ensure_dev(ctx, ctx->d_pidx, pk * 8)) != PF_OK) return rc;
@@ -742,6 +958,26 @@ const char* pf_last_error(const pf_ctx* ctx) {
 }
 
 uint64_t pf_launch_count(const pf_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int pf_tuning_report(const pf_ctx* ctx, char* buf, uint64_t len) {
+    if (!ctx) return PF_EINVAL;
+    std::string out;
+    for (const auto& kv : ctx->tuned) {
+        char line[320];
+        snprintf(line, sizeof(line),
+                 "%s: block=%d %s sample_ms=%.3f slowest_ms=%.3f candidates=%u\n",
+                 kv.first.c_str(), kv.second.block,
+                 kv.second.persist ? "persistent" : "one-cta-per-item", kv.second.ms,
+                 kv.second.ms_worst, kv.second.candidates);
+        out += line;
+    }
+    if (buf && len > 0) {
+        const size_t n = std::min<size_t>(out.size(), (size_t)len - 1);
+        memcpy(buf, out.data(), n);
+        buf[n] = '\0';
+    }
+    return (int)ctx->tuned.size();
+}
 
 int pf_curve_latency(pf_ctx* ctx, uint64_t n_curves, double* out_ns) {
     if (!ctx || (!out_ns && n_curves)) return PF_EINVAL;

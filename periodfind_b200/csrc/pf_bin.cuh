@@ -120,14 +120,13 @@ __device__ __forceinline__ double aov_sbx_fast(uint32_t tbase, uint32_t nP, uint
 //   AOV = (n - nP)/(nP - 1) * s1 / s2, s1 = sum_b X_b^2 / c_b - X^2 / n,
 //         s2 = sum x^2 - sum_b X_b^2 / c_b (X_b the fixed-point bin sums).
 template <int ALGO, bool CNT16, int BLOCK, bool REF_STATS>
-__global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
+__device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, uint32_t item) {
     extern __shared__ __align__(16) unsigned char smem[];
     BinPoint* tile = reinterpret_cast<BinPoint*>(smem);
     unsigned char* cnt_raw = smem + kBinTile * sizeof(BinPoint);
     const uint32_t cnt_base = (uint32_t)__cvta_generic_to_shared(cnt_raw);
 
-    stamp_start(p);
-    const WorkItem w = p.work[blockIdx.x];
+    stamp_start(p, item);
     const CurveDesc cd = p.curves[w.curve];
     const uint32_t n = cd.n;
     const int tid = threadIdx.x;
@@ -174,10 +173,13 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
                 for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
                     const float4 q = gt[i4];
                     const uint4 a01 = ga[2 * i4], a23 = ga[2 * i4 + 1];
-                    tile[4 * i4 + 0] = BinPoint{(double)q.x, a01.x, a01.y};
-                    tile[4 * i4 + 1] = BinPoint{(double)q.y, a01.z, a01.w};
-                    tile[4 * i4 + 2] = BinPoint{(double)q.z, a23.x, a23.y};
-                    tile[4 * i4 + 3] = BinPoint{(double)q.w, a23.z, a23.w};
+                    // Counter word within a phase row -> byte offset for this
+                    // CTA shape (the prepared data does not depend on BLOCK).
+                    constexpr uint32_t kColBytes = BLOCK * 4u;
+                    tile[4 * i4 + 0] = BinPoint{(double)q.x, a01.x * kColBytes, a01.y};
+                    tile[4 * i4 + 1] = BinPoint{(double)q.y, a01.z * kColBytes, a01.w};
+                    tile[4 * i4 + 2] = BinPoint{(double)q.z, a23.x * kColBytes, a23.y};
+                    tile[4 * i4 + 3] = BinPoint{(double)q.w, a23.z * kColBytes, a23.w};
                 }
             } else {
                 const uint4* ga = reinterpret_cast<const uint4*>(p.aux32 + cd.off + base);
@@ -286,12 +288,14 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
             else body(std::false_type{}, std::false_type{});
         }
     }
-    if (!active) {
-        stamp_end(p);
-        return;
-    }
+    // Every lane of the warp reaches this barrier (inactive lanes leave the
+    // item only after it and then wait at the queue loop's CTA barrier).
     compiler_fence();
     __syncwarp();
+    if (!active) {
+        stamp_end(p, item);
+        return;
+    }
     const size_t out_idx =
         (size_t)w.curve * ((size_t)p.n_per * p.n_pdt) + (size_t)pi * p.n_pdt + w.pdt;
     uint32_t* cnt32 = reinterpret_cast<uint32_t*>(cnt_raw);
@@ -361,14 +365,30 @@ __global__ void __launch_bounds__(BLOCK) bin_kernel(const FoldParams p) {
         p.out[out_idx] = (float)(scale * (s1 / (s2 <= 0.0 ? 0.0 : s2)));
 #endif
     }
-    stamp_end(p);
+    stamp_end(p, item);
 }
 
-// CE per-point bin data for bin_kernel: {byte offset of the magnitude
-// column within a phase row (without the thread term), increment}.
+// Items from the device work queue (see WorkQueue), persistently or one CTA
+// per item.
+template <int ALGO, bool CNT16, int BLOCK, bool REF_STATS, bool PERSIST>
+__global__ void __launch_bounds__(BLOCK, queue_min_blocks<ALGO, BLOCK>())
+    bin_kernel(const FoldParams p) {
+    if constexpr (PERSIST) {
+        for_each_queued_item<BLOCK>(p, [&](const WorkItem& w, uint32_t k) {
+            bin_item<ALGO, CNT16, BLOCK, REF_STATS>(p, w, k);
+        });
+    } else {
+        bin_item<ALGO, CNT16, BLOCK, REF_STATS>(p, queue_item<BLOCK>(p, blockIdx.x), blockIdx.x);
+    }
+}
+
+// CE per-point bin data for bin_kernel: {counter word of the magnitude
+// column within a phase row, increment}.  The kernel turns the word into a
+// byte offset for its CTA shape when it stages the tile, so the data serves
+// every block size the autotuner tries.
 __global__ void ce_binaux_kernel(const float* __restrict__ m, uint2* __restrict__ aux,
                                  const CurveDesc* __restrict__ curves, uint32_t n_curves,
-                                 uint32_t n_mag, float mag_bin_size, int block, int cnt16) {
+                                 uint32_t n_mag, float mag_bin_size, int cnt16) {
     const uint32_t c = blockIdx.x;
     if (c >= n_curves) return;
     const CurveDesc cd = curves[c];
@@ -382,10 +402,10 @@ __global__ void ce_binaux_kernel(const float* __restrict__ m, uint2* __restrict_
                 static_cast<unsigned long long>(mag_val / mag_bin_size);
             const uint32_t mb = (uint32_t)(mb64 % n_mag);
             if (cnt16) {
-                v.x = (mb >> 1) * (uint32_t)block * 4u;
+                v.x = mb >> 1;
                 v.y = (mb & 1u) ? 0x10000u : 1u;
             } else {
-                v.x = mb * (uint32_t)block * 4u;
+                v.x = mb;
                 v.y = 1u;
             }
         }

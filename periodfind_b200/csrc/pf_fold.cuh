@@ -30,6 +30,7 @@
 
 #include <type_traits>
 
+#include "pf_launch.h"
 #include "pf_types.h"
 
 #ifndef PF_SEM_CPU_TU
@@ -169,11 +170,53 @@ __device__ __forceinline__ unsigned long long global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-__device__ __forceinline__ void stamp_start(const FoldParams& p) {
-    if (p.stamps && threadIdx.x == 0) p.stamps[2 * blockIdx.x] = global_ns();
+__device__ __forceinline__ void stamp_start(const FoldParams& p, uint32_t item) {
+    if (p.stamps && threadIdx.x == 0) p.stamps[2 * (size_t)item] = global_ns();
 }
-__device__ __forceinline__ void stamp_end(const FoldParams& p) {
-    if (p.stamps) atomicMax(&p.stamps[2 * blockIdx.x + 1], global_ns());
+__device__ __forceinline__ void stamp_end(const FoldParams& p, uint32_t item) {
+    if (p.stamps) atomicMax(&p.stamps[2 * (size_t)item + 1], global_ns());
+}
+
+// Work item k of the device queue (see WorkQueue).
+template <int BLOCK>
+__device__ __forceinline__ WorkItem queue_item(const FoldParams& p, uint32_t k) {
+    const uint32_t tiles = (p.n_per + BLOCK - 1) / BLOCK;
+    const uint32_t tpc = tiles * p.n_pdt;
+    const uint32_t ci = k / tpc, rem = k - ci * tpc;
+    const uint32_t d = rem / tiles, tile = rem - d * tiles;
+    WorkItem w;
+    w.curve = p.q.order[ci];
+    w.pdt = d;
+    w.p0 = tile * BLOCK;
+    w.np = min((uint32_t)BLOCK, p.n_per - w.p0);
+    return w;
+}
+
+// Persistent CTA loop: take the next item from the queue until it is empty.
+// The leading barrier keeps the previous item's shared memory (tile,
+// counters, the item slot) in use until every thread has finished with it.
+// (Claiming the next item during the current one was measured: no gain, and
+// a register spill in the LS fold.)
+template <int BLOCK, class F>
+__device__ __forceinline__ void for_each_queued_item(const FoldParams& p, F&& f) {
+    __shared__ uint32_t s_item;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(p.q.next, 1u);
+        __syncthreads();
+        const uint32_t k = s_item;
+        if (k >= p.q.n_work) break;
+        f(queue_item<BLOCK>(p, k), k);
+    }
+}
+
+// Resident CTAs per SM the queue kernels are compiled for (registers held
+// so that occupancy is not lost to the register allocator; measured): the LS
+// folds and the AOV bin kernel at 5 x 256 threads, the CE bin kernel at its
+// shared-memory limit of 4 x 256 (CE 10 x 10).
+template <int ALGO, int BLOCK>
+constexpr int queue_min_blocks() {
+    return (ALGO == ALGO_CE ? 4 : 5) * 256 / BLOCK;
 }
 
 // trunc(q) for finite q in [0, 2^23): identical to the reference's
@@ -355,7 +398,7 @@ __device__ __forceinline__ void accumulate(const FoldParams& p, const Views& v, 
 }
 
 template <int ALGO, int FOLD, int ACC, int BLOCK, bool OVL>
-__global__ void __launch_bounds__(BLOCK) fold_kernel(const FoldParams p) {
+__device__ __forceinline__ void fold_item(const FoldParams& p, const WorkItem w, uint32_t item) {
     using TT = tile_t_type<FOLD>;
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr size_t kAuxBytes = (ALGO == ALGO_AOV && ACC == AOVACC_FIX) ? 8 : 4;
@@ -376,8 +419,7 @@ __global__ void __launch_bounds__(BLOCK) fold_kernel(const FoldParams p) {
     v.a_sum = reinterpret_cast<float*>(hist_raw) + (size_t)nP * BLOCK;
     v.a_sq = reinterpret_cast<float*>(hist_raw) + (size_t)2 * nP * BLOCK;
 
-    stamp_start(p);
-    const WorkItem w = p.work[blockIdx.x];
+    stamp_start(p, item);
     const CurveDesc cd = p.curves[w.curve];
     const uint32_t n = cd.n;
     const int tid = threadIdx.x;
@@ -419,7 +461,7 @@ __global__ void __launch_bounds__(BLOCK) fold_kernel(const FoldParams p) {
     }
 
     if (!active) {
-        stamp_end(p);
+        stamp_end(p, item);
         return;
     }
     const size_t out_idx =
@@ -531,7 +573,27 @@ __global__ void __launch_bounds__(BLOCK) fold_kernel(const FoldParams p) {
         p.out[out_idx] = 0.5f * ((numerator_l / denominator_l) + (numerator_r / denominator_r));
 #endif
     }
-    stamp_end(p);
+    stamp_end(p, item);
+}
+
+// The chosen folds (exact, split-precision) take items from the device
+// queue, persistently (PERSIST) or one CTA per item; the reference fold and
+// the all-FP32 study fold take one CTA per item of the host-built list, as
+// the reference launches.
+template <int ALGO, int FOLD, int ACC, int BLOCK, bool OVL, bool PERSIST>
+__global__ void __launch_bounds__(BLOCK, (ALGO == ALGO_LS && uses_queue(KIND_FOLD, FOLD))
+                                             ? queue_min_blocks<ALGO_LS, BLOCK>()
+                                             : 1)
+    fold_kernel(const FoldParams p) {
+    if constexpr (!uses_queue(KIND_FOLD, FOLD)) {
+        fold_item<ALGO, FOLD, ACC, BLOCK, OVL>(p, p.work[blockIdx.x], blockIdx.x);
+    } else if constexpr (PERSIST) {
+        for_each_queued_item<BLOCK>(p, [&](const WorkItem& w, uint32_t k) {
+            fold_item<ALGO, FOLD, ACC, BLOCK, OVL>(p, w, k);
+        });
+    } else {
+        fold_item<ALGO, FOLD, ACC, BLOCK, OVL>(p, queue_item<BLOCK>(p, blockIdx.x), blockIdx.x);
+    }
 }
 
 // ------------------------------------------------------------- preparation

@@ -10,6 +10,15 @@ namespace pfk {
 
 enum : int { KIND_FOLD = 0, KIND_BIN = 1 };
 
+// Kernels that take their items from the device work queue (a curve order;
+// the device derives the items): the chosen bin kernel and the chosen folds.
+// Each runs either persistently (a fixed grid pulling items from an atomic
+// counter) or statically (one CTA per item).  The reference fold and the
+// all-FP32 study fold take one CTA per item of a host-built list.
+__host__ __device__ constexpr bool uses_queue(int kind, int fold) {
+    return kind == KIND_BIN || fold == FOLD_EXACT || fold == FOLD_DF;
+}
+
 struct FoldConfig {
     int kind;   // KIND_FOLD: fold_kernel; KIND_BIN: the chosen CE/AOV bin_kernel
     bool cnt16; // bin_kernel CE: 16-bit counters
@@ -19,6 +28,8 @@ struct FoldConfig {
     int block;  // threads per CTA: 64, 128 or 256
     bool ovl;   // general bin-overlap path
     bool ref_stats; // bin_kernel: the reference's statistic operation sequence
+    bool persist;   // queue kernels: persistent grid instead of one CTA per item
+    int n_sm;       // persistent kernels: grid = n_sm x resident CTAs per SM
 };
 
 size_t fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag);

@@ -72,12 +72,15 @@ int fail(char* err, uint64_t err_len, int code, const char* fmt, ...) {
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Work items in launch order: curve-major, then period derivative, then
-// tiles of kBlock periods (the same decomposition the fold kernel expects).
-__global__ void work_gen_kernel(WorkItem* __restrict__ work, uint32_t n_work, uint32_t n_pdt,
+// tiles of kBlock periods (the same decomposition the fold kernel expects),
+// and the curve order of the persistent folds' queue (input order).
+__global__ void work_gen_kernel(WorkItem* __restrict__ work, uint32_t* __restrict__ order,
+                                uint32_t n_curves, uint32_t n_work, uint32_t n_pdt,
                                 uint32_t n_per) {
     const uint32_t tiles = (n_per + kBlock - 1) / kBlock;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_work;
          k += gridDim.x * blockDim.x) {
+        if (k < n_curves) order[k] = k;
         const uint32_t per_curve = n_pdt * tiles;
         const uint32_t c = k / per_curve;
         const uint32_t r = k % per_curve;
@@ -127,9 +130,11 @@ extern "C" int pf_ls_peaks_dev_noalloc(const float* d_times, const float* d_mags
     const uint64_t n_work = n_curves * n_pdt * tiles;
     if (n_work > 0x7FFFFFFFull) return fail(err, err_len, PF_EINVAL, "too much work for one launch");
     const size_t o_tmax = 0;
+    const size_t o_queue = 128;  // queue counter of the persistent folds
     const size_t o_meta = 256;
     const size_t o_work = o_meta + meta_bytes;
-    const size_t o_t = align256(o_work + n_work * sizeof(WorkItem));
+    const size_t o_order = align256(o_work + n_work * sizeof(WorkItem));
+    const size_t o_t = align256(o_order + n_curves * sizeof(uint32_t));
     const size_t o_m = align256(o_t + total_pts * 4);
     const size_t o_pg = align256(o_m + total_pts * 4);
     const size_t need = o_pg + (size_t)n_curves * n_per * n_pdt * 4;
@@ -186,8 +191,10 @@ extern "C" int pf_ls_peaks_dev_noalloc(const float* d_times, const float* d_mags
     float* pg = reinterpret_cast<float*>(base + o_pg);
     unsigned* tmax = reinterpret_cast<unsigned*>(base + o_tmax);
 
+    uint32_t* dorder = reinterpret_cast<uint32_t*>(base + o_order);
     const int gen_blocks = (int)std::min<uint64_t>((n_work + 255) / 256, 4096);
-    work_gen_kernel<<<gen_blocks, 256, 0, s>>>(dwork, (uint32_t)n_work, (uint32_t)n_pdt,
+    work_gen_kernel<<<gen_blocks, 256, 0, s>>>(dwork, dorder, (uint32_t)n_curves,
+                                                (uint32_t)n_work, (uint32_t)n_pdt,
                                                 (uint32_t)n_per);
     if ((e = cudaGetLastError()) != cudaSuccess)
         return fail(err, err_len, PF_ECUDA, "work-list kernel: %s", cudaGetErrorString(e));
@@ -198,7 +205,11 @@ extern "C" int pf_ls_peaks_dev_noalloc(const float* d_times, const float* d_mags
     if ((e = launch_tmax(pt, total_pts, tmax, s)) != cudaSuccess)
         return fail(err, err_len, PF_ECUDA, "max|t| kernel: %s", cudaGetErrorString(e));
 
+    int n_sm = 0;
+    if ((e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return fail(err, err_len, PF_ECUDA, "device attribute: %s", cudaGetErrorString(e));
     FoldConfig cfg{};
+    cfg.n_sm = n_sm;
     cfg.kind = KIND_FOLD;
     cfg.algo = ALGO_LS;
     cfg.acc = 0;
@@ -225,6 +236,9 @@ extern "C" int pf_ls_peaks_dev_noalloc(const float* d_times, const float* d_mags
     p.p_overlap = 1;
     p.m_overlap = 1;
     p.tmax_bits = tmax;
+    p.q.order = dorder;
+    p.q.n_work = (uint32_t)n_work;
+    p.q.next = reinterpret_cast<unsigned*>(base + o_queue);
     e = (mode & PF_SEM_CPU) ? launch_fold_cpusem(cfg, p, (uint32_t)n_work, s)
                             : launch_fold_cudasem(cfg, p, (uint32_t)n_work, s);
     if (e != cudaSuccess) return fail(err, err_len, PF_ECUDA, "LS kernel: %s", cudaGetErrorString(e));

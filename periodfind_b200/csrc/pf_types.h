@@ -47,6 +47,18 @@ struct WorkItem {
     uint32_t np;
 };
 
+// Device work queue of the persistent (chosen-form) kernels.  Item k of a
+// launch is curve order[k / (n_pdt * tiles)], then period derivative and
+// tile of BLOCK consecutive periods from the remainder (tiles =
+// ceil(n_per / BLOCK)); CTAs take items from *next, which is zeroed before
+// the launch.  `order` lists the curves longest first, so the long items
+// start first and the short ones fill the tail.
+struct WorkQueue {
+    const uint32_t* order;
+    uint32_t n_work;
+    unsigned* next;
+};
+
 struct FoldParams {
     const float* t;          // packed times
     const float* m;          // packed magnitudes (AOV F32, LS)
@@ -63,6 +75,7 @@ struct FoldParams {
     const unsigned* tmax_bits;  // float bits of max |t| over the batch
     uint32_t edge_d;            // bin-edge guard (units of 2^-20 of a bin)
     unsigned long long* stamps; // optional: [work item][start, end] globaltimer ns
+    WorkQueue q;                // persistent kernels (instead of `work`)
 };
 
 // Shared-memory bytes of the chosen bin kernel (pf_bin.cuh).

@@ -471,3 +471,27 @@ def test_per_curve_device_timestamps(gpu, algo, mode):
         outs.append(out.cpu().numpy())
     np.testing.assert_array_equal(outs[0], outs[1])
     assert np.all(lat > 0) and np.all(lat <= wall_ns), lat
+
+
+def test_autotuned_launch_shapes_change_no_value(gpu):
+    """Curves in every length class: the autotuner picks a launch shape per
+    class (block size, persistent or one CTA per item); the values equal the
+    untuned launch's bit for bit, and the report lists the tuned classes."""
+    from periodfind_b200 import _native as nat
+
+    lengths = [10, 40, 63, 64, 100, 255, 256, 700, 1023, 1024, 3000, 4095, 4096, 6000]
+    ts, ms = _ragged(seed=41, lengths=lengths)
+    msn = [lc.normalize(m) for m in ms]
+    P, D = _grid(900, pdts=(0.0, 2e-5))
+    ctx = nat.default_context(0)
+    for make, mags in ((lambda **k: gpu.ConditionalEntropy(**k), msn),
+                       (lambda **k: gpu.AOV(15, **k), ms),
+                       (lambda **k: gpu.LombScargle(**k), [lc.center(m) for m in ms])):
+        tuned = make(mode="chosen").periodograms(ts, mags, P, D)
+        untuned_obj = make(mode="chosen")
+        untuned_obj._flags |= nat.PF_NO_TUNE
+        np.testing.assert_array_equal(tuned, untuned_obj.periodograms(ts, mags, P, D))
+    report = ctx.tuning_report()
+    for name in ("[0,64)", "[64,256)", "[256,1024)", "[1024,4096)", "[4096,inf)"):
+        assert f"class={name}" in report, report
+    assert "ce bin" in report and "aov bin" in report and "ls fold-split" in report
