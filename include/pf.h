@@ -209,6 +209,36 @@ int pf_ls_peaks_dev_noalloc(const float* d_times, const float* d_mags,
                             int64_t* d_out_idx, float* d_out_val, void* stream,
                             char* err, uint64_t err_len);
 
+/* ------------------------------------------------------------ batch plans
+ * No counterpart in the reference, whose drivers copy, launch and
+ * synchronise per call.  A plan records the whole device pipeline for one
+ * fixed batch shape -- curve packing, preparation kernels, the chosen
+ * kernels' per-length-class queue launches (tuned when the plan is made),
+ * and the optional top-N peak search -- as one CUDA graph, which
+ * pf_plan_launch replays on any stream.  The device buffers named at
+ * creation (times, magnitudes, grids, outputs) are read and written at each
+ * launch, so a caller may refill the inputs in place between launches; the
+ * curve offsets are copied and fixed.  Creation runs the pipeline once
+ * eagerly (tuning, buffer sizing) and synchronises.  A plan owns a private
+ * context; plans do not share buffers with each other or with contexts.
+ * Launches of one plan must not overlap on the GPU (they share its
+ * buffers).  n_peaks = 0: periodogram only.  PF_TIMING is rejected. */
+#define PF_ALGO_CE 0
+#define PF_ALGO_AOV 1
+#define PF_ALGO_LS 2
+typedef struct pf_plan pf_plan;
+int pf_plan_create(int device, int algo, const float* d_times, const float* d_mags,
+                   const int64_t* offsets, uint64_t n_curves, const float* d_periods,
+                   uint64_t n_per, const float* d_pdts, uint64_t n_pdt, uint32_t n_phase,
+                   uint32_t n_mag, uint32_t phase_overlap, uint32_t mag_overlap, int mode,
+                   float* d_out, uint32_t n_peaks, uint32_t min_distance, int64_t* d_peak_idx,
+                   float* d_peak_val, pf_plan** out);
+int pf_plan_launch(pf_plan* plan, void* stream);
+/* Last failure of this plan's launches; with NULL, of the last failed
+ * pf_plan_create on this thread. */
+const char* pf_plan_error(const pf_plan* plan);
+void pf_plan_destroy(pf_plan* plan);
+
 /* Per-curve device latency of the last PF_TIMING launch on this context:
  * out_ns[c] = last end - first start (ns) over the CTAs that computed curve
  * c's periodogram; n_curves must be that launch's.  Synchronises the

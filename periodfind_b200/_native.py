@@ -31,6 +31,7 @@ PF_FOLD_EXACT = 0x400
 PF_TIMING = 0x1000
 PF_REF_STATS = 0x2000
 PF_NO_TUNE = 0x4000
+PF_ALGO_CE, PF_ALGO_AOV, PF_ALGO_LS = 0, 1, 2
 
 _vp = ctypes.c_void_p
 _u64 = ctypes.c_uint64
@@ -70,6 +71,11 @@ SIGNATURES = {
                             _vp], _int),
     "pf_ls_refine_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _vp, _u64, _u32, _vp, _vp, _vp], _int),
     "pf_tuning_report": ([_vp, ctypes.c_char_p, _u64], _int),
+    "pf_plan_create": ([_int, _int, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32,
+                        _u32, _int, _vp, _u32, _u32, _vp, _vp, ctypes.POINTER(_vp)], _int),
+    "pf_plan_launch": ([_vp, _vp], _int),
+    "pf_plan_error": ([_vp], ctypes.c_char_p),
+    "pf_plan_destroy": ([_vp], None),
     "pf_launch_count": ([_vp], _u64),
     "pf_last_kernel_ms": ([_vp], ctypes.c_double),
 }

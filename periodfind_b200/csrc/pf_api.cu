@@ -1323,6 +1323,145 @@ int pf_find_peaks_dev(pf_ctx* ctx, const float* d_data, uint64_t n_curves, uint6
     return PF_OK;
 }
 
+// ------------------------------------------------------------- batch plans
+
+}  // extern "C"
+
+struct pf_plan {
+    pf_ctx* ctx = nullptr;  // private: its buffers and staging belong to the plan
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+struct PlanArgs {
+    Job j;
+    const float* d_times;
+    const float* d_mags;
+    std::vector<int64_t> offsets;
+    uint32_t n_peaks, min_distance;
+    int64_t* d_peak_idx;
+    float* d_peak_val;
+};
+
+// The plan's work on `s`: the device-pointer pipeline, then the peak search.
+int plan_enqueue(pf_ctx* ctx, const PlanArgs& a, cudaStream_t s) {
+    int rc = run_dev(ctx, a.j, a.d_times, a.d_mags, a.offsets.data(), s);
+    if (rc != PF_OK) return rc;
+    if (a.n_peaks > 0 && a.j.n_curves > 0 && a.j.n_per * a.j.n_pdt > 0) {
+        PF_CUDA(launch_peaks(a.j.out, a.j.n_curves, a.j.n_per * a.j.n_pdt, a.n_peaks,
+                             a.min_distance, a.j.algo == ALGO_CE ? 0 : 1, a.d_peak_idx,
+                             a.d_peak_val, s),
+                "peak kernel launch");
+        ctx->launches++;
+    }
+    return PF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pf_plan_create(int device, int algo, const float* d_times, const float* d_mags,
+                   const int64_t* offsets, uint64_t n_curves, const float* d_periods,
+                   uint64_t n_per, const float* d_pdts, uint64_t n_pdt, uint32_t n_phase,
+                   uint32_t n_mag, uint32_t phase_overlap, uint32_t mag_overlap, int mode,
+                   float* d_out, uint32_t n_peaks, uint32_t min_distance, int64_t* d_peak_idx,
+                   float* d_peak_val, pf_plan** out) {
+    if (!out) return PF_EINVAL;
+    *out = nullptr;
+    if (algo != PF_ALGO_CE && algo != PF_ALGO_AOV && algo != PF_ALGO_LS) {
+        g_create_error = "algo must be PF_ALGO_CE, PF_ALGO_AOV or PF_ALGO_LS";
+        return PF_EINVAL;
+    }
+    if (mode & PF_TIMING) {
+        g_create_error = "PF_TIMING is not available in a plan";
+        return PF_EINVAL;
+    }
+    if (!offsets || !d_out || (n_peaks > 0 && (!d_peak_idx || !d_peak_val))) {
+        g_create_error = "NULL argument";
+        return PF_EINVAL;
+    }
+    PlanArgs a;
+    a.j.algo = algo == PF_ALGO_CE ? ALGO_CE : algo == PF_ALGO_AOV ? ALGO_AOV : ALGO_LS;
+    a.j.mode = mode;
+    a.j.n_curves = n_curves;
+    a.j.periods = d_periods;
+    a.j.n_per = n_per;
+    a.j.pdts = d_pdts;
+    a.j.n_pdt = n_pdt;
+    a.j.n_phase = n_phase;
+    a.j.n_mag = n_mag;
+    a.j.po = phase_overlap;
+    a.j.mo = mag_overlap;
+    a.j.out = d_out;
+    a.d_times = d_times;
+    a.d_mags = d_mags;
+    a.offsets.assign(offsets, offsets + n_curves + 1);
+    a.n_peaks = n_peaks;
+    a.min_distance = min_distance;
+    a.d_peak_idx = d_peak_idx;
+    a.d_peak_val = d_peak_val;
+
+    pf_plan* plan = new pf_plan();
+    int rc = pf_ctx_create(&plan->ctx, device);
+    if (rc != PF_OK) {
+        delete plan;
+        return rc;
+    }
+    pf_ctx* ctx = plan->ctx;
+    auto bail = [&](int code) {
+        g_create_error = ctx->err;
+        pf_plan_destroy(plan);
+        return code;
+    };
+    // Eager pass: tunes the launch shapes, sizes every buffer, loads kernels.
+    cudaStream_t s = ctx->stream;
+    if ((rc = plan_enqueue(ctx, a, s)) != PF_OK) return bail(rc);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "plan warm-up"));
+    ctx->staged_pending = false;
+    ctx->done_recorded = false;
+    ctx->timed_pending = false;
+    // Captured pass: the same calls find the tuned shapes and sized buffers,
+    // so nothing allocates or synchronises while the stream is captured.
+    if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+        return bail(cuda_fail(ctx, e, "begin capture"));
+    rc = plan_enqueue(ctx, a, s);
+    e = cudaStreamEndCapture(s, &plan->graph);
+    ctx->staged_pending = false;
+    ctx->done_recorded = false;
+    ctx->timed_pending = false;
+    if (rc != PF_OK) return bail(rc);
+    if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "end capture"));
+    if ((e = cudaGraphInstantiate(&plan->exec, plan->graph, 0)) != cudaSuccess)
+        return bail(cuda_fail(ctx, e, "graph instantiate"));
+    *out = plan;
+    return PF_OK;
+}
+
+int pf_plan_launch(pf_plan* plan, void* stream) {
+    if (!plan || !plan->exec) return PF_EINVAL;
+    pf_ctx* ctx = plan->ctx;
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    PF_CUDA(cudaGraphLaunch(plan->exec, (cudaStream_t)stream), "graph launch");
+    return PF_OK;
+}
+
+const char* pf_plan_error(const pf_plan* plan) {
+    return plan ? plan->ctx->err.c_str() : g_create_error.c_str();
+}
+
+void pf_plan_destroy(pf_plan* plan) {
+    if (!plan) return;
+    if (plan->ctx) cudaSetDevice(plan->ctx->device);
+    if (plan->exec) cudaGraphExecDestroy(plan->exec);
+    if (plan->graph) cudaGraphDestroy(plan->graph);
+    if (plan->ctx) pf_ctx_destroy(plan->ctx);
+    delete plan;
+}
+
 int pf_find_peaks(pf_ctx* ctx, const float* data, uint64_t n_curves, uint64_t flat_len,
                   uint32_t n_peaks, uint32_t min_distance, int use_max, int64_t* out_idx,
                   float* out_val) {

@@ -147,3 +147,79 @@ def test_lsst_like_cadence(gpu):
                 continue
             got = obj.calc([t], [m], P, ZERO)[0].params[0]
             assert any(abs(got - c) / c < 0.01 for c in (true_p, true_p / 2, 2 * true_p)), got
+
+
+@pytest.mark.parametrize("algo", ["ce", "aov", "ls"])
+def test_batch_plan_replays_the_pipeline(algo):
+    """A plan (the device pipeline captured as a CUDA graph) gives the direct
+    call's periodogram and peaks on two launches in a row, and follows new
+    data written into its input buffers in place."""
+    import torch
+
+    from periodfind_b200 import _native as nat
+    from periodfind_b200.plan import BatchPlan
+
+    rng = np.random.default_rng(5)
+    lengths = [30, 300, 1200, 80, 5000, 7]
+    ts = [lc.uniform_times(rng, n, 500.0) for n in lengths]
+    ms = [lc.normalize(lc.noisy(rng, lc.sinusoid(t, 3.3), 0.1)).astype(np.float32) for t in ts]
+    off = np.zeros(len(ts) + 1, np.int64)
+    np.cumsum(lengths, out=off[1:])
+    d_t = torch.from_numpy(np.concatenate(ts)).cuda()
+    d_m = torch.from_numpy(np.concatenate(ms)).cuda()
+    P = torch.from_numpy(np.linspace(0.5, 12.0, 700).astype(np.float32)).cuda()
+    D = torch.tensor([0.0, 1e-5], dtype=torch.float32, device="cuda")
+    shape = (len(ts), 700, 2)
+    out = torch.empty(shape, device="cuda")
+    pidx = torch.empty((len(ts), 8), dtype=torch.int64, device="cuda")
+    pval = torch.empty((len(ts), 8), device="cuda")
+    plan = BatchPlan(algo, d_t, d_m, off, P, D, out, n_phase=12, n_mag=8, n_peaks=8,
+                     peak_idx=pidx, peak_val=pval)
+    ctx = nat.default_context(0)
+
+    def direct():
+        ref = torch.empty(shape, device="cuda")
+        ri = torch.empty((len(ts), 8), dtype=torch.int64, device="cuda")
+        rv = torch.empty((len(ts), 8), device="cuda")
+        c = (ctx.handle, d_t.data_ptr(), d_m.data_ptr(), off.ctypes.data, len(ts), P.data_ptr(),
+             700, D.data_ptr(), 2)
+        with ctx.lock:
+            if algo == "ce":
+                ctx.check(ctx.lib.pf_ce_dev(*c, 12, 8, 1, 1, nat.PF_MODE_CHOSEN, ref.data_ptr(), 0))
+            elif algo == "aov":
+                ctx.check(ctx.lib.pf_aov_dev(*c, 12, 1, nat.PF_MODE_CHOSEN, ref.data_ptr(), 0))
+            else:
+                ctx.check(ctx.lib.pf_ls_dev(*c, nat.PF_MODE_CHOSEN, ref.data_ptr(), 0))
+            ctx.check(ctx.lib.pf_find_peaks_dev(ctx.handle, ref.data_ptr(), len(ts), 1400, 8, 1,
+                                                0 if algo == "ce" else 1, ri.data_ptr(),
+                                                rv.data_ptr(), 0))
+        torch.cuda.synchronize()
+        return ref, ri, rv
+
+    for _ in range(2):
+        out.fill_(-7.0)
+        plan.launch()
+        torch.cuda.synchronize()
+        ref, ri, rv = direct()
+        assert torch.equal(out, ref) and torch.equal(pidx, ri) and torch.equal(pval, rv)
+    # refill the magnitudes in place: the next launch follows them
+    d_m.copy_(torch.from_numpy(np.concatenate(
+        [lc.normalize(rng.normal(size=n).astype(np.float32)) for n in lengths])).cuda())
+    plan.launch()
+    torch.cuda.synchronize()
+    ref, ri, rv = direct()
+    assert torch.equal(out, ref) and torch.equal(pidx, ri)
+    plan.close()
+
+
+def test_batch_plan_rejects_bad_arguments():
+    import ctypes
+
+    from periodfind_b200 import _native as nat
+
+    lib = nat.load()
+    h = ctypes.c_void_p()
+    off = np.array([0, 3], np.int64)
+    rc = lib.pf_plan_create(0, 7, None, None, off.ctypes.data, 1, None, 1, None, 1, 10, 10, 1, 1,
+                            nat.PF_MODE_CHOSEN, None, 0, 1, None, None, ctypes.byref(h))
+    assert rc == nat.PF_EINVAL and b"algo" in lib.pf_plan_error(None)
