@@ -446,6 +446,85 @@ def ragged_arm(args):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------ small CE batch
+
+
+def small_arm(args):
+    """CE 10 x 10 on 100 curves x 1024 points (times uniform in [0, 1000] d,
+    15 + 0.3 sin(2 pi t / P + phi) + N(0, 0.05^2), P ~ U[0.5, 10] d) over
+    1000 periods linspace(0.5, 10) d, period_dts [0], output 'stats'.
+    Device time of the chosen and plain forms, end-to-end calc() time, bin
+    agreement of the two forms, and the CPU port on all host cores."""
+    import torch
+
+    from periodfind_b200 import _native as nat
+    from periodfind_b200 import gpu
+
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(SEED + 1)
+    n_curves, n_pts = 100, 1024
+    ts, ms = [], []
+    for _ in range(n_curves):
+        t = np.sort(rng.uniform(0.0, 1000.0, n_pts)).astype(np.float32)
+        per, ph = rng.uniform(0.5, 10.0), rng.uniform(0.0, 2 * np.pi)
+        m = 15.0 + 0.3 * np.sin(2 * np.pi * t.astype(np.float64) / per + ph)
+        ts.append(t)
+        ms.append((m + rng.normal(0.0, 0.05, n_pts)).astype(np.float32))
+    periods = np.linspace(0.5, 10.0, 1000).astype(np.float32)
+    pdts = np.zeros(1, np.float32)
+    evals = n_curves * n_pts * len(periods)
+    msn = [((m - m.min()) / (m.max() - m.min()) * np.float32(0.999) + np.float32(5e-4))
+           .astype(np.float32) for m in ms]
+    off = np.arange(n_curves + 1, dtype=np.int64) * n_pts
+    d_t = torch.from_numpy(np.concatenate(ts)).cuda()
+    d_m = torch.from_numpy(np.concatenate(msn)).cuda()
+    d_p = torch.from_numpy(periods).cuda()
+    d_d = torch.from_numpy(pdts).cuda()
+    pg = torch.empty((n_curves, len(periods)), device="cuda")
+    ctx = nat.default_context(0)
+    s = torch.cuda.current_stream().cuda_stream
+    out = {"workload": "CE 10x10 stats, 100 curves x 1024 points x 1000 periods "
+                       "linspace(0.5, 10) d, period_dts [0]", "evals": evals}
+    for mode, flags in (("chosen", nat.PF_MODE_CHOSEN), ("plain", nat.PF_MODE_PLAIN)):
+        def run(flags=flags):
+            ctx.check(ctx.lib.pf_ce_dev(ctx.handle, d_t.data_ptr(), d_m.data_ptr(),
+                                        off.ctypes.data, n_curves, d_p.data_ptr(), len(periods),
+                                        d_d.data_ptr(), 1, 10, 10, 1, 1, flags, pg.data_ptr(), s))
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        k = []
+        for _ in range(max(3, args.steps)):
+            run()
+            torch.cuda.synchronize()
+            k.append(ctx.lib.pf_last_kernel_ms(ctx.handle))
+        obj = gpu.ConditionalEntropy(10, 10, mode=mode)
+        obj.calc(ts, ms, periods, pdts, output="stats")
+        w = []
+        for _ in range(max(3, args.steps)):
+            t0 = time.perf_counter()
+            obj.calc(ts, ms, periods, pdts, output="stats")
+            w.append(time.perf_counter() - t0)
+        kms, ws = float(np.median(k)), float(np.median(w))
+        out[mode] = {"kernel_ms": kms, "evals_per_s": evals / (kms * 1e-3),
+                     "e2e_ms": ws * 1e3, "e2e_evals_per_s": evals / ws}
+    a = gpu.ConditionalEntropy(mode="plain").periodograms(ts, msn, periods, pdts)
+    b = gpu.ConditionalEntropy(mode="chosen", reference_stats=True).periodograms(
+        ts, msn, periods, pdts)
+    out["bins_identical_chosen_vs_plain"] = bool(np.array_equal(a, b))
+    out["chosen_over_plain"] = out["plain"]["kernel_ms"] / out["chosen"]["kernel_ms"]
+    if not args.no_cpu:
+        from oracle import oracle as O
+
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        O.ce(ts, msn, periods, pdts, 10, 10, n_threads=cores)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": evals / dt, "unit": "evals/s", "cores": cores,
+                               "kind": "port", "sample": f"all {n_curves} curves, {dt:.2f} s"}
+    print(json.dumps(out), flush=True)
+
+
 # ------------------------------------------------- LS derivatives and study
 
 
@@ -627,8 +706,9 @@ def main():
     ap.add_argument("--curves", type=int, default=N_CURVES)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "ragged", "lsgrad", "precision"],
-                    help="'ragged': the mixed ragged batch; 'lsgrad': LS derivatives and "
+                    choices=["batch", "small", "ragged", "lsgrad", "precision"],
+                    help="'small': CE stats on 100 x 1024; 'ragged': the mixed ragged batch; "
+                         "'lsgrad': LS derivatives and "
                          "Newton refinement; 'precision': LS folds on the precision-study "
                          "batch (separate reports, 1 GPU)")
     args = ap.parse_args()
@@ -636,7 +716,8 @@ def main():
         reference_arm(args)
         return
     if args.workload != "batch":
-        {"ragged": ragged_arm, "lsgrad": lsgrad_arm, "precision": precision_arm}[args.workload](args)
+        {"small": small_arm, "ragged": ragged_arm, "lsgrad": lsgrad_arm,
+         "precision": precision_arm}[args.workload](args)
         return
 
     import torch
