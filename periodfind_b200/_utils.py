@@ -26,13 +26,31 @@ def prepare_magnitudes(mags, center, normalize):
     if center:
         return [mag - np.mean(mag) for mag in mags]
     if normalize:
+        return _normalize_batch(mags)
+    return mags
+
+
+def _normalize_batch(mags):
+    """The per-curve normalisation over the whole batch at once: the same
+    elementwise float32 expression and exact per-curve min / max, so every
+    value equals the one-curve-at-a-time result.  Batches with an empty
+    curve, or not all float32 1-D, take the per-curve path (and its errors)."""
+    arrs = [np.asarray(m) for m in mags]
+    if not arrs or any(a.ndim != 1 or a.size == 0 or a.dtype != np.float32 for a in arrs):
         out = []
         for mag in mags:
             lo = np.min(mag)
             hi = np.max(mag)
             out.append(((mag - lo) / (hi - lo)) * 0.999 + 5e-4)
         return out
-    return mags
+    lens = np.fromiter((a.size for a in arrs), dtype=np.int64, count=len(arrs))
+    flat = np.concatenate(arrs)
+    starts = np.zeros(len(arrs), dtype=np.int64)
+    np.cumsum(lens[:-1], out=starts[1:])
+    lo = np.repeat(np.minimum.reduceat(flat, starts), lens)
+    hi = np.repeat(np.maximum.reduceat(flat, starts), lens)
+    res = ((flat - lo) / (hi - lo)) * 0.999 + 5e-4
+    return np.split(res, starts[1:])
 
 
 def validate_inputs(times, mags):

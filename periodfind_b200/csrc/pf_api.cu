@@ -71,6 +71,7 @@ struct pf_ctx {
     struct Tuned {
         int block;
         bool persist;
+        int rounds;
         float ms;        // sample time of the winner
         float ms_worst;  // and of the slowest candidate
         uint32_t candidates;
@@ -244,12 +245,14 @@ FoldConfig choose_config(pf_ctx* ctx, const Job& j, uint32_t max_len, bool& ok) 
     }
     c.acc = AOVACC_F32;
     c.n_sm = ctx->n_sm;
+    c.rounds = 1;
     c.ovl = (j.algo == ALGO_CE) ? (j.po > 1 || j.mo > 1) : (j.algo == ALGO_AOV && j.po > 1);
     if (chosen && !c.ovl && (j.algo == ALGO_CE || j.algo == ALGO_AOV) && max_len < 65536u) {
         c.kind = KIND_BIN;
         c.cnt16 = (j.algo == ALGO_CE);
         c.ref_stats = (j.mode & PF_REF_STATS) != 0;
-        c.persist = true;  // measured: the bin kernel gains from the persistent queue
+        // The reference statistic (parity tests) is built in one shape only.
+        c.persist = false;
     } else if (j.algo == ALGO_AOV && chosen &&
                (uint64_t)max_len * j.po < (1ull << (64 - kFixCountShift)) - 1ull) {
         c.acc = AOVACC_FIX;
@@ -446,8 +449,9 @@ const char* class_name(int c) {
 constexpr size_t kCounterOffset = 64;
 constexpr int kTuneCounter = kClasses;
 
-uint64_t queue_items(const Job& j, uint64_t n_curves, int block) {
-    return n_curves * j.n_pdt * ((j.n_per + block - 1) / block);
+// Items of a queue launch over n_curves curves, `per_item` periods each.
+uint64_t queue_items(const Job& j, uint64_t n_curves, int per_item) {
+    return n_curves * j.n_pdt * ((j.n_per + per_item - 1) / per_item);
 }
 
 std::string tune_key(const Job& j, const FoldConfig& c, int cls) {
@@ -484,6 +488,7 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
     if (it != ctx->tuned.end()) {
         out.block = it->second.block;
         out.persist = it->second.persist;
+        out.rounds = it->second.rounds;
         return PF_OK;
     }
     if (j.mode & PF_NO_TUNE) return PF_OK;
@@ -499,14 +504,19 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
     ps.stamps = nullptr;
     ps.q.order = p.q.order + s0;
     ps.q.next = reinterpret_cast<unsigned*>((char*)ctx->d_misc.p + kCounterOffset) + kTuneCounter;
-    pf_ctx::Tuned best{base.block, base.persist, 1e30f, 0.0f, 0};
+    pf_ctx::Tuned best{base.block, base.persist, base.rounds, 1e30f, 0.0f, 0};
+    // The reference statistic is built in one shape; the bin kernel's
+    // chosen statistic also in 4 rounds per item.
+    const bool shapes = !(base.kind == KIND_BIN && base.ref_stats);
     for (int block : {64, 128, 256}) {
         FoldConfig t = base;
         t.block = block;
         if (fold_smem(t, j.n_phase, j.n_mag) > ctx->smem_optin) continue;
-        for (bool persist : {false, true}) {
-            t.persist = persist;
-            const uint64_t nw = queue_items(j, k, block);
+        for (int shape = 0; shape < (shapes ? 4 : 1); shape++) {
+            t.persist = (shape & 1) != 0;
+            t.rounds = (base.kind == KIND_BIN && (shape & 2)) ? 4 : 1;
+            if (base.kind != KIND_BIN && (shape & 2)) continue;
+            const uint64_t nw = queue_items(j, k, item_periods(t));
             if (nw == 0 || nw > 0x7FFFFFFFull) continue;
             ps.q.n_work = (uint32_t)nw;
             float ms = 0.0f;
@@ -523,7 +533,8 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
             if (ms < best.ms) {
                 best.ms = ms;
                 best.block = block;
-                best.persist = persist;
+                best.persist = t.persist;
+                best.rounds = t.rounds;
             }
         }
     }
@@ -531,6 +542,7 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
     ctx->tuned[key] = best;
     out.block = best.block;
     out.persist = best.persist;
+    out.rounds = best.rounds;
     return PF_OK;
 }
 
@@ -560,7 +572,7 @@ int launch_classes(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig&
         if ((rc = tuned_config(ctx, j, cfg, c, r[c].c0, r[c].n, r[c].points, p, s, cc[c])) !=
             PF_OK)
             return rc;
-        total_items += queue_items(j, r[c].n, cc[c].block);
+        total_items += queue_items(j, r[c].n, item_periods(cc[c]));
     }
     if (total_items > 0x7FFFFFFFull) return fail(ctx, PF_EINVAL, "too much work for one launch");
     if (j.mode & PF_TIMING) {
@@ -574,7 +586,7 @@ int launch_classes(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig&
     uint64_t base = 0;
     for (int c = 0; c < kClasses; c++) {
         if (!r[c].n) continue;
-        const uint64_t nw = queue_items(j, r[c].n, cc[c].block);
+        const uint64_t nw = queue_items(j, r[c].n, item_periods(cc[c]));
         FoldParams pc = p;
         pc.q.order = p.q.order + r[c].c0;
         pc.q.n_work = (uint32_t)nw;
@@ -582,7 +594,7 @@ int launch_classes(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig&
         pc.stamps = nullptr;
         if (j.mode & PF_TIMING) {
             pc.stamps = (unsigned long long*)ctx->d_stamps.p + 2 * base;
-            const uint64_t tpc = queue_items(j, 1, cc[c].block);
+            const uint64_t tpc = queue_items(j, 1, item_periods(cc[c]));
             for (uint64_t k = 0; k < nw; k++)
                 ctx->stamp_curves[base + k] = L.order[r[c].c0 + k / tpc];
         }
@@ -965,8 +977,8 @@ int pf_tuning_report(const pf_ctx* ctx, char* buf, uint64_t len) {
     for (const auto& kv : ctx->tuned) {
         char line[320];
         snprintf(line, sizeof(line),
-                 "%s: block=%d %s sample_ms=%.3f slowest_ms=%.3f candidates=%u\n",
-                 kv.first.c_str(), kv.second.block,
+                 "%s: block=%d rounds=%d %s sample_ms=%.3f slowest_ms=%.3f candidates=%u\n",
+                 kv.first.c_str(), kv.second.block, kv.second.rounds,
                  kv.second.persist ? "persistent" : "one-cta-per-item", kv.second.ms,
                  kv.second.ms_worst, kv.second.candidates);
         out += line;

@@ -119,7 +119,7 @@ __device__ __forceinline__ double aov_sbx_fast(uint32_t tbase, uint32_t nP, uint
 //         summed, with the 1/n scale taken out of the logs);
 //   AOV = (n - nP)/(nP - 1) * s1 / s2, s1 = sum_b X_b^2 / c_b - X^2 / n,
 //         s2 = sum x^2 - sum_b X_b^2 / c_b (X_b the fixed-point bin sums).
-template <int ALGO, bool CNT16, int BLOCK, bool REF_STATS>
+template <int ALGO, bool CNT16, int BLOCK, bool REF_STATS, int ROUNDS>
 __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, uint32_t item) {
     extern __shared__ __align__(16) unsigned char smem[];
     BinPoint* tile = reinterpret_cast<BinPoint*>(smem);
@@ -130,29 +130,34 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
     const CurveDesc cd = p.curves[w.curve];
     const uint32_t n = cd.n;
     const int tid = threadIdx.x;
-    const bool active = (uint32_t)tid < w.np;
-    const uint32_t pi = w.p0 + (active ? (uint32_t)tid : 0u);
     const float period_dt = p.pdts[w.pdt];
     const uint32_t nP = p.n_phase, nM = p.n_mag;
-
-    Cell s;
-    cell_setup<FOLD_EXACT>(s, p.periods[pi], period_dt);
 
     // Counter layout: CE  [nP rows][W words][BLOCK] u32, W = nM or ceil(nM/2)
     //                 AOV [2][nP][BLOCK] u32 (count, fixed-point sum)
     const uint32_t W = (ALGO == ALGO_CE) ? (CNT16 ? (nM + 1) / 2 : nM) : 1;
     const uint32_t row_stride = W * BLOCK * 4;  // bytes per phase row
     const uint32_t slots = (ALGO == ALGO_CE) ? nP * W : 2 * nP;
-    for (uint32_t k = 0; k < slots; k++)
-        reinterpret_cast<uint32_t*>(cnt_raw)[k * BLOCK + tid] = 0u;
     const uint32_t tbase = cnt_base + tid * 4;
     const uint32_t sum_off = nP * BLOCK * 4;  // AOV: sums after counts
 
-    // Range guard for y = q * n * 2^20 (uniform over the CTA).  Non-finite
-    // periods or derivatives (device-pointer callers are not checked on the
-    // host) also take the generic loop, whose bins are always clamped.
-    const double qb = cta_qbound<BLOCK>(p, pi, period_dt);
-    const bool fin = isfinite(s.yhi) && isfinite(s.ylo) && isfinite(s.c);
+    // The item covers ROUNDS x BLOCK periods; thread tid takes period
+    // p0 + r * BLOCK + tid in round r.  Range guard for y = q * n * 2^20 over
+    // every round (uniform over the CTA).  The cell constants (1 / P as a
+    // double-double, pdt / 2P) are finite exactly when P is finite and non-zero
+    // and pdt is finite; non-finite periods or derivatives (device-pointer
+    // callers are not checked on the host) take the generic loop, whose bins
+    // are always clamped.
+    bool fin = isfinite(period_dt);
+    double my_pmin = INFINITY;
+#pragma unroll
+    for (int r = 0; r < ROUNDS; r++) {
+        const uint32_t j = (uint32_t)(r * BLOCK + tid);
+        const float per = p.periods[w.p0 + (j < w.np ? j : 0u)];
+        fin = fin && isfinite(per) && per != 0.0f;
+        my_pmin = fmin(my_pmin, fabs((double)per));
+    }
+    const double qb = cta_qbound_of<BLOCK>(p, my_pmin, period_dt);
     const bool fast = __syncthreads_and(fin ? 1 : 0) && qb * (double)nP < 1073741824.0;  // 2^30
 
     const double nd20 = (double)nP * 1048576.0;
@@ -162,41 +167,62 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
     const uint32_t edge_add = p.edge_d << 12;
     const uint32_t edge_lim = (2u * p.edge_d) << 12;
 
-    for (uint32_t base = 0; base < n; base += kBinTile) {
-        const uint32_t cnt = min(kBinTile, n - base);
-        __syncthreads();
-        {
-            const float4* gt = reinterpret_cast<const float4*>(p.t + cd.off + base);
-            const uint32_t n4 = (cnt + 3) >> 2;
-            if constexpr (ALGO == ALGO_CE) {
-                const uint4* ga = reinterpret_cast<const uint4*>(p.aux64 + cd.off + base);
-                for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
-                    const float4 q = gt[i4];
-                    const uint4 a01 = ga[2 * i4], a23 = ga[2 * i4 + 1];
-                    // Counter word within a phase row -> byte offset for this
-                    // CTA shape (the prepared data does not depend on BLOCK).
-                    constexpr uint32_t kColBytes = BLOCK * 4u;
-                    tile[4 * i4 + 0] = BinPoint{(double)q.x, a01.x * kColBytes, a01.y};
-                    tile[4 * i4 + 1] = BinPoint{(double)q.y, a01.z * kColBytes, a01.w};
-                    tile[4 * i4 + 2] = BinPoint{(double)q.z, a23.x * kColBytes, a23.y};
-                    tile[4 * i4 + 3] = BinPoint{(double)q.w, a23.z * kColBytes, a23.w};
-                }
-            } else {
-                const uint4* ga = reinterpret_cast<const uint4*>(p.aux32 + cd.off + base);
-                for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
-                    const float4 q = gt[i4];
-                    const uint4 a = ga[i4];
-                    tile[4 * i4 + 0] = BinPoint{(double)q.x, a.x, 0u};
-                    tile[4 * i4 + 1] = BinPoint{(double)q.y, a.y, 0u};
-                    tile[4 * i4 + 2] = BinPoint{(double)q.z, a.z, 0u};
-                    tile[4 * i4 + 3] = BinPoint{(double)q.w, a.w, 0u};
-                }
+    auto stage = [&](uint32_t base, uint32_t cnt) {
+        const float4* gt = reinterpret_cast<const float4*>(p.t + cd.off + base);
+        const uint32_t n4 = (cnt + 3) >> 2;
+        if constexpr (ALGO == ALGO_CE) {
+            const uint4* ga = reinterpret_cast<const uint4*>(p.aux64 + cd.off + base);
+            for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
+                const float4 q = gt[i4];
+                const uint4 a01 = ga[2 * i4], a23 = ga[2 * i4 + 1];
+                // Counter word within a phase row -> byte offset for this
+                // CTA shape (the prepared data does not depend on BLOCK).
+                constexpr uint32_t kColBytes = BLOCK * 4u;
+                tile[4 * i4 + 0] = BinPoint{(double)q.x, a01.x * kColBytes, a01.y};
+                tile[4 * i4 + 1] = BinPoint{(double)q.y, a01.z * kColBytes, a01.w};
+                tile[4 * i4 + 2] = BinPoint{(double)q.z, a23.x * kColBytes, a23.y};
+                tile[4 * i4 + 3] = BinPoint{(double)q.w, a23.z * kColBytes, a23.w};
+            }
+        } else {
+            const uint4* ga = reinterpret_cast<const uint4*>(p.aux32 + cd.off + base);
+            for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
+                const float4 q = gt[i4];
+                const uint4 a = ga[i4];
+                tile[4 * i4 + 0] = BinPoint{(double)q.x, a.x, 0u};
+                tile[4 * i4 + 1] = BinPoint{(double)q.y, a.y, 0u};
+                tile[4 * i4 + 2] = BinPoint{(double)q.z, a.z, 0u};
+                tile[4 * i4 + 3] = BinPoint{(double)q.w, a.w, 0u};
             }
         }
+    };
+    // A curve that fits one tile is staged once for every round.
+    const bool one_tile = n <= kBinTile;
+    if (one_tile) {
         __syncthreads();
+        stage(0, n);
+        __syncthreads();
+    }
+
+#pragma unroll 1
+    for (int r = 0; r < ROUNDS; r++) {
+    const uint32_t jr = (uint32_t)(r * BLOCK + tid);
+    const bool active = jr < w.np;
+    const uint32_t pi = w.p0 + (active ? jr : 0u);
+    Cell s;
+    cell_setup<FOLD_EXACT>(s, p.periods[pi], period_dt);
+    for (uint32_t k = 0; k < slots; k++)
+        reinterpret_cast<uint32_t*>(cnt_raw)[k * BLOCK + tid] = 0u;
+
+    for (uint32_t base = 0; base < n; base += kBinTile) {
+        const uint32_t cnt = min(kBinTile, n - base);
+        if (!one_tile) {
+            __syncthreads();
+            stage(base, cnt);
+            __syncthreads();
+        }
         if (!active) continue;
 
-        // One 128-bit shared load per point record.
+    // One 128-bit shared load per point record.
         auto load_point = [&](uint32_t i) -> BinPoint {
             const uint4 raw = reinterpret_cast<const uint4*>(tile)[i];
             return BinPoint{__hiloint2double((int)raw.y, (int)raw.x), raw.z, raw.w};
@@ -288,14 +314,11 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
             else body(std::false_type{}, std::false_type{});
         }
     }
-    // Every lane of the warp reaches this barrier (inactive lanes leave the
-    // item only after it and then wait at the queue loop's CTA barrier).
+    // Every lane of the warp reaches this barrier (inactive lanes skip the
+    // statistic after it).
     compiler_fence();
     __syncwarp();
-    if (!active) {
-        stamp_end(p, item);
-        return;
-    }
+    if (active) {
     const size_t out_idx =
         (size_t)w.curve * ((size_t)p.n_per * p.n_pdt) + (size_t)pi * p.n_pdt + w.pdt;
     uint32_t* cnt32 = reinterpret_cast<uint32_t*>(cnt_raw);
@@ -365,20 +388,23 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
         p.out[out_idx] = (float)(scale * (s1 / (s2 <= 0.0 ? 0.0 : s2)));
 #endif
     }
+    }  // active
+    }  // rounds
     stamp_end(p, item);
 }
 
 // Items from the device work queue (see WorkQueue), persistently or one CTA
-// per item.
-template <int ALGO, bool CNT16, int BLOCK, bool REF_STATS, bool PERSIST>
+// per item; an item is ROUNDS x BLOCK consecutive periods.
+template <int ALGO, bool CNT16, int BLOCK, bool REF_STATS, bool PERSIST, int ROUNDS>
 __global__ void __launch_bounds__(BLOCK, queue_min_blocks<ALGO, BLOCK>())
     bin_kernel(const FoldParams p) {
     if constexpr (PERSIST) {
-        for_each_queued_item<BLOCK>(p, [&](const WorkItem& w, uint32_t k) {
-            bin_item<ALGO, CNT16, BLOCK, REF_STATS>(p, w, k);
+        for_each_queued_item<BLOCK * ROUNDS>(p, [&](const WorkItem& w, uint32_t k) {
+            bin_item<ALGO, CNT16, BLOCK, REF_STATS, ROUNDS>(p, w, k);
         });
     } else {
-        bin_item<ALGO, CNT16, BLOCK, REF_STATS>(p, queue_item<BLOCK>(p, blockIdx.x), blockIdx.x);
+        bin_item<ALGO, CNT16, BLOCK, REF_STATS, ROUNDS>(
+            p, queue_item<BLOCK * ROUNDS>(p, blockIdx.x), blockIdx.x);
     }
 }
 

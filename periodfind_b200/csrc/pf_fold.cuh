@@ -147,11 +147,12 @@ __device__ __forceinline__ float fold_df(float t, const Cell& s) {
 }
 
 // Bound on |t_corr / P| over this CTA's cells: max|t| / min|P| +
-// |pdt| max|t|^2 / (2 min|P|^2).  All threads of the CTA must call it.
+// |pdt| max|t|^2 / (2 min|P|^2), min|P| over every thread's `my_min_abs_p`.
+// All threads of the CTA must call it.
 template <int BLOCK>
-__device__ double cta_qbound(const FoldParams& p, uint32_t pi, float period_dt) {
+__device__ double cta_qbound_of(const FoldParams& p, double my_min_abs_p, float period_dt) {
     __shared__ double warp_min[BLOCK / 32];
-    double mn = fabs((double)p.periods[pi]);
+    double mn = my_min_abs_p;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
     if ((threadIdx.x & 31) == 0) warp_min[threadIdx.x >> 5] = mn;
@@ -161,6 +162,11 @@ __device__ double cta_qbound(const FoldParams& p, uint32_t pi, float period_dt) 
     for (int k = 1; k < BLOCK / 32; k++) pmin = fmin(pmin, warp_min[k]);
     const double tmax = (double)__uint_as_float(*p.tmax_bits);
     return tmax / pmin + fabs((double)period_dt) * tmax * tmax / (2.0 * pmin * pmin);
+}
+
+template <int BLOCK>
+__device__ double cta_qbound(const FoldParams& p, uint32_t pi, float period_dt) {
+    return cta_qbound_of<BLOCK>(p, fabs((double)p.periods[pi]), period_dt);
 }
 
 // Optional per-work-item timing (%globaltimer, ns): the CTA's first thread

@@ -29,10 +29,16 @@ struct FoldConfig {
     bool ovl;   // general bin-overlap path
     bool ref_stats; // bin_kernel: the reference's statistic operation sequence
     bool persist;   // queue kernels: persistent grid instead of one CTA per item
+    int rounds;     // bin kernel: an item is rounds x block periods (1 or 4)
     int n_sm;       // persistent kernels: grid = n_sm x resident CTAs per SM
 };
 
 size_t fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag);
+
+// Periods in one work item of a queue kernel.
+inline int item_periods(const FoldConfig& c) {
+    return c.block * (c.kind == KIND_BIN && c.rounds > 1 ? c.rounds : 1);
+}
 
 // Semantics of the reference's CUDA build (-use_fast_math).
 cudaError_t launch_fold_cudasem(const FoldConfig& c, const FoldParams& p, uint32_t n_work,

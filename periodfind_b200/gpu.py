@@ -67,18 +67,16 @@ def unravel_peaks(peak_indices, peak_values, periods, period_dts, n_peaks):
     """Flat peak indices -> list (per curve) of lists of Statistics, stopping
     at the first -1 (periodfind/cpu/__init__.py:46-70)."""
     n_pdts = len(period_dts)
-    results = []
-    for ci in range(peak_indices.shape[0]):
-        curve = []
-        for pi in range(n_peaks):
-            k = peak_indices[ci, pi]
-            if k < 0:
-                break
-            curve.append(Statistics(
-                params=[float(periods[int(k // n_pdts)]), float(period_dts[int(k % n_pdts)])],
-                value=float(peak_values[ci, pi]), mean=0.0, std=1.0, median=0.0, mad=1.0))
-        results.append(curve)
-    return results
+    idx = np.asarray(peak_indices, dtype=np.int64)[:, :n_peaks]
+    valid = idx >= 0
+    # Each curve's list stops at its first -1.
+    count = np.where(valid.all(axis=1), idx.shape[1], np.argmin(valid, axis=1)).tolist()
+    safe = np.where(valid, idx, 0)
+    per = np.asarray(periods)[safe // n_pdts].astype(np.float64).tolist()
+    pdt = np.asarray(period_dts)[safe % n_pdts].astype(np.float64).tolist()
+    val = np.asarray(peak_values)[:, :n_peaks].astype(np.float64).tolist()
+    return [[Statistics([pr[k], dr[k]], vr[k], 0.0, 1.0, 0.0, 1.0) for k in range(cnt)]
+            for pr, dr, vr, cnt in zip(per, pdt, val, count)]
 
 
 class _Periodogram:
