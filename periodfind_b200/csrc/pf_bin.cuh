@@ -275,13 +275,26 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
                 for (uint32_t g = 0; g < cnt; g += 32) {
                     const uint32_t gend = min(g + 32u, cnt);
                     uint32_t emin = 0xFFFFFFFFu;
+                    if (gend - g == 32u) {
+                        // A full group unrolled completely: no loop control
+                        // per point (measured 10% faster than unrolling by 4).
+#pragma unroll
+                        for (uint32_t ii = 0; ii < 32u; ii++) {
+                            const BinPoint pt = load_point(g + ii);
+                            uint32_t ev;
+                            const uint32_t row = fast_bin(pt.t, has_pdt_tag, ev);
+                            emin = min(emin, ev);
+                            add(row, pt, 1u);
+                        }
+                    } else {
 #pragma unroll 4
-                    for (uint32_t i = g; i < gend; i++) {
-                        const BinPoint pt = load_point(i);
-                        uint32_t ev;
-                        const uint32_t row = fast_bin(pt.t, has_pdt_tag, ev);
-                        emin = min(emin, ev);
-                        add(row, pt, 1u);
+                        for (uint32_t i = g; i < gend; i++) {
+                            const BinPoint pt = load_point(i);
+                            uint32_t ev;
+                            const uint32_t row = fast_bin(pt.t, has_pdt_tag, ev);
+                            emin = min(emin, ev);
+                            add(row, pt, 1u);
+                        }
                     }
                     if (emin < edge_lim) {
                         for (uint32_t i = g; i < gend; i++) {
