@@ -295,6 +295,15 @@ int pf_ls_refine_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
                      const double* d_half_width, uint64_t n_freq, uint32_t n_steps,
                      double* d_omega, float* d_power, void* stream);
 
+/* The reference's normalize=True magnitude preparation
+ * (periodfind/_utils.py:39-45): out[c][i] = ((m - min) / (max - min)) * 0.999
+ * + 5e-4 per curve in float32, bit-identical to numpy's evaluation of that
+ * expression (one rounding per operation; NaN propagates through min / max).
+ * Host arrays; several host threads for large batches.  Empty curves are
+ * PF_EINVAL (numpy raises for them). */
+int pf_normalize_mags(const float* const* mags, const uint64_t* lengths, uint64_t n_curves,
+                      float* const* out);
+
 /* The autotuner's decisions on this context, one line per (computation,
  * length class): the launch shape kept and the sample times of the fastest
  * and slowest candidates.  Writes at most len bytes (NUL-terminated) and

@@ -31,10 +31,11 @@ def prepare_magnitudes(mags, center, normalize):
 
 
 def _normalize_batch(mags):
-    """The per-curve normalisation over the whole batch at once: the same
-    elementwise float32 expression and exact per-curve min / max, so every
-    value equals the one-curve-at-a-time result.  Batches with an empty
-    curve, or not all float32 1-D, take the per-curve path (and its errors)."""
+    """The per-curve normalisation of a whole batch in the native library:
+    the same float32 expression with exact per-curve min / max, so every
+    value equals numpy's one-curve-at-a-time result.  Batches with an empty
+    curve, or not all float32 1-D, take the per-curve numpy path (and its
+    errors)."""
     arrs = [np.asarray(m) for m in mags]
     if not arrs or any(a.ndim != 1 or a.size == 0 or a.dtype != np.float32 for a in arrs):
         out = []
@@ -43,14 +44,22 @@ def _normalize_batch(mags):
             hi = np.max(mag)
             out.append(((mag - lo) / (hi - lo)) * 0.999 + 5e-4)
         return out
-    lens = np.fromiter((a.size for a in arrs), dtype=np.int64, count=len(arrs))
-    flat = np.concatenate(arrs)
+    # In the native library (multithreaded, same float32 arithmetic).
+    from . import _native as nat
+
+    arrs = [np.ascontiguousarray(a) for a in arrs]
+    lens = np.fromiter((a.size for a in arrs), dtype=np.uint64, count=len(arrs))
+    flat = np.empty(int(lens.sum()), dtype=np.float32)
     starts = np.zeros(len(arrs), dtype=np.int64)
-    np.cumsum(lens[:-1], out=starts[1:])
-    lo = np.repeat(np.minimum.reduceat(flat, starts), lens)
-    hi = np.repeat(np.maximum.reduceat(flat, starts), lens)
-    res = ((flat - lo) / (hi - lo)) * 0.999 + 5e-4
-    return np.split(res, starts[1:])
+    np.cumsum(lens[:-1].astype(np.int64), out=starts[1:])
+    out = np.split(flat, starts[1:])
+    src = np.fromiter((a.ctypes.data for a in arrs), dtype=np.uintp, count=len(arrs))
+    dst = np.fromiter((o.ctypes.data for o in out), dtype=np.uintp, count=len(out))
+    rc = nat.load().pf_normalize_mags(src.ctypes.data, lens.ctypes.data, len(arrs),
+                                      dst.ctypes.data)
+    if rc != nat.PF_OK:
+        raise RuntimeError(f"magnitude normalisation failed ({rc})")
+    return out
 
 
 def validate_inputs(times, mags):

@@ -19,6 +19,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
+#include <limits>
 #include <map>
 #include <numeric>
 #include <string>
@@ -970,6 +972,51 @@ const char* pf_last_error(const pf_ctx* ctx) {
 }
 
 uint64_t pf_launch_count(const pf_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int pf_normalize_mags(const float* const* mags, const uint64_t* lengths, uint64_t n_curves,
+                      float* const* out) {
+    if (n_curves == 0) return PF_OK;
+    if (!mags || !lengths || !out) return PF_EINVAL;
+    uint64_t total = 0;
+    for (uint64_t c = 0; c < n_curves; c++) {
+        if (lengths[c] == 0) return PF_EINVAL;  // numpy's min/max of an empty array raise
+        if (!mags[c] || !out[c]) return PF_EINVAL;
+        total += lengths[c];
+    }
+    // Per curve: numpy's float32 min / max (NaN propagates), then
+    // ((m - lo) / (hi - lo)) * 0.999f + 5e-4f in single precision, one
+    // rounding per operation, as numpy evaluates the same expression.
+    auto one = [&](uint64_t c) {
+        const float* m = mags[c];
+        const uint64_t n = lengths[c];
+        float lo = m[0], hi = m[0];
+        bool nan = std::isnan(m[0]);
+        for (uint64_t i = 1; i < n; i++) {
+            const float v = m[i];
+            nan |= std::isnan(v);
+            lo = v < lo ? v : lo;
+            hi = v > hi ? v : hi;
+        }
+        if (nan) lo = hi = std::numeric_limits<float>::quiet_NaN();
+        // This unit is built with -ffp-contract=off: no fused multiply-add.
+        const float range = hi - lo;
+        float* o = out[c];
+        for (uint64_t i = 0; i < n; i++) o[i] = ((m[i] - lo) / range) * 0.999f + 5e-4f;
+    };
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const unsigned nthr = total > (1u << 20) ? hw : 1u;
+    if (nthr == 1) {
+        for (uint64_t c = 0; c < n_curves; c++) one(c);
+        return PF_OK;
+    }
+    std::vector<std::thread> th;
+    for (unsigned w = 0; w < nthr; w++)
+        th.emplace_back([&, w] {
+            for (uint64_t c = w; c < n_curves; c += nthr) one(c);
+        });
+    for (auto& t : th) t.join();
+    return PF_OK;
+}
 
 int pf_tuning_report(const pf_ctx* ctx, char* buf, uint64_t len) {
     if (!ctx) return PF_EINVAL;

@@ -173,3 +173,30 @@ def test_mode_and_semantics_validation():
         gpu.AOV(semantics="rust")
     assert gpu.AOV(mode="plain", semantics="cpu")._flags == _native.PF_SEM_CPU
     assert gpu.LombScargle(fold="df")._flags & _native.PF_FOLD_DF
+
+
+def test_native_normalisation_matches_numpy_bit_for_bit():
+    """prepare_magnitudes(normalize=True) runs in the native library for
+    float32 batches; every value equals numpy's evaluation of the reference
+    expression, including NaN / inf / constant / single-point / tiny curves."""
+    import warnings
+
+    from periodfind_b200._utils import prepare_magnitudes
+
+    rng = np.random.default_rng(12)
+    ms = [rng.normal(15, 0.3, int(n)).astype(np.float32) for n in rng.integers(1, 3000, 300)]
+    ms[3][5] = np.nan
+    ms[7][:] = 2.0
+    ms[9][2] = np.inf
+    ms[11] = np.array([1.0], np.float32)
+    ms[13] = (rng.normal(size=777) * 1e-30).astype(np.float32)
+    got = prepare_magnitudes(ms, False, True)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        want = [((m - np.min(m)) / (np.max(m) - np.min(m))) * 0.999 + 5e-4 for m in ms]
+    for g, w in zip(got, want):
+        assert g.dtype == w.dtype == np.float32
+        np.testing.assert_array_equal(g, w)
+    # an empty curve keeps numpy's error
+    with pytest.raises(ValueError):
+        prepare_magnitudes([np.zeros(0, np.float32)], False, True)
