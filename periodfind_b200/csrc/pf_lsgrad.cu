@@ -21,10 +21,10 @@
 // curve's time span, which keeps the t and t^2 weights small.  w does depend
 // on t0: every kernel here derives t0 the same way (exact min/max).
 //
-// Arithmetic: the phase omega dt / 2pi is reduced in FP64 (one multiply and
-// a round-to-nearest by the 1.5 * 2^52 shift), the sine and cosine and all
-// sums are FP32, and the closed form above is evaluated in FP64 once per
-// (curve, frequency).  Degenerate M (det <= 1e-6 CC SS, e.g. one point or
+// Arithmetic: the phase omega dt / 2pi is a split-precision FP32 product of
+// float pairs (FP64 for |f dt| >= 2^21 turns), the sine and cosine come from
+// the MUFU unit, all sums are FP32, and the closed form above is evaluated
+// in FP64 once per (curve, frequency).  Degenerate M (det <= 1e-6 CC SS, e.g. one point or
 // all phases equal) gives power 0 and zero derivatives, as the reference's
 // zero denominators give 0 (ls.cu:131-134).
 #include <cuda_runtime.h>
@@ -57,24 +57,56 @@ struct Sums {
     float C2, S2, CC2, CS2;
 };
 
-// A staged point: time from the curve's t0 in FP64 (for the phase), the
-// same in FP32 (the derivative weight), and the magnitude.
+// An unevaluated float pair hi + lo.  A time measured from the curve's t0
+// (t an f32, t0 the midpoint of two f32 values) has at most 26 significant
+// bits, so hi + lo holds it exactly.
+struct F2 {
+    float hi, lo;
+};
+__device__ __forceinline__ F2 split2(double v) {
+    F2 r;
+    r.hi = __double2float_rn(v);
+    r.lo = __double2float_rn(v - (double)r.hi);
+    return r;
+}
+
+// A staged point: its time from t0 as a float pair (dh is also the FP32
+// derivative weight) and its magnitude.
 struct __align__(16) StagedPoint {
-    double dt;
-    float x, y;
+    float dh, dl, y, unused;
 };
 
 struct Deriv {
     double P, P1, P2, alpha, beta;
 };
 
-// sin and cos of 2 pi * (f * dt reduced to [-0.5, 0.5]).
-__device__ __forceinline__ void phase_sincos(double f, double dt, float* s, float* c) {
+// Phase in turns of frequency f (turns per time unit) at time dt, reduced to
+// about [-0.5, 0.5].  Split precision (the default): the product of the two
+// float pairs as p + e, with p = RN(fh * dh) and e its exact rounding error
+// (one fma) plus the cross terms fh * dl + fl * dh (fl * dl is below 2^-40
+// of the product); the integer part is removed from p exactly (|p| < 2^22);
+// the phase is good to the f32 rounding of the result, as the FP64
+// reduction below.  Needs |f dt| < 2^21 (checked by the callers).
+__device__ __forceinline__ float phase_df(F2 f, F2 d) {
+    const float p = __fmul_rn(f.hi, d.hi);
+    float e = __fmaf_rn(f.hi, d.hi, -p);
+    e = __fmaf_rn(f.hi, d.lo, e);
+    e = __fmaf_rn(f.lo, d.hi, e);
+    const float n = __fsub_rn(__fadd_rn(p, 12582912.0f), 12582912.0f);  // rint, |p| < 2^22
+    return __fadd_rn(__fsub_rn(p, n), e);
+}
+// FP64 reduction for frequencies or spans beyond that range.
+__device__ __forceinline__ float phase_f64(double f, double dt) {
     const double u = f * dt;
     const double n = __dsub_rn(__dadd_rn(u, kShift), kShift);
-    const float r = (float)__dsub_rn(u, n);
-    sincospif(2.0f * r, s, c);
+    return (float)__dsub_rn(u, n);
 }
+// sine and cosine of 2 pi * phase (|phase| <= ~0.5): the MUFU unit (absolute
+// error ~4e-7, inside every tolerance of these derivatives).
+__device__ __forceinline__ void sincos_turns(float ph, float* s, float* c) {
+    __sincosf(6.28318530717958647692f * ph, s, c);
+}
+constexpr double kDfLimit = 2097152.0;  // 2^21 turns
 
 template <int ORDER>
 __device__ __forceinline__ void add_point(Sums& a, float x, float y, float s, float c) {
@@ -155,8 +187,10 @@ __device__ Deriv finish(const Sums& a, uint32_t n) {
 }
 
 // Midpoint of the curve's time span (exact min / max, so every kernel and
-// every CTA derives the same t0).  Block-wide; all threads must call it.
-__device__ double curve_t0(const float* __restrict__ t, int64_t o, uint32_t n) {
+// every CTA derives the same t0) and the half span.  Block-wide; all threads
+// must call it.
+__device__ double curve_t0(const float* __restrict__ t, int64_t o, uint32_t n,
+                           double* half_span) {
     __shared__ float red_lo[kLsWarps], red_hi[kLsWarps];
     float lo = INFINITY, hi = -INFINITY;
     for (uint32_t i = threadIdx.x; i < n; i += kLsThreads) {
@@ -183,6 +217,7 @@ __device__ double curve_t0(const float* __restrict__ t, int64_t o, uint32_t n) {
         lo = fminf(lo, red_lo[w]);
         hi = fmaxf(hi, red_hi[w]);
     }
+    *half_span = n ? 0.5 * ((double)hi - (double)lo) : 0.0;
     return n ? 0.5 * ((double)lo + (double)hi) : 0.0;
 }
 
@@ -201,7 +236,8 @@ __global__ void __launch_bounds__(kLsThreads)
     const int64_t o = p.off[c];
     const uint32_t n = (uint32_t)(p.off[c + 1] - o);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const double t0 = curve_t0(p.t, o, n);
+    double half_span;
+    const double t0 = curve_t0(p.t, o, n, &half_span);
     const uint32_t ntiles = (n + kLsTile - 1) / kLsTile;
     const uint32_t n_eval = REFINE ? p.n_steps + 1 : 1;
 
@@ -219,6 +255,8 @@ __global__ void __launch_bounds__(kLsThreads)
         }
         for (uint32_t e = 0; e < n_eval; e++) {
             const double f = w * kInv2Pi;
+            const F2 fp = split2(f);
+            const bool df = fabs(f) * half_span < kDfLimit;  // uniform per warp
             Sums a{};
             for (uint32_t tt = 0; tt < ntiles; tt++) {
                 const uint32_t base = tt * kLsTile;
@@ -226,16 +264,25 @@ __global__ void __launch_bounds__(kLsThreads)
                 if (ntiles > 1 || (j == 0 && e == 0)) {
                     __syncthreads();
                     for (uint32_t i = threadIdx.x; i < cnt; i += kLsThreads) {
-                        const double dt = (double)p.t[o + base + i] - t0;
-                        tile[i] = StagedPoint{dt, (float)dt, p.y[o + base + i]};
+                        const F2 d = split2((double)p.t[o + base + i] - t0);
+                        tile[i] = StagedPoint{d.hi, d.lo, p.y[o + base + i], 0.0f};
                     }
                     __syncthreads();
                 }
-                for (uint32_t i = lane; i < cnt; i += 32) {
-                    const StagedPoint q = tile[i];
-                    float s, cs;
-                    phase_sincos(f, q.dt, &s, &cs);
-                    add_point<ORDER>(a, q.x, q.y, s, cs);
+                if (df) {
+                    for (uint32_t i = lane; i < cnt; i += 32) {
+                        const StagedPoint q = tile[i];
+                        float s, cs;
+                        sincos_turns(phase_df(fp, F2{q.dh, q.dl}), &s, &cs);
+                        add_point<ORDER>(a, q.dh, q.y, s, cs);
+                    }
+                } else {
+                    for (uint32_t i = lane; i < cnt; i += 32) {
+                        const StagedPoint q = tile[i];
+                        float s, cs;
+                        sincos_turns(phase_f64(f, (double)q.dh + (double)q.dl), &s, &cs);
+                        add_point<ORDER>(a, q.dh, q.y, s, cs);
+                    }
                 }
             }
             warp_reduce<ORDER>(a);
@@ -281,6 +328,7 @@ __global__ void __launch_bounds__(kLsThreads)
 __global__ void __launch_bounds__(kLsThreads)
     ls_grad_kernel(LsGradParams p) {
     __shared__ double sf[kGradFreqTile];
+    __shared__ float sfh[kGradFreqTile], sfl[kGradFreqTile];
     __shared__ float sa[kGradFreqTile], sb[kGradFreqTile];
     const uint64_t c = blockIdx.y;
     const int64_t o = p.off[c];
@@ -288,28 +336,46 @@ __global__ void __launch_bounds__(kLsThreads)
     const uint32_t i = blockIdx.x * kLsThreads + threadIdx.x;
     const bool head = blockIdx.x == 0;
     if (!head && blockIdx.x * kLsThreads >= n) return;  // whole CTA past the curve
-    const double t0 = curve_t0(p.t, o, n);
+    double half_span;
+    const double t0 = curve_t0(p.t, o, n, &half_span);
     const bool have = i < n;
     const double dt = have ? (double)p.t[o + i] - t0 : 0.0;
+    const F2 d = split2(dt);
     float acc = 0.0f;
     for (uint64_t k0 = 0; k0 < p.n_freq; k0 += kGradFreqTile) {
         const uint32_t cnt = (uint32_t)min((uint64_t)kGradFreqTile, p.n_freq - k0);
         __syncthreads();
+        bool ok = true;
         for (uint32_t q = threadIdx.x; q < cnt; q += kLsThreads) {
             const uint64_t cell = c * p.n_freq + k0 + q;
             const float gp = p.grad_power[cell];
-            sf[q] = p.omega[c * p.omega_stride + k0 + q] * kInv2Pi;
+            const double f = p.omega[c * p.omega_stride + k0 + q] * kInv2Pi;
+            const F2 fp = split2(f);
+            sf[q] = f;
+            sfh[q] = fp.hi;
+            sfl[q] = fp.lo;
+            ok = ok && fabs(f) * half_span < kDfLimit;
             sa[q] = gp * p.coef[2 * cell];
             sb[q] = gp * p.coef[2 * cell + 1];
             if (head && p.grad_omega) p.grad_omega[cell] = (double)(gp * p.dpdw[cell]);
         }
-        __syncthreads();
+        // Every frequency of the tile within the split-precision range?
+        const bool df = __syncthreads_and(ok ? 1 : 0) != 0;
         if (p.grad_mags && have) {
-            for (uint32_t q = 0; q < cnt; q++) {
-                float s, cs;
-                phase_sincos(sf[q], dt, &s, &cs);
-                acc = fmaf(sa[q], cs, acc);
-                acc = fmaf(sb[q], s, acc);
+            if (df) {
+                for (uint32_t q = 0; q < cnt; q++) {
+                    float s, cs;
+                    sincos_turns(phase_df(F2{sfh[q], sfl[q]}, d), &s, &cs);
+                    acc = fmaf(sa[q], cs, acc);
+                    acc = fmaf(sb[q], s, acc);
+                }
+            } else {
+                for (uint32_t q = 0; q < cnt; q++) {
+                    float s, cs;
+                    sincos_turns(phase_f64(sf[q], dt), &s, &cs);
+                    acc = fmaf(sa[q], cs, acc);
+                    acc = fmaf(sb[q], s, acc);
+                }
             }
         }
     }
