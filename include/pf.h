@@ -149,6 +149,33 @@ int pf_ls_peaks(pf_ctx* ctx, const float* const* times,
                 uint32_t min_distance, int mode, int64_t* out_idx,
                 float* out_val);
 
+/* Periodogram + the 'stats' output computed on the device: what the
+ * reference's Statistics.statistics_from_data (periodfind/__init__.py:
+ * 338-400) derives from each curve's periodogram with numpy, with numpy's
+ * results bit for bit -- out_stats[4 * c + {0, 1, 2, 3}] = np.mean, np.std
+ * (float32, numpy's pairwise summation order), np.median, and the median of
+ * |data - median|; out_idx / out_val [n_curves][n_top] = the n_top best cells
+ * of the flattened [period][pdt] grid (smallest for CE, largest for AOV / LS;
+ * NaN ranks largest), best first, ties by lower index.  (For the largest,
+ * the reference partitions at len(data) - n, the period count, so with more
+ * than one period derivative its pick is numpy's partition order; callers
+ * wanting that exact behaviour use the periodogram.)  PF_EUNSUPPORTED when
+ * a row exceeds about 1.1e6 cells. */
+int pf_ce_stats(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                const uint64_t* lengths, uint64_t n_curves, const float* periods,
+                uint64_t n_per, const float* period_dts, uint64_t n_pdt, uint32_t n_phase,
+                uint32_t n_mag, uint32_t phase_overlap, uint32_t mag_overlap, uint32_t n_top,
+                int mode, float* out_stats, int64_t* out_idx, float* out_val);
+int pf_aov_stats(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                 const uint64_t* lengths, uint64_t n_curves, const float* periods,
+                 uint64_t n_per, const float* period_dts, uint64_t n_pdt, uint32_t n_phase,
+                 uint32_t phase_overlap, uint32_t n_top, int mode, float* out_stats,
+                 int64_t* out_idx, float* out_val);
+int pf_ls_stats(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                const uint64_t* lengths, uint64_t n_curves, const float* periods,
+                uint64_t n_per, const float* period_dts, uint64_t n_pdt, uint32_t n_top,
+                int mode, float* out_stats, int64_t* out_idx, float* out_val);
+
 /* Peak search alone on periodograms already on the host, [n_curves][flat];
  * replaces find_top_peaks_batched (rust/src/lib.rs:508-548). */
 int pf_find_peaks(pf_ctx* ctx, const float* data, uint64_t n_curves,

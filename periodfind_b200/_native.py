@@ -54,6 +54,12 @@ SIGNATURES = {
                       _int, _vp, _vp], _int),
     "pf_ls_peaks": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int, _vp,
                      _vp], _int),
+    "pf_ce_stats": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32,
+                     _u32, _int, _vp, _vp, _vp], _int),
+    "pf_aov_stats": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _int,
+                      _vp, _vp, _vp], _int),
+    "pf_ls_stats": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _int, _vp, _vp, _vp],
+                    _int),
     "pf_find_peaks": ([_vp, _vp, _u64, _u64, _u32, _u32, _int, _vp, _vp], _int),
     "pf_ce_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32, _int,
                    _vp, _vp], _int),

@@ -36,6 +36,7 @@ UNITS = {
     "pf_api.cu": ["-Xcompiler", "-ffp-contract=off"],  # host float32 arithmetic as numpy
     "pf_noalloc.cu": [],
     "pf_lsgrad.cu": [],
+    "pf_stats.cu": ["-fmad=false"],  # numpy's float32 arithmetic, one rounding per operation
 }
 
 LIB = os.path.join(HERE, "libpfb200.so")

@@ -57,7 +57,7 @@ struct pf_ctx {
     cudaEvent_t ev_done = nullptr;              // last device-pointer call done
     bool staged_pending = false, done_recorded = false, timed_pending = false;
     std::string err;
-    DevBuf d_in, d_aux32, d_aux64, d_out, d_pidx, d_pval, d_pack, d_misc, d_stamps;
+    DevBuf d_in, d_aux32, d_aux64, d_out, d_pidx, d_pval, d_pack, d_misc, d_stamps, d_stat;
     // PF_TIMING: the curve of each work item of the last timed launch, and
     // the stream it ran on.
     std::vector<uint32_t> stamp_curves;   // curve of each stamped work item
@@ -155,6 +155,11 @@ struct Job {
     uint32_t n_peaks = 0, min_distance = 1;
     int64_t* out_idx = nullptr;
     float* out_val = nullptr;
+    // 'stats' output on the device: per curve (mean, std, median, mad) into
+    // out_stats and the n_top best cells into out_idx / out_val.
+    bool stats = false;
+    uint32_t n_top = 0;
+    float* out_stats = nullptr;
 };
 
 // Layout of the packed input block (host staging and its device copy).
@@ -204,7 +209,14 @@ int validate_common(pf_ctx* ctx, const Job& j) {
     }
     if (j.peaks && (!j.out_idx || !j.out_val) && j.n_peaks > 0)
         return fail(ctx, PF_EINVAL, "peak outputs are NULL");
-    if (!j.peaks && !j.out && j.n_curves > 0) return fail(ctx, PF_EINVAL, "out is NULL");
+    if (j.stats && (!j.out_stats || (j.n_top > 0 && (!j.out_idx || !j.out_val))))
+        return fail(ctx, PF_EINVAL, "stats outputs are NULL");
+    if (j.stats && j.n_per * j.n_pdt > 0 && stats_leaf_count((uint32_t)std::min<uint64_t>(
+                                                   j.n_per * j.n_pdt, 0xFFFFFFFFull)) *
+                                                   12ull > 200ull * 1024ull)
+        return fail(ctx, PF_EUNSUPPORTED, "periodogram rows too long for the device statistics");
+    if (!j.peaks && !j.stats && !j.out && j.n_curves > 0)
+        return fail(ctx, PF_EINVAL, "out is NULL");
     return PF_OK;
 }
 
@@ -687,6 +699,17 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
         PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
         ctx->timed_pending = true;
     }
+    if (j.stats) {
+        const size_t pk = (size_t)j.n_curves * std::max<uint32_t>(j.n_top, 1u);
+        if ((rc = ensure_dev(ctx, ctx->d_pidx, pk * 8)) != PF_OK) return rc;
+        if ((rc = ensure_dev(ctx, ctx->d_pval, pk * 4)) != PF_OK) return rc;
+        if ((rc = ensure_dev(ctx, ctx->d_stat, (size_t)j.n_curves * 16)) != PF_OK) return rc;
+        PF_CUDA(launch_stats(d_out, j.n_curves, (uint32_t)(j.n_per * j.n_pdt),
+                             j.algo == ALGO_CE ? 0 : 1, j.n_top, (float*)ctx->d_stat.p,
+                             (int64_t*)ctx->d_pidx.p, (float*)ctx->d_pval.p, s),
+                "statistics kernel launch");
+        ctx->launches++;
+    }
     if (j.peaks && j.n_peaks > 0) {
         const size_t pk = (size_t)j.n_curves * j.n_peaks;
         if ((rc = ensure_dev(ctx, ctx->d_pidx, pk * 8)) != PF_OK) return rc;
@@ -778,7 +801,18 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
     rc = device_pipeline(ctx, j, L, cfg, p, (CurveDesc*)(db + L.o_curves), (float*)ctx->d_out.p,
                          s);
     if (rc != PF_OK) return rc;
-    if (!j.peaks) {
+    if (j.stats) {
+        PF_CUDA(cudaMemcpyAsync(j.out_stats, ctx->d_stat.p, (size_t)j.n_curves * 16,
+                                cudaMemcpyDeviceToHost, s),
+                "D2H statistics");
+        if (j.n_top > 0) {
+            const size_t pk = (size_t)j.n_curves * j.n_top;
+            PF_CUDA(cudaMemcpyAsync(j.out_idx, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
+                    "D2H best indices");
+            PF_CUDA(cudaMemcpyAsync(j.out_val, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s),
+                    "D2H best values");
+        }
+    } else if (!j.peaks) {
         PF_CUDA(cudaMemcpyAsync(j.out, ctx->d_out.p, out_bytes, cudaMemcpyDeviceToHost, s),
                 "D2H periodogram");
     } else if (j.n_peaks > 0) {
@@ -955,7 +989,7 @@ void pf_ctx_destroy(pf_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->done_recorded) cudaEventSynchronize(ctx->ev_done);
     for (DevBuf* b : {&ctx->d_in, &ctx->d_aux32, &ctx->d_aux64, &ctx->d_out, &ctx->d_pidx,
-                      &ctx->d_pval, &ctx->d_pack, &ctx->d_misc, &ctx->d_stamps})
+                      &ctx->d_pval, &ctx->d_pack, &ctx->d_misc, &ctx->d_stamps, &ctx->d_stat})
         if (b->p) cudaFree(b->p);
     if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -1519,6 +1553,74 @@ void pf_plan_destroy(pf_plan* plan) {
     if (plan->graph) cudaGraphDestroy(plan->graph);
     if (plan->ctx) pf_ctx_destroy(plan->ctx);
     delete plan;
+}
+
+int pf_ce_stats(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                const uint64_t* lengths, uint64_t n_curves, const float* periods,
+                uint64_t n_per, const float* period_dts, uint64_t n_pdt, uint32_t n_phase,
+                uint32_t n_mag, uint32_t phase_overlap, uint32_t mag_overlap, uint32_t n_top,
+                int mode, float* out_stats, int64_t* out_idx, float* out_val) {
+    Job j;
+    j.algo = ALGO_CE;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = period_dts;
+    j.n_pdt = n_pdt;
+    j.n_phase = n_phase;
+    j.n_mag = n_mag;
+    j.po = phase_overlap;
+    j.mo = mag_overlap;
+    j.stats = true;
+    j.n_top = n_top;
+    j.out_stats = out_stats;
+    j.out_idx = out_idx;
+    j.out_val = out_val;
+    return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_aov_stats(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                 const uint64_t* lengths, uint64_t n_curves, const float* periods,
+                 uint64_t n_per, const float* period_dts, uint64_t n_pdt, uint32_t n_phase,
+                 uint32_t phase_overlap, uint32_t n_top, int mode, float* out_stats,
+                 int64_t* out_idx, float* out_val) {
+    Job j;
+    j.algo = ALGO_AOV;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = period_dts;
+    j.n_pdt = n_pdt;
+    j.n_phase = n_phase;
+    j.po = phase_overlap;
+    j.stats = true;
+    j.n_top = n_top;
+    j.out_stats = out_stats;
+    j.out_idx = out_idx;
+    j.out_val = out_val;
+    return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_ls_stats(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                const uint64_t* lengths, uint64_t n_curves, const float* periods,
+                uint64_t n_per, const float* period_dts, uint64_t n_pdt, uint32_t n_top,
+                int mode, float* out_stats, int64_t* out_idx, float* out_val) {
+    Job j;
+    j.algo = ALGO_LS;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = period_dts;
+    j.n_pdt = n_pdt;
+    j.stats = true;
+    j.n_top = n_top;
+    j.out_stats = out_stats;
+    j.out_idx = out_idx;
+    j.out_val = out_val;
+    return run_host(ctx, j, times, mags, lengths);
 }
 
 int pf_find_peaks(pf_ctx* ctx, const float* data, uint64_t n_curves, uint64_t flat_len,

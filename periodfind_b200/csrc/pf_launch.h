@@ -122,6 +122,16 @@ cudaError_t launch_ls_eval(const LsEvalParams& p, int order, cudaStream_t stream
 cudaError_t launch_ls_refine(const LsEvalParams& p, cudaStream_t stream);
 cudaError_t launch_ls_grad(const LsGradParams& p, uint32_t max_len, cudaStream_t stream);
 
+// 'stats' output (pf_stats.cu): per row of [n_curves][n_cells], numpy's
+// mean / std / median / MAD into stats[4 * c + {0..3}] and the n_top best
+// cells, best first (use_max: largest).  stats_leaf_count is the number of
+// leaves of numpy's pairwise summation over n elements (12 B of shared
+// memory each).
+uint32_t stats_leaf_count(uint32_t n);
+cudaError_t launch_stats(const float* pg, uint64_t n_curves, uint32_t n_cells, int use_max,
+                         uint32_t n_top, float* stats, int64_t* top_idx, float* top_val,
+                         cudaStream_t stream);
+
 // Peak search (pf_peaks.cu): one CTA per curve over a [n_curves][flat]
 // periodogram; rust/src/peaks.rs semantics.
 cudaError_t launch_peaks(const float* pg, uint64_t n_curves, uint64_t flat_len,

@@ -122,6 +122,21 @@ class _Periodogram:
                                          int(min_distance), idx, val))
         return idx, val
 
+    def _stats_on_device(self, times, mags, periods, period_dts, n_stats, significance_type):
+        """The 'stats' output with the statistics computed on the device
+        (identical to numpy's); None where the device path does not apply."""
+        ctx = nat.default_context(self.device)
+        b = nat.CurveBatch(times, mags)
+        st = np.empty((b.n, 4), dtype=np.float32)
+        idx = np.empty((b.n, n_stats), dtype=np.int64)
+        val = np.empty((b.n, n_stats), dtype=np.float32)
+        with ctx.lock:
+            rc = self._native_stats(ctx, b, periods, period_dts, n_stats, st, idx, val)
+            if rc == nat.PF_EUNSUPPORTED:
+                return None
+            ctx.check(rc)
+        return _stats_from_device(st, idx, val, periods, period_dts, n_stats, significance_type)
+
     def calc(self, times, mags, periods, period_dts, output="stats", normalize=None,
              center=None, n_stats=1, significance_type="stdmean", n_peaks=N_PEAKS_DEFAULT,
              min_distance=MIN_DISTANCE_DEFAULT, errs=None):
@@ -150,12 +165,33 @@ class _Periodogram:
             idx, val = self.peaks(times, mags_use, periods, period_dts, n_peaks, min_distance)
             return unravel_peaks(idx, val, periods, period_dts, int(n_peaks))
 
+        if (output == "stats" and 1 <= int(n_stats) < len(periods) * len(period_dts)
+                and (not self._use_max or len(period_dts) == 1)):
+            res = self._stats_on_device(times, mags_use, periods, period_dts, int(n_stats),
+                                        significance_type)
+            if res is not None:
+                return res
+
         data = self.periodograms(times, mags_use, periods, period_dts)
         if output == "stats":
             return [Statistics.statistics_from_data(
                 data[i], [periods, period_dts], self._use_max, n=n_stats,
                 significance_type=significance_type) for i in range(len(times))]
         return [Periodogram(d, [periods, period_dts], self._use_max) for d in data]
+
+
+def _stats_from_device(st, idx, val, periods, period_dts, n_stats, significance_type):
+    """Statistics objects from the device statistics, typed as the reference
+    builds them from numpy (float32 scalars), best first."""
+    n_pdt = len(period_dts)
+    out = []
+    for c in range(st.shape[0]):
+        mean, std, median, mad = st[c]
+        best = [Statistics([periods[k // n_pdt], period_dts[k % n_pdt]], val[c, j], mean, std,
+                           median, mad, significance_type)
+                for j, k in enumerate(idx[c].tolist())]
+        out.append(best[0] if n_stats == 1 else best)
+    return out
 
 
 class ConditionalEntropy(_Periodogram):
@@ -184,6 +220,12 @@ class ConditionalEntropy(_Periodogram):
                              self.phase_bin_extent, self.mag_bin_extent, self._flags,
                              nat.ptr(out))
 
+    def _native_stats(self, ctx, b, periods, pdts, n_top, st, idx, val):
+        return ctx.lib.pf_ce_stats(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
+                                   nat.ptr(pdts), len(pdts), self.n_phase, self.n_mag,
+                                   self.phase_bin_extent, self.mag_bin_extent, n_top,
+                                   self._flags, nat.ptr(st), nat.ptr(idx), nat.ptr(val))
+
     def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
         return ctx.lib.pf_ce_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                                    nat.ptr(pdts), len(pdts), self.n_phase, self.n_mag,
@@ -208,6 +250,12 @@ class AOV(_Periodogram):
         return ctx.lib.pf_aov(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                               nat.ptr(pdts), len(pdts), self.n_phase, self.phase_bin_extent,
                               self._flags, nat.ptr(out))
+
+    def _native_stats(self, ctx, b, periods, pdts, n_top, st, idx, val):
+        return ctx.lib.pf_aov_stats(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
+                                    nat.ptr(pdts), len(pdts), self.n_phase,
+                                    self.phase_bin_extent, n_top, self._flags, nat.ptr(st),
+                                    nat.ptr(idx), nat.ptr(val))
 
     def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
         return ctx.lib.pf_aov_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
@@ -235,6 +283,11 @@ class LombScargle(_Periodogram):
     def _native_pgram(self, ctx, b, periods, pdts, out):
         return ctx.lib.pf_ls(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                              nat.ptr(pdts), len(pdts), self._flags, nat.ptr(out))
+
+    def _native_stats(self, ctx, b, periods, pdts, n_top, st, idx, val):
+        return ctx.lib.pf_ls_stats(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
+                                   nat.ptr(pdts), len(pdts), n_top, self._flags, nat.ptr(st),
+                                   nat.ptr(idx), nat.ptr(val))
 
     def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
         return ctx.lib.pf_ls_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),

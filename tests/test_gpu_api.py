@@ -223,3 +223,78 @@ def test_batch_plan_rejects_bad_arguments():
     rc = lib.pf_plan_create(0, 7, None, None, off.ctypes.data, 1, None, 1, None, 1, 10, 10, 1, 1,
                             nat.PF_MODE_CHOSEN, None, 0, 1, None, None, ctypes.byref(h))
     assert rc == nat.PF_EINVAL and b"algo" in lib.pf_plan_error(None)
+
+
+def _stats_equal(a, b, data=None, grid=None):
+    """Same statistics; the same best cells, except that among cells of equal
+    value (a tie) numpy's pick is its partition order and the device takes
+    the lowest index -- then the device's cell must hold that value too."""
+    for x, y in zip(a if isinstance(a, list) else [a], b if isinstance(b, list) else [b]):
+        for f in ("value", "mean", "std", "median", "mad"):
+            gx, gy = getattr(x, f), getattr(y, f)
+            assert type(gx) is type(gy) and (gx == gy or (np.isnan(gx) and np.isnan(gy))), \
+                (f, gx, gy)
+        assert [type(p) for p in x.params] == [type(p) for p in y.params]
+        if x.params != y.params:
+            P, D = grid
+            i = int(np.nonzero(P == x.params[0])[0][0])
+            j = int(np.nonzero(D == x.params[1])[0][0])
+            assert data[i, j] == x.value, "device pick is not a tie of the best value"
+
+
+@pytest.mark.parametrize("algo", ["ce", "aov", "ls"])
+@pytest.mark.parametrize("n_stats", [1, 5])
+def test_stats_on_device_equal_numpy(gpu, algo, n_stats):
+    """calc(output='stats') computes the statistics on the device; they equal
+    the reference's numpy statistics_from_data on the same periodogram bit
+    for bit (float32 mean / std in numpy's summation order, exact median /
+    MAD, the same best cells and types)."""
+    rng = np.random.default_rng(31)
+    ts, ms = [], []
+    for n in (300, 47, 1200, 9):
+        t = lc.uniform_times(rng, n, 300.0)
+        ts.append(t)
+        ms.append(lc.noisy(rng, lc.sinusoid(t, float(rng.uniform(1, 9)), amp=0.3, offset=15.0),
+                           0.05))
+    make = {"ce": lambda: gpu.ConditionalEntropy(), "aov": lambda: gpu.AOV(12),
+            "ls": lambda: gpu.LombScargle()}[algo]
+    obj = make()
+    for n_per, pdts in ((1001, [0.0]), (1000, [0.0]), (400, [0.0, 1e-5])):
+        if obj._use_max and len(pdts) > 1:
+            continue  # the reference's largest-n pick is numpy's partition order there
+        P = np.linspace(0.7, 11.0, n_per).astype(np.float32)
+        D = np.array(pdts, np.float32)
+        got = obj.calc(ts, ms, P, D, output="stats", n_stats=n_stats)
+        pgs = obj.calc(ts, ms, P, D, output="periodogram")
+        want = [Statistics.statistics_from_data(pg.data, [P, D], obj._use_max, n=n_stats)
+                for pg in pgs]
+        for g, w, pg in zip(got, want, pgs):
+            _stats_equal(g, w, pg.data, (P, D))
+
+
+def test_stats_on_device_nan_rows_and_host_cases(gpu):
+    """An empty curve (CE NaN row) gives NaN statistics as numpy does; the
+    largest-n pick with several period derivatives keeps the numpy path."""
+    t, m = lc.sine_curve(2.0)
+    m = lc.normalize(m).astype(np.float32)
+    P = np.linspace(1.0, 5.0, 300).astype(np.float32)
+    # normalize=False: an empty curve reaches the kernels (normalising it
+    # raises, as in the reference) and its CE row is NaN.
+    kw = dict(normalize=False)
+    got = gpu.ConditionalEntropy().calc([t, np.zeros(0, np.float32)],
+                                        [m, np.zeros(0, np.float32)], P,
+                                        np.zeros(1, np.float32), output="stats", **kw)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        pgs = gpu.ConditionalEntropy().calc([t, np.zeros(0, np.float32)],
+                                            [m, np.zeros(0, np.float32)], P,
+                                            np.zeros(1, np.float32), output="periodogram", **kw)
+        want = [Statistics.statistics_from_data(pg.data, [P, np.zeros(1, np.float32)], False)
+                for pg in pgs]
+    _stats_equal(got[0], want[0], pgs[0].data, (P, np.zeros(1, np.float32)))
+    assert np.isnan(got[1].mean) and np.isnan(got[1].median) and np.isnan(got[1].mad)
+    assert np.isnan(want[1].mean) and np.isnan(want[1].median)
+    D2 = np.array([0.0, 1e-5], np.float32)
+    a = gpu.AOV().calc([t], [m], P, D2, output="stats")
+    pg = gpu.AOV().calc([t], [m], P, D2, output="periodogram")[0]
+    _stats_equal(a[0], Statistics.statistics_from_data(pg.data, [P, D2], True))
