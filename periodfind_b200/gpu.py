@@ -122,6 +122,39 @@ class _Periodogram:
                                          int(min_distance), idx, val))
         return idx, val
 
+    def _peaks_overlapped(self, times, mags, periods, period_dts, n_peaks, min_distance):
+        """'peaks' output.  Building the result objects is host work of the
+        same order as the GPU time on large batches, so the batch runs in a
+        few consecutive chunks: a worker thread makes the native call of one
+        chunk (the call releases the GIL) while this thread builds the
+        previous chunk's results.  Results are identical to one call."""
+        n = len(times)
+        points = sum(len(t) for t in times)
+        n_chunks = 4 if (n >= 64 and points * len(periods) * len(period_dts) >= 2e10) else 1
+        if n_chunks == 1:
+            idx, val = self.peaks(times, mags, periods, period_dts, n_peaks, min_distance)
+            return unravel_peaks(idx, val, periods, period_dts, n_peaks)
+        import sys
+        from concurrent.futures import ThreadPoolExecutor
+
+        bounds = [round(n * k / n_chunks) for k in range(n_chunks + 1)]
+        out = []
+        # The worker needs the GIL briefly between native calls; with the
+        # default 5 ms switch interval it would wait that long behind this
+        # thread's result building at every hand-over.
+        interval = sys.getswitchinterval()
+        sys.setswitchinterval(min(interval, 2e-4))
+        try:
+            with ThreadPoolExecutor(max_workers=1) as ex:
+                futs = [ex.submit(self.peaks, times[a:b], mags[a:b], periods, period_dts,
+                                  n_peaks, min_distance) for a, b in zip(bounds[:-1], bounds[1:])]
+                for f in futs:
+                    idx, val = f.result()
+                    out.extend(unravel_peaks(idx, val, periods, period_dts, n_peaks))
+        finally:
+            sys.setswitchinterval(interval)
+        return out
+
     def _stats_on_device(self, times, mags, periods, period_dts, n_stats, significance_type):
         """The 'stats' output with the statistics computed on the device
         (identical to numpy's); None where the device path does not apply."""
@@ -162,8 +195,8 @@ class _Periodogram:
         mags_use = prepare_magnitudes(mags, center, normalize)
 
         if output == "peaks":
-            idx, val = self.peaks(times, mags_use, periods, period_dts, n_peaks, min_distance)
-            return unravel_peaks(idx, val, periods, period_dts, int(n_peaks))
+            return self._peaks_overlapped(times, mags_use, periods, period_dts, int(n_peaks),
+                                          min_distance)
 
         if (output == "stats" and 1 <= int(n_stats) < len(periods) * len(period_dts)
                 and (not self._use_max or len(period_dts) == 1)):

@@ -298,3 +298,22 @@ def test_stats_on_device_nan_rows_and_host_cases(gpu):
     a = gpu.AOV().calc([t], [m], P, D2, output="stats")
     pg = gpu.AOV().calc([t], [m], P, D2, output="periodogram")[0]
     _stats_equal(a[0], Statistics.statistics_from_data(pg.data, [P, D2], True))
+
+
+def test_peaks_output_chunked_equals_one_call(gpu):
+    """Large 'peaks' requests run in chunks overlapped with result building;
+    the result equals a single native call's peak for peak."""
+    from periodfind_b200.gpu import unravel_peaks
+
+    rng = np.random.default_rng(8)
+    ts = [lc.uniform_times(rng, 4096, 2000.0) for _ in range(256)]
+    ms = [lc.noisy(rng, lc.sinusoid(t, float(rng.uniform(0.5, 10))), 0.05) for t in ts]
+    P = np.exp(np.linspace(np.log(0.1), np.log(100.0), 20000)).astype(np.float32)
+    D = np.zeros(1, np.float32)
+    obj = gpu.AOV(15)
+    got = obj.calc(ts, ms, P, D, output="peaks", n_peaks=8)
+    idx, val = obj.peaks(ts, ms, P, D, 8)
+    want = unravel_peaks(idx, val, P, D, 8)
+    assert len(got) == len(want) == 256
+    for g, w in zip(got, want):
+        assert [(s.params, s.value) for s in g] == [(s.params, s.value) for s in w]
