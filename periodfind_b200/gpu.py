@@ -21,7 +21,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import _native as nat
-from ._utils import ensure_float32, prepare_magnitudes, validate_inputs
+from ._utils import ensure_float32, gc_paused, prepare_magnitudes, validate_inputs
 from .stats import Periodogram, Statistics
 
 N_PEAKS_DEFAULT = 32
@@ -75,8 +75,9 @@ def unravel_peaks(peak_indices, peak_values, periods, period_dts, n_peaks):
     per = np.asarray(periods)[safe // n_pdts].astype(np.float64).tolist()
     pdt = np.asarray(period_dts)[safe % n_pdts].astype(np.float64).tolist()
     val = np.asarray(peak_values)[:, :n_peaks].astype(np.float64).tolist()
-    return [[Statistics([pr[k], dr[k]], vr[k], 0.0, 1.0, 0.0, 1.0) for k in range(cnt)]
-            for pr, dr, vr, cnt in zip(per, pdt, val, count)]
+    with gc_paused():
+        return [[Statistics([pr[k], dr[k]], vr[k], 0.0, 1.0, 0.0, 1.0) for k in range(cnt)]
+                for pr, dr, vr, cnt in zip(per, pdt, val, count)]
 
 
 class _Periodogram:
@@ -206,11 +207,12 @@ class _Periodogram:
                 return res
 
         data = self.periodograms(times, mags_use, periods, period_dts)
-        if output == "stats":
-            return [Statistics.statistics_from_data(
-                data[i], [periods, period_dts], self._use_max, n=n_stats,
-                significance_type=significance_type) for i in range(len(times))]
-        return [Periodogram(d, [periods, period_dts], self._use_max) for d in data]
+        with gc_paused():
+            if output == "stats":
+                return [Statistics.statistics_from_data(
+                    data[i], [periods, period_dts], self._use_max, n=n_stats,
+                    significance_type=significance_type) for i in range(len(times))]
+            return [Periodogram(d, [periods, period_dts], self._use_max) for d in data]
 
 
 def _stats_from_device(st, idx, val, periods, period_dts, n_stats, significance_type):
@@ -218,12 +220,13 @@ def _stats_from_device(st, idx, val, periods, period_dts, n_stats, significance_
     builds them from numpy (float32 scalars), best first."""
     n_pdt = len(period_dts)
     out = []
-    for c in range(st.shape[0]):
-        mean, std, median, mad = st[c]
-        best = [Statistics([periods[k // n_pdt], period_dts[k % n_pdt]], val[c, j], mean, std,
-                           median, mad, significance_type)
-                for j, k in enumerate(idx[c].tolist())]
-        out.append(best[0] if n_stats == 1 else best)
+    with gc_paused():
+        for c in range(st.shape[0]):
+            mean, std, median, mad = st[c]
+            best = [Statistics([periods[k // n_pdt], period_dts[k % n_pdt]], val[c, j], mean,
+                               std, median, mad, significance_type)
+                    for j, k in enumerate(idx[c].tolist())]
+            out.append(best[0] if n_stats == 1 else best)
     return out
 
 

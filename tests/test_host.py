@@ -200,3 +200,30 @@ def test_native_normalisation_matches_numpy_bit_for_bit():
     # an empty curve keeps numpy's error
     with pytest.raises(ValueError):
         prepare_magnitudes([np.zeros(0, np.float32)], False, True)
+
+
+def test_result_building_restores_collector_state():
+    """Result objects are built with the cyclic collector paused; its state
+    afterwards is the caller's, enabled or disabled, and the results are
+    the reference's (periodfind/cpu/__init__.py:46-70: a curve's list stops
+    at its first -1)."""
+    import gc
+
+    from periodfind_b200.gpu import unravel_peaks
+
+    periods = np.array([1.0, 2.0, 3.0], np.float32)
+    pdts = np.array([0.0, 0.5], np.float32)
+    idx = np.array([[5, 0, -1], [2, 3, 4]], np.int64)
+    val = np.array([[0.5, 0.25, 0.0], [1.0, 2.0, 3.0]], np.float32)
+    assert gc.isenabled()
+    out = unravel_peaks(idx, val, periods, pdts, 3)
+    assert gc.isenabled()
+    assert [len(r) for r in out] == [2, 3]
+    assert out[0][0].params == [3.0, 0.5] and out[0][0].value == 0.5
+    assert out[1][2].params == [3.0, 0.0] and out[1][2].value == 3.0
+    gc.disable()
+    try:
+        unravel_peaks(idx, val, periods, pdts, 3)
+        assert not gc.isenabled()
+    finally:
+        gc.enable()
