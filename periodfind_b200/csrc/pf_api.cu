@@ -533,15 +533,20 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
             const uint64_t nw = queue_items(j, k, item_periods(t));
             if (nw == 0 || nw > 0x7FFFFFFFull) continue;
             ps.q.n_work = (uint32_t)nw;
-            float ms = 0.0f;
-            for (int rep = 0; rep < 2; rep++) {  // the first launch warms up
+            // The first launch warms up; the faster of the next two counts
+            // (shapes within a few percent of each other otherwise swap
+            // places by launch-to-launch noise on a ~1 ms sample).
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3; rep++) {
+                float m = 0.0f;
                 PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
                 PF_CUDA(launch_fold_sem(j, t, ps, (uint32_t)nw, s), "tuning launch");
                 PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
                 PF_CUDA(cudaEventSynchronize(ctx->ev1), "tuning sync");
-                PF_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1), "event time");
+                PF_CUDA(cudaEventElapsedTime(&m, ctx->ev0, ctx->ev1), "event time");
+                if (rep > 0) ms = std::min(ms, m);
             }
-            ctx->launches += 2;
+            ctx->launches += 3;
             best.candidates++;
             best.ms_worst = std::max(best.ms_worst, ms);
             if (ms < best.ms) {

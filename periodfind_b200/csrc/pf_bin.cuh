@@ -71,10 +71,14 @@ struct BinPoint {
 template <bool CNT16>
 __device__ __forceinline__ float ce_stat_fast(uint32_t tbase, uint32_t nP, uint32_t W,
                                               uint32_t block, uint32_t n) {
-    // c ln c, zero for c = 0 and 1: one log per bin, no divide.
+    // c log2 c, zero for c = 0 and 1: one log per bin, no divide, and ln 2
+    // applied once at the end.  A count (< 2^16 here: the bin kernel runs
+    // curves of fewer than 65536 points) becomes a float exactly by placing
+    // it in the mantissa of 2^23, which costs a bitwise OR and an add
+    // instead of an integer-to-float conversion.
     auto xlx = [](uint32_t c) -> float {
-        const float f = (float)max(c, 1u);
-        return f * logf(f);
+        const float f = __uint_as_float(c | 0x4B000000u) - 8388608.0f;
+        return f * log2f(fmaxf(f, 1.0f));
     };
     float acc = 0.0f;
     for (uint32_t j = 0; j < nP; j++) {
@@ -83,17 +87,19 @@ __device__ __forceinline__ float ce_stat_fast(uint32_t tbase, uint32_t nP, uint3
         for (uint32_t wi = 0; wi < W; wi++) {
             const uint32_t wv = lds_u32(tbase + (j * W + wi) * block * 4u);
             if constexpr (CNT16) {
-                const uint32_t c0 = wv & 0xFFFFu, c1 = wv >> 16;
-                col += c0 + c1;
-                row += xlx(c0) + xlx(c1);
+                // Both 16-bit halves summed at once: each half's column
+                // total is at most n < 2^16, so no carry crosses halves.
+                col += wv;
+                row += xlx(wv & 0xFFFFu) + xlx(wv >> 16);
             } else {
                 col += wv;
                 row += xlx(wv);
             }
         }
+        if constexpr (CNT16) col = (col & 0xFFFFu) + (col >> 16);
         acc += xlx(col) - row;
     }
-    return acc / (float)n;
+    return acc * (0.69314718055994531f / (float)n);
 }
 
 // The chosen form's AOV sum_b X_b^2 / c_b over the fixed-point bin sums X_b
