@@ -1,6 +1,6 @@
 // pf_stats.cu -- the 'stats' output on the device: per periodogram row, the
 // values the reference computes on the host with numpy
-// (periodfind/__init__.py:303-345, Statistics.statistics_from_data):
+// (periodfind/__init__.py:338-400, Statistics.statistics_from_data):
 //   mean   = np.mean(data), std = np.std(data)   (float32, numpy's pairwise
 //            summation order: leaves of <= 128 elements summed with eight
 //            accumulators, halves split at multiples of 8, as np.add.reduce)
