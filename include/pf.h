@@ -54,6 +54,15 @@
  *                  form's divide-free one (agreeing to ~1e-6): values are then
  *                  bit-identical to the plain form exactly when the bin
  *                  occupancies are, which is how occupancy parity is tested.
+ *  PF_ASYNC        (pf_ce_peaks / pf_aov_peaks / pf_ls_peaks only) enqueue
+ *                  and return: the inputs are packed into the context's
+ *                  staging block and the work is queued on the context's
+ *                  stream, but out_idx / out_val are written later, by the
+ *                  pf_wait call that collects this call.  The caller keeps
+ *                  them alive until then.  At most two PF_ASYNC calls may be
+ *                  pending on a context; a third is PF_EINVAL.  A caller
+ *                  packs the next batch while the GPU runs this one.  Not
+ *                  with PF_TIMING.
  */
 #ifndef PERIODFIND_B200_PF_H
 #define PERIODFIND_B200_PF_H
@@ -80,6 +89,7 @@ extern "C" {
 #define PF_TIMING 0x1000
 #define PF_REF_STATS 0x2000
 #define PF_NO_TUNE 0x4000
+#define PF_ASYNC 0x8000
 
 typedef struct pf_ctx pf_ctx;
 
@@ -148,6 +158,13 @@ int pf_ls_peaks(pf_ctx* ctx, const float* const* times,
                 const float* period_dts, uint64_t n_pdt, uint32_t n_peaks,
                 uint32_t min_distance, int mode, int64_t* out_idx,
                 float* out_val);
+
+/* Collect the oldest pending PF_ASYNC peak call on this context: wait for
+ * its work, then write its peaks into the out_idx / out_val it was given.
+ * Calls are collected in the order they were made.  PF_EINVAL when none is
+ * pending; a device error of the collected call is returned here.  No
+ * reference counterpart (the reference's calls are synchronous). */
+int pf_wait(pf_ctx* ctx);
 
 /* Periodogram + the 'stats' output computed on the device: what the
  * reference's Statistics.statistics_from_data (periodfind/__init__.py:

@@ -31,6 +31,7 @@ PF_FOLD_EXACT = 0x400
 PF_TIMING = 0x1000
 PF_REF_STATS = 0x2000
 PF_NO_TUNE = 0x4000
+PF_ASYNC = 0x8000
 PF_ALGO_CE, PF_ALGO_AOV, PF_ALGO_LS = 0, 1, 2
 
 _vp = ctypes.c_void_p
@@ -54,6 +55,7 @@ SIGNATURES = {
                       _int, _vp, _vp], _int),
     "pf_ls_peaks": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int, _vp,
                      _vp], _int),
+    "pf_wait": ([_vp], _int),
     "pf_ce_stats": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32,
                      _u32, _int, _vp, _vp, _vp], _int),
     "pf_aov_stats": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _int,

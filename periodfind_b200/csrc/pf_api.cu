@@ -79,6 +79,19 @@ struct pf_ctx {
         uint32_t candidates;
     };
     std::map<std::string, Tuned> tuned;
+    // PF_ASYNC peak calls not yet collected by pf_wait, oldest first.  Each
+    // copies its peaks into its own pinned block; the event follows the copy.
+    struct Pending {
+        PinnedBuf res;
+        cudaEvent_t done = nullptr;
+        int64_t* out_idx = nullptr;
+        float* out_val = nullptr;
+        size_t n = 0;       // peak entries to hand over
+        bool work = false;  // the call queued device work
+    };
+    static constexpr int kMaxPending = 2;
+    Pending pend[kMaxPending];
+    int pend_head = 0, pend_count = 0;
 };
 
 namespace {
@@ -736,15 +749,36 @@ void read_kernel_time(pf_ctx* ctx) {
     ctx->timed_pending = false;
 }
 
+// Register a PF_ASYNC call for pf_wait: its peaks (n entries) sit in the
+// next pending slot's pinned block once the slot's event has completed.
+int push_pending(pf_ctx* ctx, const Job& j, size_t n, bool work, cudaStream_t s) {
+    pf_ctx::Pending& q = ctx->pend[(ctx->pend_head + ctx->pend_count) % pf_ctx::kMaxPending];
+    q.out_idx = j.out_idx;
+    q.out_val = j.out_val;
+    q.n = n;
+    q.work = work;
+    if (work) PF_CUDA(cudaEventRecord(q.done, s), "event");
+    ctx->pend_count++;
+    return PF_OK;
+}
+
 // The whole pipeline for host-pointer inputs.
 int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* const* mags,
              const uint64_t* lengths) {
     int rc = validate_common(ctx, j);
     if (rc != PF_OK) return rc;
-    if (j.n_curves == 0) return PF_OK;
+    const bool async = (j.mode & PF_ASYNC) != 0;
+    if (async) {
+        if (!j.peaks) return fail(ctx, PF_EINVAL, "PF_ASYNC applies to the peak calls only");
+        if (j.mode & PF_TIMING) return fail(ctx, PF_EINVAL, "PF_ASYNC excludes PF_TIMING");
+        if (ctx->pend_count == pf_ctx::kMaxPending)
+            return fail(ctx, PF_EINVAL, "%d PF_ASYNC calls are pending; collect one with pf_wait",
+                        pf_ctx::kMaxPending);
+    }
+    if (j.n_curves == 0) return async ? push_pending(ctx, j, 0, false, nullptr) : PF_OK;
     if (!times || !mags || !lengths) return fail(ctx, PF_EINVAL, "times/mags/lengths is NULL");
     const uint64_t n_cells = j.n_per * j.n_pdt;
-    if (n_cells == 0) return PF_OK;
+    if (n_cells == 0) return async ? push_pending(ctx, j, 0, false, nullptr) : PF_OK;
     if ((rc = check_grid_host(ctx, j)) != PF_OK) return rc;
     for (uint64_t c = 0; c < j.n_curves; c++)
         if (lengths[c] > 0 && (!times[c] || !mags[c]))
@@ -820,12 +854,30 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
     } else if (!j.peaks) {
         PF_CUDA(cudaMemcpyAsync(j.out, ctx->d_out.p, out_bytes, cudaMemcpyDeviceToHost, s),
                 "D2H periodogram");
-    } else if (j.n_peaks > 0) {
+    } else if (j.n_peaks > 0 && !async) {
         const size_t pk = (size_t)j.n_curves * j.n_peaks;
         PF_CUDA(cudaMemcpyAsync(j.out_idx, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
                 "D2H peak indices");
         PF_CUDA(cudaMemcpyAsync(j.out_val, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s),
                 "D2H peak values");
+    }
+    if (async) {
+        // The peaks go to this call's pinned block (a free slot: its last
+        // user was collected, so no copy into it is in flight), and the
+        // call returns with its work queued.  The staging block stays
+        // marked in use until the H2D copy above has finished.
+        const size_t pk = (size_t)j.n_curves * j.n_peaks;
+        if (pk > 0) {
+            pf_ctx::Pending& q =
+                ctx->pend[(ctx->pend_head + ctx->pend_count) % pf_ctx::kMaxPending];
+            if ((rc = ensure_pinned(ctx, q.res, pk * 12)) != PF_OK) return rc;
+            char* hr = (char*)q.res.p;
+            PF_CUDA(cudaMemcpyAsync(hr, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
+                    "D2H peak indices");
+            PF_CUDA(cudaMemcpyAsync(hr + pk * 8, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s),
+                    "D2H peak values");
+        }
+        return push_pending(ctx, j, pk, true, s);
     }
     PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
     ctx->staged_pending = false;
@@ -979,9 +1031,13 @@ int pf_ctx_create(pf_ctx** out, int device) {
         (e = cudaEventCreate(&ctx->ev0)) != cudaSuccess ||
         (e = cudaEventCreate(&ctx->ev1)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->ev_staged, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&ctx->ev_done, cudaEventDisableTiming)) != cudaSuccess) {
+        (e = cudaEventCreateWithFlags(&ctx->ev_done, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->pend[0].done, cudaEventDisableTiming)) !=
+            cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->pend[1].done, cudaEventDisableTiming)) !=
+            cudaSuccess) {
         g_create_error = cudaGetErrorString(e);
-        delete ctx;
+        pf_ctx_destroy(ctx);
         return PF_ECUDA;
     }
     *out = ctx;
@@ -997,6 +1053,10 @@ void pf_ctx_destroy(pf_ctx* ctx) {
                       &ctx->d_pval, &ctx->d_pack, &ctx->d_misc, &ctx->d_stamps, &ctx->d_stat})
         if (b->p) cudaFree(b->p);
     if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
+    for (pf_ctx::Pending& q : ctx->pend) {
+        if (q.res.p) cudaFreeHost(q.res.p);
+        if (q.done) cudaEventDestroy(q.done);
+    }
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->ev_staged) cudaEventDestroy(ctx->ev_staged);
@@ -1350,6 +1410,23 @@ int pf_ls_peaks(pf_ctx* ctx, const float* const* times, const float* const* mags
     j.out_idx = out_idx;
     j.out_val = out_val;
     return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_wait(pf_ctx* ctx) {
+    if (!ctx) return PF_EINVAL;
+    if (ctx->pend_count == 0) return fail(ctx, PF_EINVAL, "no PF_ASYNC call is pending");
+    pf_ctx::Pending& q = ctx->pend[ctx->pend_head];
+    ctx->pend_head = (ctx->pend_head + 1) % pf_ctx::kMaxPending;
+    ctx->pend_count--;
+    if (!q.work) return PF_OK;
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    PF_CUDA(cudaEventSynchronize(q.done), "asynchronous peak call");
+    if (q.n > 0) {
+        const char* hr = (const char*)q.res.p;
+        memcpy(q.out_idx, hr, q.n * 8);
+        memcpy(q.out_val, hr + q.n * 8, q.n * 4);
+    }
+    return PF_OK;
 }
 
 int pf_ce_dev(pf_ctx* ctx, const float* d_times, const float* d_mags, const int64_t* offsets,

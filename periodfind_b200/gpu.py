@@ -96,7 +96,7 @@ class _Periodogram:
     def _native_pgram(self, ctx, b, periods, pdts, out):
         raise NotImplementedError
 
-    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
+    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val, extra=0):
         raise NotImplementedError
 
     def periodograms(self, times, mags, periods, period_dts):
@@ -124,37 +124,49 @@ class _Periodogram:
         return idx, val
 
     def _peaks_overlapped(self, times, mags, periods, period_dts, n_peaks, min_distance):
-        """'peaks' output.  Building the result objects is host work of the
-        same order as the GPU time on large batches, so the batch runs in a
-        few consecutive chunks: a worker thread makes the native call of one
-        chunk (the call releases the GIL) while this thread builds the
-        previous chunk's results.  Results are identical to one call."""
+        """'peaks' output.  Large batches run as a few consecutive chunks in a
+        pipeline: each chunk's native call only queues its work (PF_ASYNC)
+        and returns, so the next chunk is packed and queued while the GPU
+        runs this one, and a chunk's result objects are built while the GPU
+        runs the next.  Results are identical to one call."""
         n = len(times)
         points = sum(len(t) for t in times)
         n_chunks = 4 if (n >= 64 and points * len(periods) * len(period_dts) >= 2e10) else 1
         if n_chunks == 1:
             idx, val = self.peaks(times, mags, periods, period_dts, n_peaks, min_distance)
             return unravel_peaks(idx, val, periods, period_dts, n_peaks)
-        import sys
-        from concurrent.futures import ThreadPoolExecutor
-
+        n_peaks = int(n_peaks)
+        if n_peaks < 0:
+            raise ValueError("n_peaks must be >= 0")
+        ctx = nat.default_context(self.device)
         bounds = [round(n * k / n_chunks) for k in range(n_chunks + 1)]
-        out = []
-        # The worker needs the GIL briefly between native calls; with the
-        # default 5 ms switch interval it would wait that long behind this
-        # thread's result building at every hand-over.
-        interval = sys.getswitchinterval()
-        sys.setswitchinterval(min(interval, 2e-4))
-        try:
-            with ThreadPoolExecutor(max_workers=1) as ex:
-                futs = [ex.submit(self.peaks, times[a:b], mags[a:b], periods, period_dts,
-                                  n_peaks, min_distance) for a, b in zip(bounds[:-1], bounds[1:])]
-                for f in futs:
-                    idx, val = f.result()
-                    out.extend(unravel_peaks(idx, val, periods, period_dts, n_peaks))
-        finally:
-            sys.setswitchinterval(interval)
-        return out
+        outs = []  # (indices, values) of each queued chunk, alive until collected
+        res = []
+        with ctx.lock:
+            def queue(k):
+                b = nat.CurveBatch(times[bounds[k]:bounds[k + 1]], mags[bounds[k]:bounds[k + 1]])
+                idx = np.full((b.n, n_peaks), -1, dtype=np.int64)
+                val = np.zeros((b.n, n_peaks), dtype=np.float32)
+                ctx.check(self._native_peaks(ctx, b, periods, period_dts, n_peaks,
+                                             int(min_distance), idx, val, nat.PF_ASYNC))
+                outs.append((idx, val))
+
+            collected = 0
+            try:
+                queue(0)
+                for k in range(n_chunks):
+                    if k + 1 < n_chunks:
+                        queue(k + 1)
+                    collected += 1
+                    ctx.check(ctx.lib.pf_wait(ctx.handle))
+                    idx, val = outs[k]
+                    res.extend(unravel_peaks(idx, val, periods, period_dts, n_peaks))
+            finally:
+                # After an error, collect what is still queued so that the
+                # context is left with nothing pending.
+                for _ in range(len(outs) - collected):
+                    ctx.lib.pf_wait(ctx.handle)
+        return res
 
     def _stats_on_device(self, times, mags, periods, period_dts, n_stats, significance_type):
         """The 'stats' output with the statistics computed on the device
@@ -262,11 +274,12 @@ class ConditionalEntropy(_Periodogram):
                                    self.phase_bin_extent, self.mag_bin_extent, n_top,
                                    self._flags, nat.ptr(st), nat.ptr(idx), nat.ptr(val))
 
-    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
+    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val, extra=0):
         return ctx.lib.pf_ce_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                                    nat.ptr(pdts), len(pdts), self.n_phase, self.n_mag,
                                    self.phase_bin_extent, self.mag_bin_extent, n_peaks,
-                                   min_distance, self._flags, nat.ptr(idx), nat.ptr(val))
+                                   min_distance, self._flags | extra, nat.ptr(idx),
+                                   nat.ptr(val))
 
 
 class AOV(_Periodogram):
@@ -293,11 +306,11 @@ class AOV(_Periodogram):
                                     self.phase_bin_extent, n_top, self._flags, nat.ptr(st),
                                     nat.ptr(idx), nat.ptr(val))
 
-    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
+    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val, extra=0):
         return ctx.lib.pf_aov_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                                     nat.ptr(pdts), len(pdts), self.n_phase,
-                                    self.phase_bin_extent, n_peaks, min_distance, self._flags,
-                                    nat.ptr(idx), nat.ptr(val))
+                                    self.phase_bin_extent, n_peaks, min_distance,
+                                    self._flags | extra, nat.ptr(idx), nat.ptr(val))
 
 
 class LombScargle(_Periodogram):
@@ -325,10 +338,10 @@ class LombScargle(_Periodogram):
                                    nat.ptr(pdts), len(pdts), n_top, self._flags, nat.ptr(st),
                                    nat.ptr(idx), nat.ptr(val))
 
-    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val):
+    def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val, extra=0):
         return ctx.lib.pf_ls_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                                    nat.ptr(pdts), len(pdts), n_peaks, min_distance,
-                                   self._flags, nat.ptr(idx), nat.ptr(val))
+                                   self._flags | extra, nat.ptr(idx), nat.ptr(val))
 
     def refine_peaks(self, times, mags, periods, peak_indices, n_steps=5, center=None):
         """Refine grid peaks off the trial grid by Newton steps on dP/domega

@@ -317,3 +317,83 @@ def test_peaks_output_chunked_equals_one_call(gpu):
     assert len(got) == len(want) == 256
     for g, w in zip(got, want):
         assert [(s.params, s.value) for s in g] == [(s.params, s.value) for s in w]
+
+
+def test_async_peak_calls_equal_synchronous_calls(gpu):
+    """PF_ASYNC peak calls queue their work and return; pf_wait collects
+    them oldest first into the arrays each call was given.  Two may be
+    pending at once; the results equal the synchronous calls' bit for bit
+    (CE, AOV, LS)."""
+    from periodfind_b200 import _native as nat
+
+    rng = np.random.default_rng(21)
+    P = np.exp(np.linspace(np.log(0.2), np.log(50.0), 3000)).astype(np.float32)
+    D = np.array([0.0, 1e-6], np.float32)
+    batches = []
+    for k in range(3):
+        ts = [lc.uniform_times(rng, int(rng.integers(20, 900)), 500.0) for _ in range(40 + k)]
+        ms = [lc.noisy(rng, lc.sinusoid(t, float(rng.uniform(0.5, 10))), 0.05) for t in ts]
+        batches.append((ts, ms))
+    ctx = nat.default_context(0)
+    for obj in (gpu.ConditionalEntropy(10, 10), gpu.AOV(12), gpu.LombScargle()):
+        prep = [(ts, [lc.normalize(m) for m in ms] if isinstance(obj, gpu.ConditionalEntropy)
+                 else ms) for ts, ms in batches]
+        want = [obj.peaks(ts, ms, P, D, 16, 2) for ts, ms in prep]
+        got = []
+        with ctx.lock:
+            for k, (ts, ms) in enumerate(prep):
+                b = nat.CurveBatch(ts, ms)
+                idx = np.full((b.n, 16), -7, np.int64)
+                val = np.full((b.n, 16), 7.0, np.float32)
+                ctx.check(obj._native_peaks(ctx, b, P, D, 16, 2, idx, val, nat.PF_ASYNC))
+                got.append((idx, val))
+                if k == 1:  # two pending: collect the first
+                    ctx.check(ctx.lib.pf_wait(ctx.handle))
+            ctx.check(ctx.lib.pf_wait(ctx.handle))
+            ctx.check(ctx.lib.pf_wait(ctx.handle))
+        for (gi, gv), (wi, wv) in zip(got, want):
+            np.testing.assert_array_equal(gi, wi)
+            np.testing.assert_array_equal(gv, wv)
+
+
+def test_async_call_rules(gpu):
+    """pf_wait with nothing pending, a third pending call, PF_ASYNC outside
+    the peak calls and PF_ASYNC with PF_TIMING are refused with PF_EINVAL;
+    an empty batch is a pending call with nothing to copy."""
+    from periodfind_b200 import _native as nat
+
+    ctx = nat.Context(0)
+    try:
+        lib, h = ctx.lib, ctx.handle
+        assert lib.pf_wait(h) == nat.PF_EINVAL
+        rng = np.random.default_rng(2)
+        ts = [lc.uniform_times(rng, 300, 100.0) for _ in range(8)]
+        ms = [lc.noisy(rng, lc.sinusoid(t, 3.0), 0.05) for t in ts]
+        b = nat.CurveBatch(ts, ms)
+        P = np.linspace(0.5, 10, 500).astype(np.float32)
+        D = np.zeros(1, np.float32)
+        idx = [np.full((8, 4), -1, np.int64) for _ in range(3)]
+        val = [np.zeros((8, 4), np.float32) for _ in range(3)]
+        flags = nat.PF_MODE_CHOSEN | nat.PF_ASYNC
+
+        def call(k, fl=flags):
+            return lib.pf_ls_peaks(h, *b.args(), nat.ptr(P), len(P), nat.ptr(D), len(D), 4, 1,
+                                   fl, nat.ptr(idx[k]), nat.ptr(val[k]))
+
+        assert call(0) == nat.PF_OK and call(1) == nat.PF_OK
+        assert call(2) == nat.PF_EINVAL
+        assert lib.pf_wait(h) == nat.PF_OK and lib.pf_wait(h) == nat.PF_OK
+        assert lib.pf_wait(h) == nat.PF_EINVAL
+        np.testing.assert_array_equal(idx[0], idx[1])
+        assert (idx[0][:, 0] >= 0).all()
+        assert call(0, flags | nat.PF_TIMING) == nat.PF_EINVAL
+        out = np.zeros((8, len(P), 1), np.float32)
+        assert lib.pf_ls(h, *b.args(), nat.ptr(P), len(P), nat.ptr(D), len(D), flags,
+                         nat.ptr(out)) == nat.PF_EINVAL
+        empty = nat.CurveBatch([], [])
+        assert lib.pf_ls_peaks(h, *empty.args(), nat.ptr(P), len(P), nat.ptr(D), len(D), 4, 1,
+                               flags, nat.ptr(idx[2]), nat.ptr(val[2])) == nat.PF_OK
+        assert lib.pf_wait(h) == nat.PF_OK
+        assert lib.pf_wait(h) == nat.PF_EINVAL
+    finally:
+        ctx.close()
