@@ -180,21 +180,74 @@ def default_context(device: int = 0) -> Context:
         return ctx
 
 
+class FlatList(list):
+    """A list of float32 curves that are consecutive views of one buffer,
+    with their data pointers already computed (what the batch magnitude
+    preparation returns).  Slices keep the pointers."""
+
+    def __init__(self, arrays, buf, ptrs):
+        super().__init__(arrays)
+        self.buf = buf
+        self.ptrs = ptrs
+
+    def __getitem__(self, k):
+        if isinstance(k, slice) and self.ptrs is not None:
+            return FlatList(list.__getitem__(self, k), self.buf, self.ptrs[k])
+        return list.__getitem__(self, k)
+
+
+def _dropping_pointers(name):
+    # A change to the list itself makes the stored pointers stale: forget
+    # them, and the curves are then addressed one by one.
+    base = getattr(list, name)
+
+    def method(self, *args, **kwargs):
+        self.ptrs = None
+        return base(self, *args, **kwargs)
+
+    method.__name__ = name
+    return method
+
+
+for _name in ("__setitem__", "__delitem__", "__iadd__", "__imul__", "append", "extend",
+              "insert", "pop", "remove", "reverse", "sort", "clear"):
+    setattr(FlatList, _name, _dropping_pointers(_name))
+
+
+def host_pointers(arrs, lengths):
+    """Data pointers (uintp) of float32 curves, and the object that keeps
+    them valid.  Short curves are gathered into one buffer, whose pointers
+    are arithmetic (taking an array's address costs about a microsecond,
+    more than copying a thousand points); longer ones are used in place."""
+    n = len(lengths)
+    if isinstance(arrs, FlatList) and arrs.ptrs is not None and len(arrs.ptrs) == n:
+        return arrs.ptrs, arrs
+    total = int(lengths.sum()) if n else 0
+    if 0 < n and total <= 1024 * n and total <= (1 << 22):
+        buf = np.concatenate(arrs).astype(np.float32, copy=False)
+        starts = np.zeros(n, dtype=np.uint64)
+        np.cumsum(lengths[:-1], out=starts[1:])
+        return (np.uint64(buf.ctypes.data) + np.uint64(4) * starts).astype(np.uintp), buf
+    keep = [np.ascontiguousarray(a, dtype=np.float32) for a in arrs]
+    return np.fromiter((a.ctypes.data for a in keep), dtype=np.uintp, count=n), keep
+
+
 class CurveBatch:
     """Per-curve host pointers and lengths for the host-pointer entry points.
 
-    Keeps references to the (contiguous float32) arrays so the pointers stay
+    Keeps references to the (contiguous float32) data so the pointers stay
     valid for the duration of the native call.
     """
 
     def __init__(self, times, mags):
-        self.times = [np.ascontiguousarray(t, dtype=np.float32) for t in times]
-        self.mags = [np.ascontiguousarray(m, dtype=np.float32) for m in mags]
-        n = len(self.times)
+        n = len(times)
         self.n = n
-        self.tptr = np.fromiter((a.ctypes.data for a in self.times), dtype=np.uintp, count=n)
-        self.mptr = np.fromiter((a.ctypes.data for a in self.mags), dtype=np.uintp, count=n)
-        self.lengths = np.fromiter((a.shape[0] for a in self.times), dtype=np.uint64, count=n)
+        self.lengths = np.fromiter((len(t) for t in times), dtype=np.uint64, count=n)
+        mlen = np.fromiter((len(m) for m in mags), dtype=np.uint64, count=len(mags))
+        if not np.array_equal(mlen, self.lengths):
+            raise ValueError("times and mags must have the same length for every curve")
+        self.tptr, self._times = host_pointers(times, self.lengths)
+        self.mptr, self._mags = host_pointers(mags, self.lengths)
 
     def args(self):
         return (self.tptr.ctypes.data, self.mptr.ctypes.data, self.lengths.ctypes.data, self.n)

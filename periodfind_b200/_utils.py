@@ -66,19 +66,19 @@ def _normalize_batch(mags):
     # In the native library (multithreaded, same float32 arithmetic).
     from . import _native as nat
 
-    arrs = [np.ascontiguousarray(a) for a in arrs]
-    lens = np.fromiter((a.size for a in arrs), dtype=np.uint64, count=len(arrs))
+    n = len(arrs)
+    lens = np.fromiter((a.shape[0] for a in arrs), dtype=np.uint64, count=n)
+    starts = np.zeros(n, dtype=np.uint64)
+    np.cumsum(lens[:-1], out=starts[1:])
+    src, keep = nat.host_pointers(arrs, lens)
     flat = np.empty(int(lens.sum()), dtype=np.float32)
-    starts = np.zeros(len(arrs), dtype=np.int64)
-    np.cumsum(lens[:-1].astype(np.int64), out=starts[1:])
-    out = np.split(flat, starts[1:])
-    src = np.fromiter((a.ctypes.data for a in arrs), dtype=np.uintp, count=len(arrs))
-    dst = np.fromiter((o.ctypes.data for o in out), dtype=np.uintp, count=len(out))
-    rc = nat.load().pf_normalize_mags(src.ctypes.data, lens.ctypes.data, len(arrs),
-                                      dst.ctypes.data)
+    dst = (np.uint64(flat.ctypes.data) + np.uint64(4) * starts).astype(np.uintp)
+    rc = nat.load().pf_normalize_mags(src.ctypes.data, lens.ctypes.data, n, dst.ctypes.data)
+    del keep
     if rc != nat.PF_OK:
         raise RuntimeError(f"magnitude normalisation failed ({rc})")
-    return out
+    bounds = starts.tolist() + [flat.shape[0]]
+    return nat.FlatList([flat[a:b] for a, b in zip(bounds[:-1], bounds[1:])], flat, dst)
 
 
 def validate_inputs(times, mags):

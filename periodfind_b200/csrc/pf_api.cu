@@ -1090,7 +1090,33 @@ int pf_normalize_mags(const float* const* mags, const uint64_t* lengths, uint64_
         const uint64_t n = lengths[c];
         float lo = m[0], hi = m[0];
         bool nan = std::isnan(m[0]);
-        for (uint64_t i = 1; i < n; i++) {
+        uint64_t i = 1;
+        if (n >= 16) {
+            // Eight interleaved running minima / maxima, which the compiler
+            // turns into SIMD min / max.  Without NaN the result is the exact
+            // minimum and maximum whatever the order; only the sign of a
+            // zero extreme may differ, and lo, hi enter the output solely
+            // through m - lo and hi - lo, whose values it does not change.
+            float l[8], h[8];
+            int bad[8];
+            for (int k = 0; k < 8; k++) {
+                l[k] = h[k] = m[k];
+                bad[k] = 0;
+            }
+            for (i = 0; i + 8 <= n; i += 8)
+                for (int k = 0; k < 8; k++) {
+                    const float v = m[i + k];
+                    bad[k] |= (v != v);
+                    l[k] = v < l[k] ? v : l[k];
+                    h[k] = v > h[k] ? v : h[k];
+                }
+            for (int k = 0; k < 8; k++) {
+                nan |= bad[k] != 0;
+                lo = l[k] < lo ? l[k] : lo;
+                hi = h[k] > hi ? h[k] : hi;
+            }
+        }
+        for (; i < n; i++) {
             const float v = m[i];
             nan |= std::isnan(v);
             lo = v < lo ? v : lo;

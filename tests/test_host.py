@@ -227,3 +227,37 @@ def test_result_building_restores_collector_state():
         assert not gc.isenabled()
     finally:
         gc.enable()
+
+
+def test_curve_pointers_address_the_curves():
+    """CurveBatch's per-curve pointers address each curve's float32 data,
+    whether short curves are gathered into one buffer, long ones are used in
+    place, or the magnitudes come from the batch normalisation (a list whose
+    pointers are precomputed, dropped when the list is changed)."""
+    from periodfind_b200 import _native as nat
+    from periodfind_b200._utils import prepare_magnitudes
+
+    def read(p, n):
+        return np.ctypeslib.as_array((ctypes.c_float * n).from_address(int(p)))
+
+    rng = np.random.default_rng(5)
+    for sizes in ([5, 700, 1, 64], [3000, 5000, 2500]):
+        ts = [rng.uniform(0, 100, k).astype(np.float32) for k in sizes]
+        ms = [rng.normal(15, 0.3, k).astype(np.float64) for k in sizes]
+        b = nat.CurveBatch(ts, ms)
+        assert b.lengths.tolist() == sizes
+        for c, k in enumerate(sizes):
+            np.testing.assert_array_equal(read(b.tptr[c], k), ts[c])
+            np.testing.assert_array_equal(read(b.mptr[c], k), ms[c].astype(np.float32))
+        norm = prepare_magnitudes([m.astype(np.float32) for m in ms], False, True)
+        sub = norm[1:]
+        bn = nat.CurveBatch(ts[1:], sub)
+        assert bn.mptr is sub.ptrs
+        for c in range(len(sizes) - 1):
+            np.testing.assert_array_equal(read(bn.mptr[c], sizes[c + 1]), norm[c + 1])
+        norm[0] = norm[0].copy()
+        assert norm.ptrs is None
+        bc = nat.CurveBatch(ts, norm)
+        np.testing.assert_array_equal(read(bc.mptr[0], sizes[0]), norm[0])
+    with pytest.raises(ValueError):
+        nat.CurveBatch([np.zeros(3, np.float32)], [np.zeros(4, np.float32)])
