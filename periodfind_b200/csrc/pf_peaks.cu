@@ -18,6 +18,15 @@
 //   - a better extremum fed before that replaces it.
 // The sorted top-N list lives in shared memory (threshold in a register)
 // and is written to the caller's rows at the end.
+//
+// Extrema that cannot pass the peak test are dropped before the replay.
+// The threshold only ever gets stricter (a full list only takes a better
+// value in place of its worst), so an extremum that is not better than the
+// threshold at the start of its chunk fails the peak test at its own turn
+// too.  Such an extremum changes no state: a promotion that falls due while
+// it would be fed depends only on the candidate and the threshold, so it
+// gives the same list when done at the next extremum that is fed instead.
+// On noisy rows this leaves a few hundred of the ~n/3 extrema to replay.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -90,6 +99,7 @@ __global__ void __launch_bounds__(kPeakThreads)
     float* top_val = reinterpret_cast<float*>(psmem + kChunk * 12 + (size_t)n_peaks * 8);
     __shared__ uint32_t warp_tot[kPeakThreads / 32];
     __shared__ uint32_t chunk_count;
+    __shared__ float thr_sh;  // the replay's threshold after the last chunk
 
     const uint64_t c = blockIdx.x;
     const float* d = pg + c * flat_len;
@@ -108,18 +118,23 @@ __global__ void __launch_bounds__(kPeakThreads)
     const uint64_t md = min_distance;
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) thr_sh = s.thr;
+    __syncthreads();
     // Interior samples 1 .. flat_len-2.
     const uint64_t first = 1, last = (flat_len >= 2) ? flat_len - 2 : 0;
     for (uint64_t base = first; flat_len >= 3 && base <= last; base += kChunk) {
-        // (1) flag this thread's kPerThread consecutive samples.
+        // (1) flag this thread's kPerThread consecutive samples: strict
+        // extrema better than the threshold at the start of the chunk.
         uint32_t flags = 0;
         const uint64_t i0 = base + (uint64_t)tid * kPerThread;
+        const float thr0 = thr_sh;
 #pragma unroll
         for (int k = 0; k < kPerThread; k++) {
             const uint64_t i = i0 + k;
             if (i <= last) {
                 const float l = d[i - 1], v = d[i], r = d[i + 1];
-                const bool pk = use_max ? (v > l && v > r) : (v < l && v < r);
+                const bool pk = use_max ? (v > l && v > r && v > thr0)
+                                        : (v < l && v < r && v < thr0);
                 flags |= (pk ? 1u : 0u) << k;
             }
         }
@@ -172,6 +187,7 @@ __global__ void __launch_bounds__(kPeakThreads)
                 // Distance after feeding i: i - cand_idx + 1.
                 if (s.has_cand && (uint64_t)(i - s.cand_idx) + 1 >= md) promote(s);
             }
+            thr_sh = s.thr;
         }
         __syncthreads();
     }
