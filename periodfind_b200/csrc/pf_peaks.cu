@@ -86,6 +86,48 @@ __device__ __forceinline__ void promote(PeakState& s) {
     s.has_cand = false;
 }
 
+// The same list and candidate for n_peaks <= 32, held across one warp: lane
+// k keeps entry k, and every lane keeps the same copy of the rest of the
+// state.  An insertion takes the new entry's place from one ballot (the
+// entries not strictly worse stay ahead, which is where peaks.rs's bubble
+// stops) and shifts the entries behind it down one lane.
+struct WarpTop {
+    int64_t idx;  // this lane's entry
+    float val;
+    uint32_t count, n_peaks;
+    bool use_max;
+    bool has_cand;
+    int64_t cand_idx;
+    float cand_val;
+    float thr;
+};
+
+__device__ __forceinline__ void warp_insert(WarpTop& w, int lane, int64_t idx, float v) {
+    constexpr unsigned kAll = 0xffffffffu;
+    if (w.count == w.n_peaks &&
+        !better(w.use_max, v, __shfl_sync(kAll, w.val, (int)w.count - 1)))
+        return;
+    const bool ahead = lane < (int)w.count && !better(w.use_max, v, w.val);
+    const int pos = __popc(__ballot_sync(kAll, ahead));
+    const int64_t up_idx = __shfl_up_sync(kAll, w.idx, 1);
+    const float up_val = __shfl_up_sync(kAll, w.val, 1);
+    if (lane == pos) {
+        w.idx = idx;
+        w.val = v;
+    } else if (lane > pos) {
+        w.idx = up_idx;
+        w.val = up_val;
+    }
+    if (w.count < w.n_peaks) w.count++;
+    if (w.count == w.n_peaks) w.thr = __shfl_sync(kAll, w.val, (int)w.n_peaks - 1);
+}
+
+__device__ __forceinline__ void warp_promote(WarpTop& w, int lane) {
+    if (w.has_cand && better(w.use_max, w.cand_val, w.thr))
+        warp_insert(w, lane, w.cand_idx, w.cand_val);
+    w.has_cand = false;
+}
+
 // Dynamic shared memory: [kChunk int64 extrema indices][kChunk f32 values]
 // [n_peaks int64][n_peaks f32] (the best-first list).
 __global__ void __launch_bounds__(kPeakThreads)
@@ -104,6 +146,18 @@ __global__ void __launch_bounds__(kPeakThreads)
     const uint64_t c = blockIdx.x;
     const float* d = pg + c * flat_len;
     const bool use_max = use_max_i != 0;
+
+    const bool warp_list = n_peaks <= 32;
+    WarpTop w;
+    w.idx = -1;
+    w.val = 0.0f;
+    w.count = 0;
+    w.n_peaks = n_peaks;
+    w.use_max = use_max;
+    w.has_cand = false;
+    w.cand_idx = -1;
+    w.cand_val = use_max ? -INFINITY : INFINITY;
+    w.thr = use_max ? -INFINITY : INFINITY;
 
     PeakState s;
     s.idx = top_idx;
@@ -168,8 +222,43 @@ __global__ void __launch_bounds__(kPeakThreads)
             }
         }
         __syncthreads();
-        // (3) replay (one thread; state in registers and shared memory).
-        if (tid == 0) {
+        // (3) replay.  Up to 32 peaks: warp 0, 32 extrema at a time; lanes
+        // whose extremum no longer beats the threshold are dropped by one
+        // ballot (the threshold only gets stricter), the rest are fed in
+        // index order.
+        if (warp_list) {
+            if (wid == 0) {
+                const uint32_t ne = chunk_count;
+                for (uint32_t b0 = 0; b0 < ne; b0 += 32) {
+                    const uint32_t e = b0 + lane;
+                    const bool in = e < ne;
+                    const int64_t my_i = in ? ext_idx[e] : 0;
+                    const float my_v = in ? ext_val[e] : 0.0f;
+                    uint32_t pending =
+                        __ballot_sync(0xffffffffu, in && better(use_max, my_v, w.thr));
+                    while (pending) {
+                        const int k = __ffs(pending) - 1;
+                        const int64_t i = __shfl_sync(0xffffffffu, my_i, k);
+                        const float v = __shfl_sync(0xffffffffu, my_v, k);
+                        if (w.has_cand && (uint64_t)w.cand_idx + (md > 0 ? md - 1 : 0) <
+                                              (uint64_t)i)
+                            warp_promote(w, lane);
+                        if (better(use_max, v, w.thr) &&
+                            (!w.has_cand || better(use_max, v, w.cand_val))) {
+                            w.cand_idx = i;
+                            w.cand_val = v;
+                            w.has_cand = true;
+                        }
+                        if (w.has_cand && (uint64_t)(i - w.cand_idx) + 1 >= md)
+                            warp_promote(w, lane);
+                        pending &= ~(1u << k);
+                        pending &= __ballot_sync(0xffffffffu, better(use_max, my_v, w.thr));
+                    }
+                }
+                if (lane == 0) thr_sh = w.thr;
+            }
+        } else if (tid == 0) {
+            // More than 32 peaks: one thread, the list in shared memory.
             const uint32_t ne = chunk_count;
             for (uint32_t e = 0; e < ne; e++) {
                 const int64_t i = ext_idx[e];
@@ -191,7 +280,19 @@ __global__ void __launch_bounds__(kPeakThreads)
         }
         __syncthreads();
     }
-    if (tid == 0) promote(s);  // finalize (peaks.rs:207-209)
+    // Finalize (peaks.rs:207-209) and write the row.
+    if (warp_list) {
+        if (wid == 0) {
+            warp_promote(w, lane);
+            if (lane < (int)n_peaks) {
+                const bool have = (uint32_t)lane < w.count;
+                out_idx[c * n_peaks + lane] = have ? w.idx : -1;
+                out_val[c * n_peaks + lane] = have ? w.val : 0.0f;
+            }
+        }
+        return;
+    }
+    if (tid == 0) promote(s);
     __syncthreads();
     const uint32_t count = __shfl_sync(0xffffffffu, s.count, 0);
     if (wid == 0) {

@@ -495,3 +495,38 @@ def test_autotuned_launch_shapes_change_no_value(gpu):
     for name in ("[0,64)", "[64,256)", "[256,1024)", "[1024,4096)", "[4096,inf)"):
         assert f"class={name}" in report, report
     assert "ce bin" in report and "aov bin" in report and "ls fold-split" in report
+
+
+@pytest.mark.parametrize("use_max", [True, False])
+def test_peaks_adversarial_rows_match_oracle(gpu, oracle, use_max):
+    """The device peak search drops extrema that are not better than the
+    threshold at the start of their 2048-sample chunk before its serial
+    replay.  Rows that stress that rule match the oracle's streaming search
+    (rust/src/peaks.rs:18-238) exactly:
+
+    - a rising trend, so the threshold moves in every chunk;
+    - heavily quantised values, so extrema tie the threshold;
+    - more peaks requested than one chunk has extrema;
+    - a long min_distance;
+    - constant, NaN and infinite samples."""
+    rng = np.random.default_rng(31)
+    n = 30000  # 15 chunks
+    x = np.linspace(0.0, 5.0, n)
+    rows = [
+        x + rng.normal(0, 1, n),                      # rising trend
+        -x + rng.normal(0, 1, n),                     # falling trend
+        np.round(rng.normal(0, 1, n) * 2) / 2,        # coarse quantisation: ties
+        np.round(x * 3 + rng.normal(0, 0.5, n)),      # ties on a trend
+        np.sin(np.arange(n) * 0.37) + 1e-3 * rng.normal(0, 1, n),
+        np.full(n, 2.0),                              # no extrema
+        rng.normal(0, 1, n),
+    ]
+    rows[6][rng.integers(0, n, 50)] = np.nan
+    rows[6][rng.integers(0, n, 20)] = np.inf
+    rows[6][rng.integers(0, n, 20)] = -np.inf
+    data = np.stack(rows).astype(np.float32).reshape(len(rows), n, 1)
+    for n_peaks, min_distance in ((1, 1), (32, 1), (32, 7), (700, 1), (40, 3000)):
+        idx, val = gpu.find_top_peaks_batched(data, n_peaks, min_distance, use_max)
+        oi, ov = oracle.find_top_peaks_batched(data, n_peaks, min_distance, use_max)
+        np.testing.assert_array_equal(idx, oi, err_msg=f"{n_peaks} {min_distance}")
+        np.testing.assert_array_equal(val, ov, err_msg=f"{n_peaks} {min_distance}")
