@@ -1,16 +1,19 @@
 // pf_api.cu -- the C ABI (include/pf.h): argument checks, packing, launch
 // decomposition and the device pipeline
-//     pack (host, pinned) -> one H2D copy -> preparation kernel ->
-//     fused fold/bin/statistic kernel -> periodogram D2H, or peak search
-//     on the device and a D2H of the peaks only.
+//     pack (host, pinned) -> one H2D copy -> preparation kernels ->
+//     fused fold/bin/statistic kernel (one launch for the plain form, one
+//     per curve-length class with its tuned shape for the chosen form) ->
+//     periodogram D2H, or peak search / row statistics on the device and a
+//     D2H of those only.  Peak calls with PF_ASYNC return once their work
+//     is queued; pf_wait collects them.
 //
 // Compared with the reference's drivers (periodfind/cuda/ce.cu:420-562,
 // aov.cu:429-576, ls.cu:232-359), which allocate and free every buffer per
 // call, copy each curve with its own pageable memcpy, launch one or two
 // kernels per curve and exit() on any CUDA error, this driver keeps
 // grow-only device and pinned buffers in the context, moves the whole batch
-// in one copy, launches one kernel for the whole batch and reports errors
-// as status codes.
+// in one copy, launches a handful of kernels for the whole batch and
+// reports errors as status codes.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdarg.h>

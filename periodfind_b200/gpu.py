@@ -123,28 +123,37 @@ class _Periodogram:
                                          int(min_distance), idx, val))
         return idx, val
 
-    def _peaks_overlapped(self, times, mags, periods, period_dts, n_peaks, min_distance):
-        """'peaks' output.  Large batches run as a few consecutive chunks in a
+    # Chunk boundaries of a pipelined 'peaks' batch (fractions of its
+    # curves).  The first chunk is small so that the GPU starts early, and
+    # so is the last, whose result building nothing overlaps.
+    _CHUNK_EDGES = (0.0, 0.1, 0.37, 0.64, 0.9, 1.0)
+
+    def _peaks_overlapped(self, times, mags, periods, period_dts, n_peaks, min_distance,
+                          center=False, normalize=False):
+        """'peaks' output, with the magnitudes prepared here (centre or
+        normalise).  Large batches run as a few consecutive chunks in a
         pipeline: each chunk's native call only queues its work (PF_ASYNC)
-        and returns, so the next chunk is packed and queued while the GPU
-        runs this one, and a chunk's result objects are built while the GPU
-        runs the next.  Results are identical to one call."""
+        and returns, so the next chunk is prepared, packed and queued while
+        the GPU runs this one, and a chunk's result objects are built while
+        the GPU runs the next.  Results are identical to one call."""
         n = len(times)
         points = sum(len(t) for t in times)
-        n_chunks = 4 if (n >= 64 and points * len(periods) * len(period_dts) >= 2e10) else 1
-        if n_chunks == 1:
+        if not (n >= 64 and points * len(periods) * len(period_dts) >= 2e10):
+            mags = prepare_magnitudes(mags, center, normalize)
             idx, val = self.peaks(times, mags, periods, period_dts, n_peaks, min_distance)
             return unravel_peaks(idx, val, periods, period_dts, n_peaks)
         n_peaks = int(n_peaks)
         if n_peaks < 0:
             raise ValueError("n_peaks must be >= 0")
         ctx = nat.default_context(self.device)
-        bounds = [round(n * k / n_chunks) for k in range(n_chunks + 1)]
+        bounds = [round(n * f) for f in self._CHUNK_EDGES]
+        n_chunks = len(bounds) - 1
         outs = []  # (indices, values) of each queued chunk, alive until collected
         res = []
         with ctx.lock:
             def queue(k):
-                b = nat.CurveBatch(times[bounds[k]:bounds[k + 1]], mags[bounds[k]:bounds[k + 1]])
+                a, e = bounds[k], bounds[k + 1]
+                b = nat.CurveBatch(times[a:e], prepare_magnitudes(mags[a:e], center, normalize))
                 idx = np.full((b.n, n_peaks), -1, dtype=np.int64)
                 val = np.zeros((b.n, n_peaks), dtype=np.float32)
                 ctx.check(self._native_peaks(ctx, b, periods, period_dts, n_peaks,
@@ -205,11 +214,15 @@ class _Periodogram:
         ensure_float32(mags, "mags")
         periods = _grid(periods, "periods")
         period_dts = _grid(period_dts, "period_dts")
-        mags_use = prepare_magnitudes(mags, center, normalize)
-
         if output == "peaks":
-            return self._peaks_overlapped(times, mags_use, periods, period_dts, int(n_peaks),
-                                          min_distance)
+            # The magnitudes are prepared chunk by chunk inside the pipeline;
+            # the centre / normalise conflict warns once, here.
+            if center and normalize:
+                prepare_magnitudes([], center, normalize)
+                normalize = False
+            return self._peaks_overlapped(times, mags, periods, period_dts, int(n_peaks),
+                                          min_distance, center, normalize)
+        mags_use = prepare_magnitudes(mags, center, normalize)
 
         if (output == "stats" and 1 <= int(n_stats) < len(periods) * len(period_dts)
                 and (not self._use_max or len(period_dts) == 1)):

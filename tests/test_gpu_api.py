@@ -397,3 +397,33 @@ def test_async_call_rules(gpu):
         assert lib.pf_wait(h) == nat.PF_EINVAL
     finally:
         ctx.close()
+
+
+def test_chunked_peaks_prepare_magnitudes_per_chunk(gpu):
+    """A pipelined 'peaks' batch prepares the magnitudes chunk by chunk; CE's
+    normalisation per chunk equals the whole batch's, and the centre /
+    normalise conflict (periodfind/_utils.py:29-37) warns once per call."""
+    from periodfind_b200._utils import prepare_magnitudes
+    from periodfind_b200.gpu import unravel_peaks
+
+    rng = np.random.default_rng(12)
+    ts = [lc.uniform_times(rng, 4096, 2000.0) for _ in range(128)]
+    ms = [lc.noisy(rng, 15.0 + 0.3 * lc.sinusoid(t, float(rng.uniform(0.5, 10))), 0.05)
+          for t in ts]
+    P = np.exp(np.linspace(np.log(0.1), np.log(100.0), 40000)).astype(np.float32)
+    D = np.zeros(1, np.float32)
+    obj = gpu.ConditionalEntropy(10, 10)
+    got = obj.calc(ts, ms, P, D, output="peaks", n_peaks=8)
+    idx, val = obj.peaks(ts, prepare_magnitudes(ms, False, True), P, D, 8)
+    want = unravel_peaks(idx, val, P, D, 8)
+    assert len(got) == 128
+    for g, w in zip(got, want):
+        assert [(s.params, s.value) for s in g] == [(s.params, s.value) for s in w]
+    with warnings.catch_warnings(record=True) as rec:
+        warnings.simplefilter("always")
+        got = obj.calc(ts, ms, P, D, output="peaks", n_peaks=8, center=True, normalize=True)
+    assert sum(issubclass(r.category, RuntimeWarning) for r in rec) == 1
+    idx, val = obj.peaks(ts, [m - np.mean(m) for m in ms], P, D, 8)
+    want = unravel_peaks(idx, val, P, D, 8)
+    for g, w in zip(got, want):
+        assert [(s.params, s.value) for s in g] == [(s.params, s.value) for s in w]
