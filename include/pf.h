@@ -107,8 +107,14 @@ const char* pf_last_error(const pf_ctx* ctx);
 
 /* Replaces ConditionalEntropy::CalcCEValsBatched
  * (periodfind/cuda/ce.h, ce.cu:420-562; bound at periodfind/ce.pyx:25-39).
- * n_phase x n_mag histogram with phase_overlap / mag_overlap bin extents;
- * magnitudes are expected in [0, 1) (normalise first).  Minimum is best. */
+ * n_phase x n_mag histogram with phase_overlap / mag_overlap bin extents.
+ * Magnitudes are bin coordinates meant to lie in [0, 1) (normalise first).
+ * Values outside are accepted, as the reference accepts them (its own tests
+ * centre CE magnitudes, tests/test_periodfind.py:535-546): a negative value
+ * falls in magnitude bin 0 (the float-to-integer conversion saturates, as
+ * in the reference's CUDA and Rust paths) and a value >= 1 wraps modulo
+ * n_mag.  That is memory-safe, where the reference writes outside the
+ * curve's bins (periodfind/cuda/ce.cu:66-77).  Minimum is best. */
 int pf_ce(pf_ctx* ctx, const float* const* times, const float* const* mags,
           const uint64_t* lengths, uint64_t n_curves, const float* periods,
           uint64_t n_per, const float* period_dts, uint64_t n_pdt,

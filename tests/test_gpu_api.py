@@ -427,3 +427,27 @@ def test_chunked_peaks_prepare_magnitudes_per_chunk(gpu):
     want = unravel_peaks(idx, val, P, D, 8)
     for g, w in zip(got, want):
         assert [(s.params, s.value) for s in g] == [(s.params, s.value) for s in w]
+
+
+def test_ce_magnitudes_outside_unit_interval_run_memory_safely(gpu):
+    """CE magnitudes are bin coordinates meant to lie in [0, 1), but the
+    reference's own tests run CE on centred magnitudes
+    (tests/test_periodfind.py:535-546), so values outside are accepted.
+    Raw (15 +- 0.3), centred, NaN and >= 1 magnitudes give a periodogram of
+    the right shape; a centred curve's negative values fall in magnitude bin
+    0, which the CPU-semantics oracle (Rust's saturating cast) reproduces."""
+    from oracle import oracle as O
+
+    t, m = lc.sine_curve(2.0, n=300)
+    P = np.linspace(1.0, 5.0, 200).astype(np.float32)
+    Z = np.zeros(1, np.float32)
+    ce = gpu.ConditionalEntropy()
+    raw = (15.0 + 0.3 * m).astype(np.float32)
+    odd = lc.normalize(m).astype(np.float32)
+    odd[7], odd[9] = np.nan, 1.0
+    for mags in (raw, odd, (m - np.mean(m)).astype(np.float32)):
+        for output in ("stats", "periodogram", "peaks"):
+            assert len(ce.calc([t], [mags], P, Z, output=output, normalize=False)) == 1
+    cen = (0.3 * (m - np.mean(m))).astype(np.float32)
+    got = gpu.ConditionalEntropy(semantics="cpu").periodograms([t], [cen], P, Z)
+    np.testing.assert_allclose(got, O.ce([t], [cen], P, Z), rtol=2e-6)
