@@ -446,6 +446,58 @@ def ragged_arm(args):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------------------ FPW
+
+
+def fpw_arm(args):
+    """FPW(10) over the benchmark batch (1000 curves x 4096 points, 10000 log
+    periods in [0.1, 100] d x pdts [0, 1e-6]) with per-point uncertainties
+    U[0.02, 0.1]: device time of the chosen and plain forms (the FPW kernel,
+    CUDA events), end-to-end calc(output='peaks') from numpy lists, and the
+    oracle (the Rust path's restatement) on all host cores over a sample."""
+    from periodfind_b200 import gpu
+
+    ts, ms, periods, pdts = make_workload(args.curves)
+    rng = np.random.default_rng(SEED + 6)
+    es = [rng.uniform(0.02, 0.1, len(t)).astype(np.float32) for t in ts]
+    evals = sum(len(t) for t in ts) * len(periods) * len(pdts)
+    out = {"workload": f"FPW(10), {len(ts)} curves x {N_POINTS} pts, {N_PERIODS} log periods "
+                       f"[0.1,100] d x pdts {list(PDTS)}, errs U[0.02,0.1]", "evals": evals}
+    from periodfind_b200 import _native as nat
+
+    ctx = nat.default_context(0)
+    for mode in ("chosen", "plain"):
+        obj = gpu.FPW(10, mode=mode)
+        obj.periodograms(ts, ms, periods, pdts, errs=es)
+        k = []
+        for _ in range(max(1, args.steps)):
+            obj.periodograms(ts, ms, periods, pdts, errs=es)
+            k.append(ctx.lib.pf_last_kernel_ms(ctx.handle))
+        kms = float(np.median(k))
+        obj.calc(ts, ms, periods, pdts, errs=es, output="peaks", n_peaks=N_PEAKS)
+        w = []
+        for _ in range(max(1, min(args.steps, 3))):
+            t0 = time.perf_counter()
+            obj.calc(ts, ms, periods, pdts, errs=es, output="peaks", n_peaks=N_PEAKS)
+            w.append(time.perf_counter() - t0)
+        out[mode] = {"kernel_ms": kms, "evals_per_s": evals / (kms * 1e-3),
+                     "e2e_ms": float(np.median(w)) * 1e3,
+                     "e2e_evals_per_s": evals / float(np.median(w))}
+    out["chosen_over_plain"] = out["plain"]["kernel_ms"] / out["chosen"]["kernel_ms"]
+    if not args.no_cpu:
+        from oracle import oracle as O
+
+        cores = os.cpu_count() or 1
+        k = 20
+        t0 = time.perf_counter()
+        O.fpw(ts[:k], ms[:k], periods, pdts, 10, errs=es[:k], n_threads=cores)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": k * N_POINTS * N_PERIODS * len(PDTS) / dt,
+                               "unit": "evals/s", "cores": cores, "kind": "port",
+                               "sample": f"{k} of {len(ts)} curves, {dt:.1f} s"}
+    print(json.dumps(out), flush=True)
+
+
 # ------------------------------------------------------ small CE batch
 
 
@@ -706,18 +758,18 @@ def main():
     ap.add_argument("--curves", type=int, default=N_CURVES)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "small", "ragged", "lsgrad", "precision"],
+                    choices=["batch", "small", "ragged", "lsgrad", "precision", "fpw"],
                     help="'small': CE stats on 100 x 1024; 'ragged': the mixed ragged batch; "
                          "'lsgrad': LS derivatives and "
                          "Newton refinement; 'precision': LS folds on the precision-study "
-                         "batch (separate reports, 1 GPU)")
+                         "batch; 'fpw': FPW on the benchmark batch (separate reports, 1 GPU)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
         return
     if args.workload != "batch":
         {"small": small_arm, "ragged": ragged_arm, "lsgrad": lsgrad_arm,
-         "precision": precision_arm}[args.workload](args)
+         "precision": precision_arm, "fpw": fpw_arm}[args.workload](args)
         return
 
     import torch

@@ -165,6 +165,25 @@ int pf_ls_peaks(pf_ctx* ctx, const float* const* times,
                 uint32_t min_distance, int mode, int64_t* out_idx,
                 float* out_val);
 
+/* FPW, the fast phase-folding weighted statistic (Finkbeiner et al. 2025).
+ * Replaces FPW::CalcFPWBatched (periodfind/cuda/fpw.h, fpw.cu; bound at
+ * periodfind/fpw.pyx:14-26) and calc_fpw_batched / calc_fpw_peaks_batched
+ * (rust/src/lib.rs:202-256, 680-720).  Per point w = 1 / err^2 (errs NULL,
+ * or errs[c] NULL: err = 1); per phase bin V = sum w, Y = sum w * m; value
+ * sum over bins with V > 0 of Y^2 / (2 V).  Maximum is best.  n_bins in
+ * [1, 128].  Magnitudes are used as given.  PF_MODE_CHOSEN folds without a
+ * divide (same values); PF_SEM_CPU takes the Rust path's bin rule and IEEE
+ * arithmetic.  PF_ASYNC and PF_TIMING are refused. */
+int pf_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
+           const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
+           const float* periods, uint64_t n_per, const float* period_dts, uint64_t n_pdt,
+           uint32_t n_bins, int mode, float* out);
+int pf_fpw_peaks(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                 const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
+                 const float* periods, uint64_t n_per, const float* period_dts, uint64_t n_pdt,
+                 uint32_t n_bins, uint32_t n_peaks, uint32_t min_distance, int mode,
+                 int64_t* out_idx, float* out_val);
+
 /* Collect the oldest pending PF_ASYNC peak call on this context: wait for
  * its work, then write its peaks into the out_idx / out_val it was given.
  * Calls are collected in the order they were made.  PF_EINVAL when none is

@@ -169,6 +169,66 @@ ORC_API float orc_ce_counts(const float* times, const float* mags,
     return v;
 }
 
+/* ------------------------------------------------------------------ FPW */
+
+/* rust/src/fpw.rs:12-66 for one curve and one (period, pdt): inverse
+ * variances w = 1 / err^2 and w * m (computed once per curve by the caller),
+ * per bin V = sum w and Y = sum w * m in point order, then
+ * sum over bins with V > 0 of Y^2 / (2 V), all in f32. */
+static float orc_fpw_cell(const float* times, const float* iv, const float* ivy,
+                          uint64_t length, float period, float period_dt,
+                          uint32_t num_bins, float* vt, float* yt) {
+    const float pdt_corr = orc_pdt_correction(period, period_dt);
+    for (uint32_t k = 0; k < num_bins; k++) vt[k] = yt[k] = 0.0f;
+    for (uint64_t i = 0; i < length; i++) {
+        const float phase = orc_fold_time(times[i], period, pdt_corr, 0);
+        uint64_t bin = sat_u64(phase * (float)num_bins);
+        if (bin > num_bins - 1) bin = num_bins - 1;
+        vt[bin] += iv[i];
+        yt[bin] += ivy[i];
+    }
+    float delta_chi = 0.0f;
+    for (uint32_t k = 0; k < num_bins; k++)
+        if (vt[k] > 0.0f) delta_chi += yt[k] * yt[k] / (2.0f * vt[k]);
+    return delta_chi;
+}
+
+/* rust/src/lib.rs:202-256 (calc_fpw_batched): errs NULL means err = 1. */
+ORC_API void orc_fpw_batched(const float* times, const float* mags, const float* errs,
+                             const int64_t* offsets, int64_t n_curves,
+                             const float* periods, int64_t n_per,
+                             const float* pdts, int64_t n_pdt, uint32_t num_bins,
+                             int n_threads, float* out) {
+    set_threads(n_threads);
+    const int64_t n_pts = n_curves > 0 ? offsets[n_curves] : 0;
+    float* iv = (float*)malloc((size_t)(n_pts > 0 ? n_pts : 1) * sizeof(float));
+    float* ivy = (float*)malloc((size_t)(n_pts > 0 ? n_pts : 1) * sizeof(float));
+    for (int64_t i = 0; i < n_pts; i++) {
+        const float e = errs ? errs[i] : 1.0f;
+        iv[i] = 1.0f / (e * e);
+        ivy[i] = iv[i] * mags[i];
+    }
+    const int64_t per_curve = n_per * n_pdt;
+    const int64_t total = n_curves * per_curve;
+#pragma omp parallel
+    {
+        float* vt = (float*)malloc((size_t)num_bins * sizeof(float));
+        float* yt = (float*)malloc((size_t)num_bins * sizeof(float));
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t k = 0; k < total; k++) {
+            int64_t c = k / per_curve, g = k % per_curve;
+            int64_t p = g / n_pdt, d = g % n_pdt;
+            const int64_t o = offsets[c];
+            out[k] = orc_fpw_cell(times + o, iv + o, ivy + o, (uint64_t)(offsets[c + 1] - o),
+                                  periods[p], pdts[d], num_bins, vt, yt);
+        }
+        free(vt);
+        free(yt);
+    }
+    free(iv);
+    free(ivy);
+}
+
 /* ------------------------------------------------------------------ AOV */
 
 typedef struct {

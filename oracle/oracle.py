@@ -51,6 +51,8 @@ def _load():
     i64, u32, c_int = ctypes.c_int64, ctypes.c_uint32, ctypes.c_int
     lib.orc_ce_batched.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
                                    u32, u32, u32, u32, c_int, c_int, _f32p]
+    lib.orc_fpw_batched.argtypes = [_f32p, _f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
+                                    ctypes.c_uint32, c_int, _f32p]
     lib.orc_aov_batched.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
                                     u32, u32, c_int, c_int, _f32p]
     lib.orc_ls_batched.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
@@ -115,6 +117,22 @@ def ce(times, mags, periods, pdts, n_phase=10, n_mag=10, phase_overlap=1, mag_ov
                        _ptr(p, _f32p), len(p), _ptr(d, _f32p), len(d), n_phase, n_mag,
                        phase_overlap, mag_overlap, int(fused_tcorr), n_threads,
                        _ptr(out, _f32p))
+    return out
+
+
+def fpw(times, mags, periods, pdts, n_bins=10, errs=None, n_threads=0):
+    """rust/src/fpw.rs:12-66 batched as rust/src/lib.rs:202-256 (errs None:
+    unit uncertainties, as periodfind/cpu/__init__.py:466-467)."""
+    lib = _load()
+    t, m, off = pack(times, mags)
+    e = None
+    if errs is not None:
+        _, e, _ = pack(times, errs)
+    p, d = _grid(periods, pdts)
+    out = np.zeros((len(off) - 1, len(p), len(d)), np.float32)
+    lib.orc_fpw_batched(_ptr(t, _f32p), _ptr(m, _f32p), None if e is None else _ptr(e, _f32p),
+                        _ptr(off, _i64p), len(off) - 1, _ptr(p, _f32p), len(p), _ptr(d, _f32p),
+                        len(d), n_bins, n_threads, _ptr(out, _f32p))
     return out
 
 
@@ -309,6 +327,8 @@ def _load_ref():
             "where the reference checkout exists)")
     lib = ctypes.CDLL(_REF_PATH)
     i64, u32 = ctypes.c_int64, ctypes.c_uint32
+    lib.pfref_fpw.argtypes = [_f32p, _f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64, u32,
+                              _f32p]
     lib.pfref_ce.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
                              u32, u32, u32, u32, _f32p]
     lib.pfref_aov.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
@@ -334,6 +354,13 @@ def ref_cuda(algo, times, mags, periods, pdts, **kw):
                       _ptr(out, _f32p))
     elif algo == "ls":
         lib.pfref_ls(*args, _ptr(out, _f32p))
+    elif algo == "fpw":
+        errs = kw.get("errs")
+        e = (np.ones(len(t), np.float32) if errs is None
+             else np.ascontiguousarray(np.concatenate(errs), np.float32))
+        lib.pfref_fpw(_ptr(t, _f32p), _ptr(m, _f32p), _ptr(e, _f32p), _ptr(off, _i64p),
+                      len(off) - 1, _ptr(p, _f32p), len(p), _ptr(d, _f32p), len(d),
+                      kw.get("n_bins", 10), _ptr(out, _f32p))
     else:
         raise ValueError(algo)
     return out

@@ -1,9 +1,10 @@
 // ref_shim.cu -- C entry points onto the reference's own CUDA host drivers.
 //
 // TEST INFRASTRUCTURE ONLY.  Linked (by oracle/Makefile, target `ref`) with
-// the reference's periodfind/cuda/{ce,aov,ls}.cu compiled from the reference
+// the reference's periodfind/cuda/{ce,aov,ls,fpw}.cu compiled from the reference
 // checkout, it exposes exactly the calls the reference's Cython wrappers make
-// (periodfind/ce.pyx:183-187, aov.pyx:166-170, ls.pyx:150-154), so tests can
+// (periodfind/ce.pyx:183-187, aov.pyx:166-170, ls.pyx:150-154,
+// fpw.pyx:150-154), so tests can
 // run the reference's CUDA path on the GPU and compare bin occupancies and
 // periodograms against periodfind_b200.  The product never links this.
 #include <cstdint>
@@ -11,6 +12,7 @@
 
 #include "aov.h"
 #include "ce.h"
+#include "fpw.h"
 #include "ls.h"
 
 namespace {
@@ -69,6 +71,22 @@ int pfref_ls(const float* times, const float* mags, const int64_t* offsets,
     LombScargle ls;
     ls.CalcLSBatched(t, m, len, periods, pdts, (size_t)n_per, (size_t)n_pdt,
                      out);
+    return 0;
+}
+
+// FPW(n_bins).CalcFPWBatched; errs is packed like mags (unit errors are
+// passed explicitly, as the Cython wrapper does for errs=None).
+int pfref_fpw(const float* times, const float* mags, const float* errs,
+              const int64_t* offsets, int64_t n_curves, const float* periods,
+              int64_t n_per, const float* pdts, int64_t n_pdt, uint32_t n_bins,
+              float* out) {
+    std::vector<float*> t, m, e;
+    std::vector<size_t> len;
+    unpack(times, mags, offsets, n_curves, t, m, len);
+    e.resize(n_curves);
+    for (int64_t c = 0; c < n_curves; c++) e[c] = const_cast<float*>(errs + offsets[c]);
+    FPW fpw(n_bins);
+    fpw.CalcFPWBatched(t, m, e, len, periods, pdts, (size_t)n_per, (size_t)n_pdt, out);
     return 0;
 }
 

@@ -1,7 +1,7 @@
 """periodfind_b200: periodfind's batched periodograms (Conditional Entropy,
-Analysis of Variance, Lomb-Scargle) on NVIDIA B200 (sm_100a).
+Analysis of Variance, Lomb-Scargle, FPW) on NVIDIA B200 (sm_100a).
 
-    from periodfind_b200.gpu import ConditionalEntropy, AOV, LombScargle
+    from periodfind_b200.gpu import ConditionalEntropy, AOV, LombScargle, FPW
     ce = ConditionalEntropy(n_phase=10, n_mag=10)
     stats = ce.calc(times, mags, periods, period_dts, output="stats")
 
@@ -13,12 +13,13 @@ absent or no B200 is visible.
 
 from .stats import Periodogram, Statistics
 
-__all__ = ["Statistics", "Periodogram", "ConditionalEntropy", "AOV", "LombScargle", "gpu"]
+__all__ = ["Statistics", "Periodogram", "ConditionalEntropy", "AOV", "LombScargle", "FPW",
+           "gpu"]
 __version__ = "0.1.0"
 
 
 def __getattr__(name):
-    if name in ("ConditionalEntropy", "AOV", "LombScargle", "gpu"):
+    if name in ("ConditionalEntropy", "AOV", "LombScargle", "FPW", "gpu"):
         import importlib
 
         gpu = importlib.import_module(__name__ + ".gpu")

@@ -56,6 +56,9 @@ SIGNATURES = {
     "pf_ls_peaks": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int, _vp,
                      _vp], _int),
     "pf_wait": ([_vp], _int),
+    "pf_fpw": ([_vp, _vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _int, _vp], _int),
+    "pf_fpw_peaks": ([_vp, _vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32,
+                      _int, _vp, _vp], _int),
     "pf_ce_stats": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32,
                      _u32, _int, _vp, _vp, _vp], _int),
     "pf_aov_stats": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _int,

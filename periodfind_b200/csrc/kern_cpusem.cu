@@ -7,4 +7,5 @@
 #include "pf_launch.h"
 #include "pf_fold.cuh"
 #include "pf_bin.cuh"
+#include "pf_fpw.cuh"
 #include "pf_kern_dispatch.inc"

@@ -988,6 +988,163 @@ int ls_common_checks(pf_ctx* ctx, const float* d_times, const int64_t* offsets,
     return PF_OK;
 }
 
+// FPW for host-pointer inputs (FPW::CalcFPWBatched, periodfind/cuda/fpw.cu;
+// calc_fpw_batched / calc_fpw_peaks_batched, rust/src/lib.rs:202-256,
+// 680-720).  The host computes the per-point weights as both references do
+// (iv = 1 / err^2, ivy = iv * m, errs absent = 1), packs them with the
+// times, and one launch covers every (curve, period derivative, period
+// tile); the peaks, when asked for, are found on the device.
+int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
+            const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
+            const float* periods, uint64_t n_per, const float* pdts, uint64_t n_pdt,
+            uint32_t n_bins, int mode, float* out, bool peaks, uint32_t n_peaks,
+            uint32_t min_distance, int64_t* out_idx, float* out_val) {
+    if (!ctx) return PF_EINVAL;
+    Job j;
+    j.algo = ALGO_LS;  // no bin-count checks of CE / AOV apply
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = pdts;
+    j.n_pdt = n_pdt;
+    j.peaks = peaks;
+    j.n_peaks = n_peaks;
+    j.out_idx = out_idx;
+    j.out_val = out_val;
+    j.out = out;
+    int rc = validate_common(ctx, j);
+    if (rc != PF_OK) return rc;
+    if (mode & (PF_ASYNC | PF_TIMING))
+        return fail(ctx, PF_EINVAL, "PF_ASYNC and PF_TIMING do not apply to FPW");
+    if (n_bins < 1 || n_bins > kFpwMaxBins)
+        return fail(ctx, PF_EINVAL, "n_bins must be in [1, %u], got %u", kFpwMaxBins, n_bins);
+    if (n_curves == 0) return PF_OK;
+    if (!times || !mags || !lengths) return fail(ctx, PF_EINVAL, "times/mags/lengths is NULL");
+    const uint64_t n_cells = n_per * n_pdt;
+    if (n_cells == 0) return PF_OK;
+    if ((rc = check_grid_host(ctx, j)) != PF_OK) return rc;
+    std::vector<int64_t> off(n_curves);
+    std::vector<uint32_t> len(n_curves);
+    uint64_t total = 0;
+    for (uint64_t c = 0; c < n_curves; c++) {
+        if (lengths[c] > 0xFFFFFFFFull)
+            return fail(ctx, PF_EINVAL, "a curve has more than 2^32-1 points");
+        if (lengths[c] > 0 && (!times[c] || !mags[c]))
+            return fail(ctx, PF_EINVAL, "curve %llu has a NULL array", (unsigned long long)c);
+        off[c] = (int64_t)total;
+        len[c] = (uint32_t)lengths[c];
+        total += lengths[c];
+    }
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const size_t o_iv = align_up(total * 4, 256), o_ivy = o_iv + align_up(total * 4, 256);
+    const size_t o_off = o_ivy + align_up(total * 4, 256);
+    const size_t o_len = o_off + align_up(n_curves * 8, 256);
+    const size_t o_per = o_len + align_up(n_curves * 4, 256);
+    const size_t o_pdt = o_per + align_up(n_per * 4, 256);
+    const size_t bytes = o_pdt + align_up(n_pdt * 4, 256);
+    if ((rc = staging_ready(ctx)) != PF_OK) return rc;
+    if ((rc = ensure_pinned(ctx, ctx->h_in, bytes)) != PF_OK) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_in, bytes)) != PF_OK) return rc;
+    char* hb = (char*)ctx->h_in.p;
+    float* ht = (float*)hb;
+    float* hiv = (float*)(hb + o_iv);
+    float* hivy = (float*)(hb + o_ivy);
+    double tmax = 0.0;
+    {
+        const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        const unsigned nthr = total > (1u << 20) ? hw : 1u;
+        std::vector<int> bad(nthr, 0);
+        std::vector<float> tmx(nthr, 0.0f);
+        auto worker = [&](unsigned w) {
+            for (uint64_t c = w; c < n_curves; c += nthr) {
+                const float* t = times[c];
+                const float* m = mags[c];
+                const float* e = errs ? errs[c] : nullptr;
+                const int64_t o = off[c];
+                for (uint32_t i = 0; i < len[c]; i++) {
+                    const float x = t[i];
+                    if (!std::isfinite(x)) bad[w] = 1;
+                    tmx[w] = std::max(tmx[w], std::fabs(x));
+                    ht[o + i] = x;
+                    const float err = e ? e[i] : 1.0f;
+                    // This unit is built without multiply-add contraction.
+                    const float w_i = 1.0f / (err * err);
+                    hiv[o + i] = w_i;
+                    hivy[o + i] = w_i * m[i];
+                }
+            }
+        };
+        if (nthr == 1) {
+            worker(0);
+        } else {
+            std::vector<std::thread> th;
+            for (unsigned w = 0; w < nthr; w++) th.emplace_back(worker, w);
+            for (auto& t : th) t.join();
+        }
+        for (int b : bad)
+            if (b) return fail(ctx, PF_EINVAL, "times must be finite");
+        for (float x : tmx) tmax = std::max(tmax, (double)x);
+    }
+    memcpy(hb + o_off, off.data(), n_curves * 8);
+    memcpy(hb + o_len, len.data(), n_curves * 4);
+    memcpy(hb + o_per, periods, n_per * 4);
+    memcpy(hb + o_pdt, pdts, n_pdt * 4);
+    cudaStream_t s = ctx->stream;
+    char* db = (char*)ctx->d_in.p;
+    PF_CUDA(cudaMemcpyAsync(db, hb, bytes, cudaMemcpyHostToDevice, s), "H2D inputs");
+    PF_CUDA(cudaEventRecord(ctx->ev_staged, s), "event");
+    ctx->staged_pending = true;
+    const size_t out_bytes = (size_t)n_curves * n_cells * 4;
+    if ((rc = ensure_dev(ctx, ctx->d_out, out_bytes)) != PF_OK) return rc;
+    FpwParams p{};
+    p.t = (const float*)db;
+    p.iv = (const float*)(db + o_iv);
+    p.ivy = (const float*)(db + o_ivy);
+    p.off = (const int64_t*)(db + o_off);
+    p.len = (const uint32_t*)(db + o_len);
+    p.periods = (const float*)(db + o_per);
+    p.pdts = (const float*)(db + o_pdt);
+    p.n_per = n_per;
+    p.n_pdt = (uint32_t)n_pdt;
+    p.n_bins = n_bins;
+    // FPW::FPW (fpw.cu:19-22): 1.0 / (float)n_bins in double, stored as float.
+    p.bin_size = (float)(1.0 / (double)(float)n_bins);
+    p.out = (float*)ctx->d_out.p;
+    p.tmax = tmax;
+    p.edge_d = edge_guard(n_bins);
+    const bool exact = (mode & PF_MODE_CHOSEN) != 0;
+    PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
+    PF_CUDA((mode & PF_SEM_CPU) ? launch_fpw_cpusem(p, exact, n_curves, s)
+                                : launch_fpw_cudasem(p, exact, n_curves, s),
+            "FPW kernel launch");
+    PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
+    ctx->timed_pending = true;
+    ctx->launches++;
+    if (peaks) {
+        if (n_peaks > 0) {
+            const size_t pk = (size_t)n_curves * n_peaks;
+            if ((rc = ensure_dev(ctx, ctx->d_pidx, pk * 8)) != PF_OK) return rc;
+            if ((rc = ensure_dev(ctx, ctx->d_pval, pk * 4)) != PF_OK) return rc;
+            PF_CUDA(launch_peaks(p.out, n_curves, n_cells, n_peaks, min_distance, 1,
+                                 (int64_t*)ctx->d_pidx.p, (float*)ctx->d_pval.p, s),
+                    "peak search launch");
+            ctx->launches++;
+            PF_CUDA(cudaMemcpyAsync(out_idx, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
+                    "D2H peak indices");
+            PF_CUDA(cudaMemcpyAsync(out_val, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s),
+                    "D2H peak values");
+        }
+    } else {
+        PF_CUDA(cudaMemcpyAsync(out, p.out, out_bytes, cudaMemcpyDeviceToHost, s),
+                "D2H periodogram");
+    }
+    PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
+    ctx->staged_pending = false;
+    read_kernel_time(ctx);
+    return PF_OK;
+}
+
 }  // namespace
 
 size_t pfk::fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag) {
@@ -1439,6 +1596,23 @@ int pf_ls_peaks(pf_ctx* ctx, const float* const* times, const float* const* mags
     j.out_idx = out_idx;
     j.out_val = out_val;
     return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
+           const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
+           const float* periods, uint64_t n_per, const float* period_dts, uint64_t n_pdt,
+           uint32_t n_bins, int mode, float* out) {
+    return run_fpw(ctx, times, mags, errs, lengths, n_curves, periods, n_per, period_dts, n_pdt,
+                   n_bins, mode, out, false, 0, 0, nullptr, nullptr);
+}
+
+int pf_fpw_peaks(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                 const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
+                 const float* periods, uint64_t n_per, const float* period_dts, uint64_t n_pdt,
+                 uint32_t n_bins, uint32_t n_peaks, uint32_t min_distance, int mode,
+                 int64_t* out_idx, float* out_val) {
+    return run_fpw(ctx, times, mags, errs, lengths, n_curves, periods, n_per, period_dts, n_pdt,
+                   n_bins, mode, nullptr, true, n_peaks, min_distance, out_idx, out_val);
 }
 
 int pf_wait(pf_ctx* ctx) {

@@ -1,0 +1,158 @@
+// pf_fpw.cuh -- FPW (fast phase-folding weighted) periodogram, included by
+// each arithmetic unit after pf_fold.cuh and pf_bin.cuh.
+//
+// Statistic (rust/src/fpw.rs:12-66; periodfind/cuda/fpw.cu:45-224): each
+// point carries an inverse variance w = 1 / err^2 and w * m; the fold puts
+// it in one of n_bins phase bins; per bin V = sum w, Y = sum w * m; the
+// value is sum over bins with V > 0 of Y^2 / (2 V).  Maximum is best.
+//
+// Decomposition: a CTA per (curve, period derivative, tile of BLOCK trial
+// periods); thread j owns one period for the whole curve and keeps its own
+// V and Y in shared memory ([bin][thread], so a warp's updates hit 32
+// banks), adding the points in curve order -- the Rust path's order, so the
+// sums round as it does.  The curve streams through shared memory in tiles.
+//
+// The bin is the reference's for the unit's semantics:
+//   CUDA build: (size_t)(folded / bin_size), clamped to n_bins - 1
+//               (fpw.cu:28-30, 115-117);
+//   Rust path:  (folded * n_bins) as usize, clamped (fpw.rs:44);
+// with folded = (float)|q - floor(q)| for the correctly rounded quotient q.
+//
+// Plain form: that sequence for every point (FP64 divide).  Chosen form: the
+// bin from q' = t * RN(1/P) with a round-down floor and one round-down FMA
+// that yields floor(q' n_bins) and 20 fraction bits (the chosen CE / AOV bin
+// kernel's construction); a point whose fraction lies within the proven
+// guard of a bin edge takes the reference sequence instead (divide-free, the
+// same quotient).  Unlike the integer CE / AOV counters, float sums cannot
+// take a point back, so each point is tested before it is added.
+#pragma once
+
+#ifndef PF_KNS
+#error "include after defining PF_KNS"
+#endif
+
+namespace pfk {
+namespace PF_KNS {
+
+constexpr uint32_t kFpwTile = 1024;
+
+// The reference's bin of a folded phase, with this unit's arithmetic.
+__device__ __forceinline__ uint32_t fpw_ref_bin(float folded, const FpwParams& p) {
+#if PF_SEM_CPU_TU
+    const uint32_t b = trunc_u(folded * (float)p.n_bins);
+#else
+    const uint32_t b = trunc_u(folded / p.bin_size);
+#endif
+    return min(b, p.n_bins - 1u);
+}
+
+template <int BLOCK, bool CHOSEN>
+__global__ void __launch_bounds__(BLOCK)
+    fpw_kernel(const FpwParams p, uint32_t tiles_per_row) {
+    using TT = typename std::conditional<CHOSEN, double, float>::type;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    TT* st = reinterpret_cast<TT*>(fsm);
+    float* siv = reinterpret_cast<float*>(st + kFpwTile);
+    float* sivy = siv + kFpwTile;
+    float* bv = sivy + kFpwTile;          // [n_bins][BLOCK]
+    float* by = bv + p.n_bins * BLOCK;    // [n_bins][BLOCK]
+    __shared__ double warp_min[BLOCK / 32];
+
+    const uint64_t cta = blockIdx.x;
+    const uint32_t tile = (uint32_t)(cta % tiles_per_row);
+    const uint64_t row = cta / tiles_per_row;     // curve * n_pdt + pdt
+    const uint64_t c = row / p.n_pdt;
+    const uint32_t d = (uint32_t)(row % p.n_pdt);
+    const int tid = threadIdx.x;
+    const uint64_t pi = (uint64_t)tile * BLOCK + tid;
+    const bool active = pi < p.n_per;
+
+    const int64_t off = p.off[c];
+    const uint32_t n = p.len[c];
+    const uint32_t nb = p.n_bins;
+    for (uint32_t k = 0; k < nb; k++) {
+        bv[k * BLOCK + tid] = 0.0f;
+        by[k * BLOCK + tid] = 0.0f;
+    }
+    const float period = p.periods[active ? pi : (uint64_t)tile * BLOCK];
+    const float period_dt = p.pdts[d];
+    Cell s;
+    cell_setup<CHOSEN ? FOLD_EXACT : FOLD_REF>(s, period, period_dt);
+    const bool has_pdt = period_dt != 0.0f;
+
+    // Chosen form: the fast bin is exact away from bin edges while
+    // |q| * n_bins < 2^30 (the same bound as the chosen CE / AOV kernels),
+    // checked for the CTA from max|t| and its smallest |P|.
+    bool fast = false;
+    if constexpr (CHOSEN) {
+        double mn = fabs((double)period);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        if ((tid & 31) == 0) warp_min[tid >> 5] = mn;
+        __syncthreads();
+        double pmin = warp_min[0];
+#pragma unroll
+        for (int k = 1; k < BLOCK / 32; k++) pmin = fmin(pmin, warp_min[k]);
+        const double qb = p.tmax / pmin + fabs((double)period_dt) * p.tmax * p.tmax /
+                                              (2.0 * pmin * pmin);
+        fast = qb * (double)nb < 1073741824.0;  // 2^30
+    }
+    const double nd20 = (double)nb * 1048576.0;
+    const uint32_t n_neg = 0u - nb;
+    const uint32_t edge_add = p.edge_d << 12;
+    const uint32_t edge_lim = (2u * p.edge_d) << 12;
+
+    for (uint32_t base = 0; base < n; base += kFpwTile) {
+        const uint32_t cnt = min(kFpwTile, n - base);
+        __syncthreads();
+        for (uint32_t i = tid; i < cnt; i += BLOCK) {
+            st[i] = (TT)p.t[off + base + i];
+            siv[i] = p.iv[off + base + i];
+            sivy[i] = p.ivy[off + base + i];
+        }
+        __syncthreads();
+        if (!active) continue;
+#pragma unroll 4
+        for (uint32_t i = 0; i < cnt; i++) {
+            uint32_t bin;
+            if constexpr (CHOSEN) {
+                const double td = st[i];
+                if (fast) {
+                    const double a = has_pdt ? td - s.c * td * td : td;
+                    const double qh = __dmul_rn(a, s.yhi);
+                    const double r = __dadd_rd(qh, kMagic15);
+                    const double y = __fma_rd(qh, nd20, kMagic15);
+                    const uint32_t ylo = (uint32_t)__double2loint(y);
+                    const uint32_t yhi = (uint32_t)__double2hiint(y);
+                    // floor(q' n_bins) - n_bins floor(q'), biased by 2^31 by
+                    // the magic constant's top mantissa bit.
+                    bin = __funnelshift_r(ylo, yhi, 20) + (uint32_t)__double2loint(r) * n_neg -
+                          0x80000000u;
+                    if (ylo * 4096u + edge_add < edge_lim)
+                        bin = fpw_ref_bin(has_pdt ? fold_exact<true>(td, s)
+                                                  : fold_exact<false>(td, s), p);
+                } else {
+                    bin = fpw_ref_bin(has_pdt ? fold_exact<true>(td, s)
+                                              : fold_exact<false>(td, s), p);
+                }
+            } else {
+                bin = fpw_ref_bin(fold_ref(st[i], s), p);
+            }
+            bv[bin * BLOCK + tid] += siv[i];
+            by[bin * BLOCK + tid] += sivy[i];
+        }
+    }
+    if (!active) return;
+    float acc = 0.0f;
+    for (uint32_t k = 0; k < nb; k++) {
+        const float v = bv[k * BLOCK + tid];
+        if (v > 0.0f) {
+            const float y = by[k * BLOCK + tid];
+            acc += y * y / (2.0f * v);
+        }
+    }
+    p.out[(uint64_t)c * (p.n_per * p.n_pdt) + pi * p.n_pdt + d] = acc;
+}
+
+}  // namespace PF_KNS
+}  // namespace pfk

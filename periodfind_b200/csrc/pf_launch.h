@@ -60,6 +60,33 @@ cudaError_t launch_binaux_cpusem(const float* m, void* aux, const CurveDesc* cur
                                  uint32_t n_curves, uint32_t n_mag, float mag_bin_size,
                                  int block, int cnt16, cudaStream_t s);
 
+// FPW (pf_fpw.cuh): per point t, inverse variance iv = 1 / err^2 and
+// ivy = iv * m, packed per curve at off[c] with len[c] points; out is
+// [curve][period][pdt].  bin_size = 1 / n_bins as the reference rounds it.
+struct FpwParams {
+    const float* t;
+    const float* iv;
+    const float* ivy;
+    const int64_t* off;
+    const uint32_t* len;
+    const float* periods;
+    const float* pdts;
+    uint64_t n_per;
+    uint32_t n_pdt;
+    uint32_t n_bins;
+    float bin_size;
+    float* out;
+    double tmax;      // max |t| over the batch (the chosen form's range guard)
+    uint32_t edge_d;  // bin-edge guard, units of 2^-20 bin (as the CE / AOV bin kernels)
+};
+constexpr uint32_t kFpwMaxBins = 128;
+// exact: the chosen form (fast bins with the reference sequence near bin
+// edges; the same values).
+cudaError_t launch_fpw_cudasem(const FpwParams& p, bool exact, uint64_t n_curves,
+                               cudaStream_t s);
+cudaError_t launch_fpw_cpusem(const FpwParams& p, bool exact, uint64_t n_curves,
+                              cudaStream_t s);
+
 // Folded phase of every (period, time) pair with one fold variant
 // (FOLD_REF / FOLD_EXACT / FOLD_F32 / FOLD_DF), out[p * n + i].
 cudaError_t launch_phase_probe_cudasem(int fold, const float* t, uint64_t n,

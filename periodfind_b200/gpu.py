@@ -402,6 +402,104 @@ class LombScargle(_Periodogram):
                 np.where(valid, pw, np.float32(0.0)).astype(np.float32))
 
 
+class FPW(_Periodogram):
+    """Fast phase-folding weighted (FPW) periodogram (Finkbeiner et al.
+    2025), maximum is best (periodfind/fpw.pyx:29-177; the CPU class
+    periodfind/cpu/__init__.py:400-521, whose 'peaks' output it also has).
+
+    Per point an inverse variance 1 / err^2 weights the magnitude; per
+    phase bin V = sum of weights, Y = sum of weighted magnitudes; the value
+    is sum over non-empty bins of Y^2 / (2 V).  `errs` None means unit
+    uncertainties; `normalize` and `center` are accepted and unused, as in
+    the reference.
+    """
+
+    _use_max = True
+
+    def __init__(self, n_bins=10, *, mode="chosen", semantics="cuda", device=0):
+        super().__init__(mode=mode, semantics=semantics, device=device)
+        self.n_bins = int(n_bins)
+
+    @staticmethod
+    def _check_errs(times, errs):
+        # periodfind/cpu/__init__.py:466-481.
+        if errs is None:
+            return None
+        ensure_float32(errs, "errs")
+        if len(errs) != len(times):
+            raise ValueError(
+                f"errs must have the same number of arrays as times, "
+                f"got {len(errs)} and {len(times)}")
+        for i, (e, t) in enumerate(zip(errs, times)):
+            if len(e) != len(t):
+                raise ValueError(
+                    f"errs[{i}] and times[{i}] have different lengths: {len(e)} vs {len(t)}")
+        return errs
+
+    def _call(self, ctx, fn, times, mags, errs, periods, pdts, *tail):
+        b = nat.CurveBatch(times, mags)
+        eptr, keep = (None, None) if errs is None else nat.host_pointers(errs, b.lengths)
+        tptr, mptr, lens, n = b.args()
+        rc = fn(ctx.handle, tptr, mptr, None if eptr is None else eptr.ctypes.data, lens, n,
+                nat.ptr(periods), len(periods), nat.ptr(pdts), len(pdts), self.n_bins, *tail)
+        del keep
+        return rc
+
+    def periodograms(self, times, mags, periods, period_dts, errs=None):
+        """Raw [n_curves, n_periods, n_pdts] float32 array."""
+        ctx = nat.default_context(self.device)
+        out = np.empty((len(times), len(periods), len(period_dts)), dtype=np.float32)
+        with ctx.lock:
+            ctx.check(self._call(ctx, ctx.lib.pf_fpw, times, mags, errs, periods, period_dts,
+                                 self._flags, nat.ptr(out)))
+        return out
+
+    def peaks(self, times, mags, periods, period_dts, n_peaks=N_PEAKS_DEFAULT,
+              min_distance=MIN_DISTANCE_DEFAULT, errs=None):
+        """(indices int64 [n_curves, n_peaks] with -1 padding, values float32)."""
+        ctx = nat.default_context(self.device)
+        n_peaks = int(n_peaks)
+        if n_peaks < 0:
+            raise ValueError("n_peaks must be >= 0")
+        idx = np.full((len(times), n_peaks), -1, dtype=np.int64)
+        val = np.zeros((len(times), n_peaks), dtype=np.float32)
+        with ctx.lock:
+            ctx.check(self._call(ctx, ctx.lib.pf_fpw_peaks, times, mags, errs, periods,
+                                 period_dts, n_peaks, int(min_distance), self._flags,
+                                 nat.ptr(idx), nat.ptr(val)))
+        return idx, val
+
+    def calc(self, times, mags, periods, period_dts, errs=None, output="stats",
+             normalize=False, center=False, n_stats=1, significance_type="stdmean",
+             n_peaks=N_PEAKS_DEFAULT, min_distance=MIN_DISTANCE_DEFAULT):
+        """Compute the FPW periodogram of every light curve.
+
+        Returns a list of Statistics (output='stats'; lists of them when
+        n_stats > 1), a list of Periodogram (output='periodogram'), or a list
+        of lists of Statistics for the top peaks (output='peaks').
+        """
+        if output not in _OUTPUTS:
+            raise NotImplementedError(
+                f'Output type "{output}" is not implemented. '
+                f'Use "stats", "periodogram", or "peaks".')
+        validate_inputs(times, mags)
+        ensure_float32(times, "times")
+        ensure_float32(mags, "mags")
+        errs = self._check_errs(times, errs)
+        periods = _grid(periods, "periods")
+        period_dts = _grid(period_dts, "period_dts")
+        if output == "peaks":
+            idx, val = self.peaks(times, mags, periods, period_dts, n_peaks, min_distance, errs)
+            return unravel_peaks(idx, val, periods, period_dts, int(n_peaks))
+        data = self.periodograms(times, mags, periods, period_dts, errs)
+        with gc_paused():
+            if output == "stats":
+                return [Statistics.statistics_from_data(
+                    data[i], [periods, period_dts], True, n=n_stats,
+                    significance_type=significance_type) for i in range(len(times))]
+            return [Periodogram(d, [periods, period_dts], True) for d in data]
+
+
 def find_top_peaks_batched(data, n_peaks, min_distance, use_max, device=0):
     """Top peaks of precomputed periodograms [n_curves, n_periods, n_pdts]
     (rust/src/lib.rs:508-548), computed on the GPU."""

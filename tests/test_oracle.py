@@ -125,3 +125,62 @@ def test_batched_equals_per_curve(oracle):
     for i in range(3):
         one = oracle.ce([ts[i]], [ms[i]], periods, pdts)
         np.testing.assert_array_equal(allb[i], one[0])
+
+
+def _fpw_numpy(t, m, e, periods, pdts, n_bins):
+    """FPW from numpy: the fold and the f32 bin rule of rust/src/fpw.rs:41-44,
+    the bin sums and the statistic in float64 (fpw.rs:46-63)."""
+    t64 = t.astype(np.float64)
+    w = (1.0 / (e.astype(np.float64) ** 2)) if e is not None else np.ones(len(t))
+    out = np.zeros((len(periods), len(pdts)))
+    for pi, P in enumerate(periods):
+        for di, dt in enumerate(pdts):
+            corr = np.float32(np.float32(dt) / np.float32(P)) / np.float32(2.0)
+            r = (t64 - np.float64(corr) * t64 * t64) / np.float64(P)
+            phase = np.abs(r - np.floor(r)).astype(np.float32)
+            b = np.minimum((phase * np.float32(n_bins)).astype(np.int64), n_bins - 1)
+            V = np.bincount(b, weights=w, minlength=n_bins)
+            Y = np.bincount(b, weights=w * m.astype(np.float64), minlength=n_bins)
+            ok = V > 0
+            out[pi, di] = np.sum(Y[ok] ** 2 / (2 * V[ok]))
+    return out
+
+
+def test_fpw_matches_numpy_restatement(oracle):
+    """The oracle's FPW (f32 sums in point order, as rust/src/fpw.rs) is within
+    f32 rounding of the same statistic summed in float64."""
+    rng = np.random.default_rng(3)
+    t = lc.uniform_times(rng, 700, 300.0)
+    m = lc.noisy(rng, lc.sinusoid(t, 3.7, amp=0.4, offset=15.0), 0.05)
+    e = rng.uniform(0.02, 0.2, 700).astype(np.float32)
+    P = lc.trial_periods(3.7, n=60)
+    D = np.array([0.0, 1e-4], np.float32)
+    for errs, nb in ((None, 10), ([e], 20), ([e], 7)):
+        got = oracle.fpw([t], [m], P, D, nb, errs=errs)[0]
+        want = _fpw_numpy(t, m, None if errs is None else e, P, D, nb)
+        np.testing.assert_allclose(got, want, rtol=2e-5)
+
+
+@pytest.mark.parametrize("case", [
+    dict(period=5.0, n=800, noise=0.02, span=200.0, n_bins=20, errs=None),
+    dict(period=3.0, n=600, noise=0.05, span=150.0, n_bins=15, errs="const"),
+    dict(period=2.0, n=500, noise=0.03, span=100.0, n_bins=10, errs=None),
+    dict(period=4.0, n=800, noise=None, span=200.0, n_bins=15, errs="var"),
+])
+def test_fpw_known_period(oracle, case):
+    """Known-answer cases of the reference's CPU FPW tests
+    (tests/test_cpu_standalone.py:412-465 and the variable-uncertainty case
+    after it): the best period is the injected one to 5%."""
+    rng = np.random.default_rng(42)
+    t = lc.uniform_times(rng, case["n"], case["span"])
+    if case["errs"] == "var":
+        e = rng.uniform(0.01, 0.2, case["n"]).astype(np.float32)
+        m = (lc.sinusoid(t, case["period"]) + rng.normal(0, 1, case["n"]) * e).astype(np.float32)
+    else:
+        m = lc.noisy(rng, lc.sinusoid(t, case["period"]), case["noise"])
+        e = np.full(case["n"], 0.05, np.float32) if case["errs"] == "const" else None
+    P = lc.trial_periods(case["period"], n=500)
+    pg = oracle.fpw([t], [m], P, np.zeros(1, np.float32), case["n_bins"],
+                    errs=None if e is None else [e])[0, :, 0]
+    best = P[int(np.argmax(pg))]
+    assert abs(best - case["period"]) / case["period"] < 0.05, best
