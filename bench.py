@@ -498,6 +498,54 @@ def fpw_arm(args):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------- device-resident I/O
+
+
+def device_arm(args):
+    """CE(10x10) and AOV(15) periodograms of the benchmark batch (1000 curves x
+    4096 points x 10000 periods x 2 pdts) from curves already on the GPU,
+    left on the GPU (periodograms_device: magnitude preparation on the
+    device, no host copy), against the public host path
+    calc(output='periodogram') from numpy lists, which returns the 80 MB
+    periodogram per algorithm to the host.  Wall time per step, synchronised."""
+    import torch
+
+    from periodfind_b200 import gpu
+
+    torch.cuda.set_device(0)
+    ts, ms, periods, pdts = make_workload(args.curves)
+    off = np.zeros(len(ts) + 1, np.int64)
+    np.cumsum([len(t) for t in ts], out=off[1:])
+    d_t = torch.from_numpy(np.concatenate(ts)).cuda()
+    d_m = torch.from_numpy(np.concatenate(ms)).cuda()
+    evals = 2 * int(off[-1]) * len(periods) * len(pdts)
+    ce, aov = gpu.ConditionalEntropy(10, 10), gpu.AOV(15)
+
+    def dev_step():
+        a = ce.periodograms_device(d_t, d_m, off, periods, pdts)
+        b = aov.periodograms_device(d_t, d_m, off, periods, pdts)
+        torch.cuda.synchronize()
+        return a, b
+
+    def host_step():
+        return (ce.calc(ts, ms, periods, pdts, output="periodogram"),
+                aov.calc(ts, ms, periods, pdts, output="periodogram"))
+
+    out = {"workload": f"CE(10x10) + AOV(15) periodograms, {len(ts)} curves x {N_POINTS} pts x "
+                       f"{N_PERIODS} periods x {len(PDTS)} pdts", "evals": evals}
+    for name, fn in (("device_resident", dev_step), ("host_calc_periodogram", host_step)):
+        for _ in range(2):
+            fn()
+        w = []
+        for _ in range(max(3, args.steps)):
+            t0 = time.perf_counter()
+            fn()
+            w.append(time.perf_counter() - t0)
+        ms_ = float(np.median(w)) * 1e3
+        out[name] = {"ms": ms_, "evals_per_s": evals / (ms_ * 1e-3)}
+    print(json.dumps(out), flush=True)
+
+
 # ------------------------------------------------------ small CE batch
 
 
@@ -758,18 +806,19 @@ def main():
     ap.add_argument("--curves", type=int, default=N_CURVES)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "small", "ragged", "lsgrad", "precision", "fpw"],
+                    choices=["batch", "small", "ragged", "lsgrad", "precision", "fpw", "device"],
                     help="'small': CE stats on 100 x 1024; 'ragged': the mixed ragged batch; "
                          "'lsgrad': LS derivatives and "
                          "Newton refinement; 'precision': LS folds on the precision-study "
-                         "batch; 'fpw': FPW on the benchmark batch (separate reports, 1 GPU)")
+                         "batch; 'fpw': FPW on the benchmark batch; 'device': periodograms of "
+                         "device-resident curves left on the GPU (separate reports, 1 GPU)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
         return
     if args.workload != "batch":
         {"small": small_arm, "ragged": ragged_arm, "lsgrad": lsgrad_arm,
-         "precision": precision_arm, "fpw": fpw_arm}[args.workload](args)
+         "precision": precision_arm, "fpw": fpw_arm, "device": device_arm}[args.workload](args)
         return
 
     import torch

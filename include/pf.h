@@ -184,6 +184,21 @@ int pf_fpw_peaks(pf_ctx* ctx, const float* const* times, const float* const* mag
                  uint32_t n_bins, uint32_t n_peaks, uint32_t min_distance, int mode,
                  int64_t* out_idx, float* out_val);
 
+/* Magnitude preparation on the device for device-resident curves (curve c
+ * is d_mags[offsets[c] .. offsets[c+1]), offsets on the host), with the
+ * values the reference's prepare_magnitudes gets from numpy on the host
+ * (periodfind/_utils.py:29-45), bit for bit: PF_PREP_CENTER writes
+ * m - np.mean(m) (numpy's pairwise float32 sum), PF_PREP_NORMALIZE writes
+ * ((m - min) / (max - min)) * 0.999 + 5e-4 in float32 (NaN propagating).
+ * d_out may equal d_mags.  Enqueued on `stream` (NULL: the default stream);
+ * a later call on this context waits for this one's kernel before it
+ * rewrites the context's copy of the offsets.  No reference counterpart:
+ * the reference prepares magnitudes with numpy on the host. */
+#define PF_PREP_CENTER 1
+#define PF_PREP_NORMALIZE 2
+int pf_prepare_mags_dev(pf_ctx* ctx, const float* d_mags, const int64_t* offsets,
+                        uint64_t n_curves, int kind, float* d_out, void* stream);
+
 /* Collect the oldest pending PF_ASYNC peak call on this context: wait for
  * its work, then write its peaks into the out_idx / out_val it was given.
  * Calls are collected in the order they were made.  PF_EINVAL when none is

@@ -32,6 +32,7 @@ PF_TIMING = 0x1000
 PF_REF_STATS = 0x2000
 PF_NO_TUNE = 0x4000
 PF_ASYNC = 0x8000
+PF_PREP_CENTER, PF_PREP_NORMALIZE = 1, 2
 PF_ALGO_CE, PF_ALGO_AOV, PF_ALGO_LS = 0, 1, 2
 
 _vp = ctypes.c_void_p
@@ -56,6 +57,7 @@ SIGNATURES = {
     "pf_ls_peaks": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int, _vp,
                      _vp], _int),
     "pf_wait": ([_vp], _int),
+    "pf_prepare_mags_dev": ([_vp, _vp, _vp, _u64, _int, _vp, _vp], _int),
     "pf_fpw": ([_vp, _vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _int, _vp], _int),
     "pf_fpw_peaks": ([_vp, _vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32,
                       _int, _vp, _vp], _int),

@@ -61,6 +61,12 @@ struct pf_ctx {
     bool staged_pending = false, done_recorded = false, timed_pending = false;
     std::string err;
     DevBuf d_in, d_aux32, d_aux64, d_out, d_pidx, d_pval, d_pack, d_misc, d_stamps, d_stat;
+    // pf_prepare_mags_dev: the curve offsets on the device, and the event
+    // after the last kernel that read them (the buffer is rewritten only
+    // once that kernel is done).
+    DevBuf d_prep;
+    cudaEvent_t ev_prep = nullptr;
+    bool prep_pending = false;
     // PF_TIMING: the curve of each work item of the last timed launch, and
     // the stream it ran on.
     std::vector<uint32_t> stamp_curves;   // curve of each stamped work item
@@ -1195,7 +1201,8 @@ int pf_ctx_create(pf_ctx** out, int device) {
         (e = cudaEventCreateWithFlags(&ctx->pend[0].done, cudaEventDisableTiming)) !=
             cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->pend[1].done, cudaEventDisableTiming)) !=
-            cudaSuccess) {
+            cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_prep, cudaEventDisableTiming)) != cudaSuccess) {
         g_create_error = cudaGetErrorString(e);
         pf_ctx_destroy(ctx);
         return PF_ECUDA;
@@ -1209,14 +1216,17 @@ void pf_ctx_destroy(pf_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->done_recorded) cudaEventSynchronize(ctx->ev_done);
+    if (ctx->prep_pending) cudaEventSynchronize(ctx->ev_prep);
     for (DevBuf* b : {&ctx->d_in, &ctx->d_aux32, &ctx->d_aux64, &ctx->d_out, &ctx->d_pidx,
-                      &ctx->d_pval, &ctx->d_pack, &ctx->d_misc, &ctx->d_stamps, &ctx->d_stat})
+                      &ctx->d_pval, &ctx->d_pack, &ctx->d_misc, &ctx->d_stamps, &ctx->d_stat,
+                      &ctx->d_prep})
         if (b->p) cudaFree(b->p);
     if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
     for (pf_ctx::Pending& q : ctx->pend) {
         if (q.res.p) cudaFreeHost(q.res.p);
         if (q.done) cudaEventDestroy(q.done);
     }
+    if (ctx->ev_prep) cudaEventDestroy(ctx->ev_prep);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->ev_staged) cudaEventDestroy(ctx->ev_staged);
@@ -1613,6 +1623,48 @@ int pf_fpw_peaks(pf_ctx* ctx, const float* const* times, const float* const* mag
                  int64_t* out_idx, float* out_val) {
     return run_fpw(ctx, times, mags, errs, lengths, n_curves, periods, n_per, period_dts, n_pdt,
                    n_bins, mode, nullptr, true, n_peaks, min_distance, out_idx, out_val);
+}
+
+int pf_prepare_mags_dev(pf_ctx* ctx, const float* d_mags, const int64_t* offsets,
+                        uint64_t n_curves, int kind, float* d_out, void* stream) {
+    if (!ctx) return PF_EINVAL;
+    if (kind != PF_PREP_CENTER && kind != PF_PREP_NORMALIZE)
+        return fail(ctx, PF_EINVAL, "kind must be PF_PREP_CENTER or PF_PREP_NORMALIZE");
+    if (n_curves == 0) return PF_OK;
+    if (!offsets) return fail(ctx, PF_EINVAL, "offsets is NULL");
+    if (n_curves > 0x7FFFFFFFull) return fail(ctx, PF_EINVAL, "too many curves");
+    if (offsets[0] < 0) return fail(ctx, PF_EINVAL, "offsets[0] is negative");
+    uint32_t leaf_cap = 1;
+    for (uint64_t c = 0; c < n_curves; c++) {
+        const int64_t len = offsets[c + 1] - offsets[c];
+        if (len < 0 || len > 0xFFFFFFFFll)
+            return fail(ctx, PF_EINVAL, "offsets must be non-decreasing (curve %llu)",
+                        (unsigned long long)c);
+        if (kind == PF_PREP_CENTER && len > 0)
+            leaf_cap = std::max(leaf_cap, stats_leaf_count((uint32_t)len));
+    }
+    if ((size_t)leaf_cap * 12 > 200u * 1024u)
+        return fail(ctx, PF_EUNSUPPORTED, "a curve is too long for the device mean");
+    if (offsets[n_curves] > offsets[0] && (!d_mags || !d_out))
+        return fail(ctx, PF_EINVAL, "d_mags / d_out is NULL");
+    PF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (ctx->prep_pending) {
+        PF_CUDA(cudaEventSynchronize(ctx->ev_prep), "previous preparation");
+        ctx->prep_pending = false;
+    }
+    int rc;
+    if ((rc = ensure_dev(ctx, ctx->d_prep, (n_curves + 1) * 8)) != PF_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    PF_CUDA(cudaMemcpyAsync(ctx->d_prep.p, offsets, (n_curves + 1) * 8, cudaMemcpyHostToDevice,
+                            s),
+            "H2D offsets");
+    PF_CUDA(launch_prep_mags(d_mags, (const int64_t*)ctx->d_prep.p, n_curves, leaf_cap, kind,
+                             d_out, s),
+            "magnitude preparation launch");
+    PF_CUDA(cudaEventRecord(ctx->ev_prep, s), "event");
+    ctx->prep_pending = true;
+    ctx->launches++;
+    return PF_OK;
 }
 
 int pf_wait(pf_ctx* ctx) {

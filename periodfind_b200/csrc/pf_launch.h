@@ -155,6 +155,11 @@ cudaError_t launch_ls_grad(const LsGradParams& p, uint32_t max_len, cudaStream_t
 // leaves of numpy's pairwise summation over n elements (12 B of shared
 // memory each).
 uint32_t stats_leaf_count(uint32_t n);
+// Magnitude preparation on the device (kind 1: centre, 2: normalise) as
+// numpy does it; curve c is m[d_off[c] .. d_off[c+1]); leaf_cap is the
+// largest stats_leaf_count over the curves (kind 1).
+cudaError_t launch_prep_mags(const float* m, const int64_t* d_off, uint64_t n_curves,
+                             uint32_t leaf_cap, int kind, float* out, cudaStream_t s);
 cudaError_t launch_stats(const float* pg, uint64_t n_curves, uint32_t n_cells, int use_max,
                          uint32_t n_top, float* stats, int64_t* top_idx, float* top_val,
                          cudaStream_t stream);

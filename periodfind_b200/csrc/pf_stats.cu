@@ -278,6 +278,74 @@ __global__ void __launch_bounds__(kStatThreads)
     }
 }
 
+// Magnitude preparation on the device, a CTA per curve, with the values
+// the reference's prepare_magnitudes gets from numpy (periodfind/_utils.py:
+// 29-45): kind 1 centres, m - np.mean(m) (numpy's pairwise float32 sum
+// divided by n); kind 2 normalises, ((m - min) / (max - min)) * 0.999 +
+// 5e-4 in float32 with NaN propagating through min / max.  Curve c is
+// m[off[c] .. off[c+1]); its output goes to the same place in out.
+__global__ void __launch_bounds__(kStatThreads)
+    prep_mags_kernel(const float* __restrict__ m, const int64_t* __restrict__ off, int kind,
+                     uint32_t leaf_cap, float* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char psm[];
+    __shared__ uint32_t s_leaves;
+    __shared__ float s_lo[kStatThreads / 32], s_hi[kStatThreads / 32];
+    __shared__ int s_nan;
+    const uint64_t c = blockIdx.x;
+    const int64_t lo = off[c];
+    const uint32_t n = (uint32_t)(off[c + 1] - lo);
+    if (n == 0) return;  // uniform over the CTA
+    const float* x = m + lo;
+    float* y = out + lo;
+    if (kind == 1) {
+        // leaf arrays for leaf_cap leaves: the host's maximum over the curves
+        uint32_t* leaf_lo = reinterpret_cast<uint32_t*>(psm);
+        uint32_t* leaf_len = leaf_lo + leaf_cap;
+        float* leaf = reinterpret_cast<float*>(leaf_len + leaf_cap);
+        if (threadIdx.x == 0) {
+            uint32_t count = 0;
+            list_leaves(0, n, leaf_lo, leaf_len, count);
+            s_leaves = count;
+        }
+        __syncthreads();
+        const float sum = pairwise_row(x, n, T_X, 0.0f, s_leaves, leaf_lo, leaf_len, leaf);
+        const float mean = __fdiv_rn(sum, (float)n);
+        for (uint32_t i = threadIdx.x; i < n; i += kStatThreads) y[i] = __fsub_rn(x[i], mean);
+        return;
+    }
+    // np.min / np.max: exact, any order; NaN anywhere gives NaN.
+    float mn = INFINITY, mx = -INFINITY;
+    int nan_local = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += kStatThreads) {
+        const float v = x[i];
+        nan_local |= isnan(v) ? 1 : 0;
+        mn = fminf(mn, v);
+        mx = fmaxf(mx, v);
+    }
+    if (threadIdx.x == 0) s_nan = 0;
+    __syncthreads();
+    if (nan_local) atomicOr(&s_nan, 1);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_lo[threadIdx.x >> 5] = mn;
+        s_hi[threadIdx.x >> 5] = mx;
+    }
+    __syncthreads();
+    float cmin = s_lo[0], cmax = s_hi[0];
+    for (int w = 1; w < kStatThreads / 32; w++) {
+        cmin = fminf(cmin, s_lo[w]);
+        cmax = fmaxf(cmax, s_hi[w]);
+    }
+    if (s_nan) cmin = cmax = __uint_as_float(0x7FC00000u);
+    const float range = __fsub_rn(cmax, cmin);
+    for (uint32_t i = threadIdx.x; i < n; i += kStatThreads)
+        y[i] = __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(x[i], cmin), range), 0.999f), 5e-4f);
+}
+
 }  // namespace
 
 uint32_t stats_leaf_count(uint32_t n) {
@@ -312,6 +380,22 @@ cudaError_t launch_stats(const float* pg, uint64_t n_curves, uint32_t n_cells, i
     if (e != cudaSuccess) return e;
     stats_kernel<<<(unsigned)n_curves, kStatThreads, smem, s>>>(pg, n_cells, use_max, n_top,
                                                                 leaves, stats, top_idx, top_val);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prep_mags(const float* m, const int64_t* d_off, uint64_t n_curves,
+                             uint32_t leaf_cap, int kind, float* out, cudaStream_t s) {
+    if (n_curves == 0) return cudaSuccess;
+    if (kind != 1 && kind != 2) return cudaErrorInvalidValue;
+    if (n_curves > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+    const uint32_t leaves = leaf_cap ? leaf_cap : 1;
+    const size_t smem = (size_t)leaves * 12;
+    if (smem > 200u * 1024u) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(prep_mags_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    prep_mags_kernel<<<(unsigned)n_curves, kStatThreads, smem, s>>>(m, d_off, kind, leaves,
+                                                                     out);
     return cudaGetLastError();
 }
 

@@ -108,6 +108,65 @@ class _Periodogram:
             ctx.check(self._native_pgram(ctx, b, periods, period_dts, out))
         return out
 
+    def periodograms_device(self, t, m, offsets, periods, period_dts, normalize=None,
+                            center=None):
+        """Periodograms of curves already on the GPU, left on the GPU.
+
+        t, m: contiguous 1-D float32 CUDA tensors on this object's device
+        holding the curves back to back (curve c is [offsets[c],
+        offsets[c+1])); offsets: n_curves + 1 int64 values (host).  The
+        magnitudes are prepared on the device as calc() prepares them (CE
+        normalises, LS centres; `normalize` / `center` override), with
+        numpy's values bit for bit.  Returns a float32 CUDA tensor [n_curves,
+        n_periods, n_pdts] on the current stream (DLPack through torch).  No
+        counterpart in the reference, whose results always come back to the
+        host."""
+        import torch
+
+        if normalize is None:
+            normalize = self._normalize_default
+        if center is None:
+            center = self._center_default
+        if center and normalize:  # the reference's conflict warning, then centre
+            prepare_magnitudes([], center, normalize)
+            normalize = False
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        if off.ndim != 1 or len(off) < 1:
+            raise ValueError("offsets must be a 1-D array of n_curves + 1 values")
+        n = len(off) - 1
+        for name, a in (("t", t), ("m", m)):
+            if not (torch.is_tensor(a) and a.is_cuda and a.dtype == torch.float32
+                    and a.dim() == 1 and a.is_contiguous()):
+                raise TypeError(f"{name} must be a contiguous 1-D float32 CUDA tensor")
+            if a.device.index != self.device:
+                raise ValueError(f"{name} is on cuda:{a.device.index}, not cuda:{self.device}")
+        if t.numel() != m.numel() or off[0] < 0 or off[-1] > t.numel() or np.any(np.diff(off) < 0):
+            raise ValueError("offsets must be non-decreasing and within the tensors")
+        periods = _grid(periods, "periods")
+        period_dts = _grid(period_dts, "period_dts")
+        dev = t.device
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        out = torch.empty((n, len(periods), len(period_dts)), dtype=torch.float32, device=dev)
+        if n == 0:
+            return out
+        kind = nat.PF_PREP_CENTER if center else (nat.PF_PREP_NORMALIZE if normalize else 0)
+        ctx = nat.default_context(self.device)
+        d_p = torch.from_numpy(periods).to(dev)
+        d_d = torch.from_numpy(period_dts).to(dev)
+        mp = m
+        with ctx.lock:
+            if kind:
+                mp = torch.empty_like(m)
+                ctx.check(ctx.lib.pf_prepare_mags_dev(ctx.handle, m.data_ptr(), off.ctypes.data,
+                                                      n, kind, mp.data_ptr(), stream))
+            ctx.check(self._native_dev(ctx, t.data_ptr(), mp.data_ptr(), off, n,
+                                       d_p.data_ptr(), len(periods), d_d.data_ptr(),
+                                       len(period_dts), out.data_ptr(), stream))
+        return out
+
+    def _native_dev(self, ctx, d_t, d_m, off, n, d_p, n_per, d_d, n_pdt, d_out, stream):
+        raise NotImplementedError
+
     def peaks(self, times, mags, periods, period_dts, n_peaks=N_PEAKS_DEFAULT,
               min_distance=MIN_DISTANCE_DEFAULT):
         """(indices int64 [n_curves, n_peaks] with -1 padding, values float32)."""
@@ -287,6 +346,11 @@ class ConditionalEntropy(_Periodogram):
                                    self.phase_bin_extent, self.mag_bin_extent, n_top,
                                    self._flags, nat.ptr(st), nat.ptr(idx), nat.ptr(val))
 
+    def _native_dev(self, ctx, d_t, d_m, off, n, d_p, n_per, d_d, n_pdt, d_out, stream):
+        return ctx.lib.pf_ce_dev(ctx.handle, d_t, d_m, off.ctypes.data, n, d_p, n_per, d_d,
+                                 n_pdt, self.n_phase, self.n_mag, self.phase_bin_extent,
+                                 self.mag_bin_extent, self._flags, d_out, stream)
+
     def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val, extra=0):
         return ctx.lib.pf_ce_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                                    nat.ptr(pdts), len(pdts), self.n_phase, self.n_mag,
@@ -319,6 +383,11 @@ class AOV(_Periodogram):
                                     self.phase_bin_extent, n_top, self._flags, nat.ptr(st),
                                     nat.ptr(idx), nat.ptr(val))
 
+    def _native_dev(self, ctx, d_t, d_m, off, n, d_p, n_per, d_d, n_pdt, d_out, stream):
+        return ctx.lib.pf_aov_dev(ctx.handle, d_t, d_m, off.ctypes.data, n, d_p, n_per, d_d,
+                                  n_pdt, self.n_phase, self.phase_bin_extent, self._flags,
+                                  d_out, stream)
+
     def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val, extra=0):
         return ctx.lib.pf_aov_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                                     nat.ptr(pdts), len(pdts), self.n_phase,
@@ -350,6 +419,10 @@ class LombScargle(_Periodogram):
         return ctx.lib.pf_ls_stats(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                                    nat.ptr(pdts), len(pdts), n_top, self._flags, nat.ptr(st),
                                    nat.ptr(idx), nat.ptr(val))
+
+    def _native_dev(self, ctx, d_t, d_m, off, n, d_p, n_per, d_d, n_pdt, d_out, stream):
+        return ctx.lib.pf_ls_dev(ctx.handle, d_t, d_m, off.ctypes.data, n, d_p, n_per, d_d,
+                                 n_pdt, self._flags, d_out, stream)
 
     def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val, extra=0):
         return ctx.lib.pf_ls_peaks(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
