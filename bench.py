@@ -449,25 +449,27 @@ def ragged_arm(args):
 # ------------------------------------------------------------------ FPW
 
 
-def fpw_arm(args):
-    """FPW(10) over the benchmark batch (1000 curves x 4096 points, 10000 log
-    periods in [0.1, 100] d x pdts [0, 1e-6]) with per-point uncertainties
-    U[0.02, 0.1]: device time of the chosen and plain forms (the FPW kernel,
-    CUDA events), end-to-end calc(output='peaks') from numpy lists, and the
-    oracle (the Rust path's restatement) on all host cores over a sample."""
+def fpw_arm(args, bls=False):
+    """FPW(10) -- or, with bls, BoxLeastSquares(50, 0.01, 0.5) -- over the
+    benchmark batch (1000 curves x 4096 points, 10000 log periods in
+    [0.1, 100] d x pdts [0, 1e-6]) with per-point uncertainties U[0.02, 0.1]:
+    device time of the chosen and plain forms (the kernel, CUDA events),
+    end-to-end calc(output='peaks') from numpy lists, and the oracle (the
+    Rust path's restatement) on all host cores over a sample."""
     from periodfind_b200 import gpu
 
     ts, ms, periods, pdts = make_workload(args.curves)
     rng = np.random.default_rng(SEED + 6)
     es = [rng.uniform(0.02, 0.1, len(t)).astype(np.float32) for t in ts]
     evals = sum(len(t) for t in ts) * len(periods) * len(pdts)
-    out = {"workload": f"FPW(10), {len(ts)} curves x {N_POINTS} pts, {N_PERIODS} log periods "
+    label = "BLS(50, qmin 0.01, qmax 0.5)" if bls else "FPW(10)"
+    out = {"workload": f"{label}, {len(ts)} curves x {N_POINTS} pts, {N_PERIODS} log periods "
                        f"[0.1,100] d x pdts {list(PDTS)}, errs U[0.02,0.1]", "evals": evals}
     from periodfind_b200 import _native as nat
 
     ctx = nat.default_context(0)
     for mode in ("chosen", "plain"):
-        obj = gpu.FPW(10, mode=mode)
+        obj = gpu.BoxLeastSquares(50, 0.01, 0.5, mode=mode) if bls else gpu.FPW(10, mode=mode)
         obj.periodograms(ts, ms, periods, pdts, errs=es)
         k = []
         for _ in range(max(1, args.steps)):
@@ -490,7 +492,10 @@ def fpw_arm(args):
         cores = os.cpu_count() or 1
         k = 20
         t0 = time.perf_counter()
-        O.fpw(ts[:k], ms[:k], periods, pdts, 10, errs=es[:k], n_threads=cores)
+        if bls:
+            O.bls(ts[:k], ms[:k], periods, pdts, 50, 0.01, 0.5, errs=es[:k], n_threads=cores)
+        else:
+            O.fpw(ts[:k], ms[:k], periods, pdts, 10, errs=es[:k], n_threads=cores)
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": k * N_POINTS * N_PERIODS * len(PDTS) / dt,
                                "unit": "evals/s", "cores": cores, "kind": "port",
@@ -806,11 +811,13 @@ def main():
     ap.add_argument("--curves", type=int, default=N_CURVES)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "small", "ragged", "lsgrad", "precision", "fpw", "device"],
+                    choices=["batch", "small", "ragged", "lsgrad", "precision", "fpw", "bls",
+                             "device"],
                     help="'small': CE stats on 100 x 1024; 'ragged': the mixed ragged batch; "
                          "'lsgrad': LS derivatives and "
                          "Newton refinement; 'precision': LS folds on the precision-study "
-                         "batch; 'fpw': FPW on the benchmark batch; 'device': periodograms of "
+                         "batch; 'fpw' / 'bls': FPW / BLS on the benchmark batch; 'device': "
+                         "periodograms of "
                          "device-resident curves left on the GPU (separate reports, 1 GPU)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -818,7 +825,8 @@ def main():
         return
     if args.workload != "batch":
         {"small": small_arm, "ragged": ragged_arm, "lsgrad": lsgrad_arm,
-         "precision": precision_arm, "fpw": fpw_arm, "device": device_arm}[args.workload](args)
+         "precision": precision_arm, "fpw": fpw_arm, "bls": lambda a: fpw_arm(a, bls=True),
+         "device": device_arm}[args.workload](args)
         return
 
     import torch

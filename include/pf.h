@@ -184,6 +184,26 @@ int pf_fpw_peaks(pf_ctx* ctx, const float* const* times, const float* const* mag
                  uint32_t n_bins, uint32_t n_peaks, uint32_t min_distance, int mode,
                  int64_t* out_idx, float* out_val);
 
+/* BLS, box least squares (Kovacs, Zucker & Mazeh 2002).  Replaces
+ * BLS::CalcBLSBatched (periodfind/cuda/bls.h, bls.cu; bound at
+ * periodfind/bls.pyx:20-33) and calc_bls_batched / calc_bls_peaks_batched
+ * (rust/src/lib.rs:264-322, 718-760).  Per point w = 1 / err^2 (errs NULL:
+ * err = 1) and w * (m - mean), mean = sum(w m) / sum(w) in sequential f32
+ * sums; per phase bin W and Y; the value is the best s^2 / (r (W_total - r))
+ * over windows of nb_min .. nb_max consecutive bins (wrapping; nb_min =
+ * max(floor(qmin n_bins), 1), nb_max = min(ceil(qmax n_bins), n_bins - 1))
+ * whose weight fraction r / W_total lies in (0, 1).  Maximum is best.
+ * n_bins in [1, 128]; modes as pf_fpw. */
+int pf_bls(pf_ctx* ctx, const float* const* times, const float* const* mags,
+           const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
+           const float* periods, uint64_t n_per, const float* period_dts, uint64_t n_pdt,
+           uint32_t n_bins, float qmin, float qmax, int mode, float* out);
+int pf_bls_peaks(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                 const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
+                 const float* periods, uint64_t n_per, const float* period_dts, uint64_t n_pdt,
+                 uint32_t n_bins, float qmin, float qmax, uint32_t n_peaks,
+                 uint32_t min_distance, int mode, int64_t* out_idx, float* out_val);
+
 /* Magnitude preparation on the device for device-resident curves (curve c
  * is d_mags[offsets[c] .. offsets[c+1]), offsets on the host), with the
  * values the reference's prepare_magnitudes gets from numpy on the host

@@ -229,6 +229,106 @@ ORC_API void orc_fpw_batched(const float* times, const float* mags, const float*
     free(ivy);
 }
 
+/* ------------------------------------------------------------------ BLS */
+
+/* rust/src/bls.rs:19-134 for one curve and one (period, pdt): bins of w and
+ * w * (m - mean) (the caller's arrays), prefix sums, and the best
+ * s^2 / (r (W - r)) over windows of nb_min .. nb_max bins, all in f32. */
+static float orc_bls_cell(const float* times, const float* iv, const float* iyw,
+                          uint64_t length, float period, float period_dt, uint32_t num_bins,
+                          uint64_t nb_min, uint64_t nb_max, float* wb, float* yb,
+                          float* wp, float* yp) {
+    const float pdt_corr = orc_pdt_correction(period, period_dt);
+    for (uint32_t k = 0; k < num_bins; k++) wb[k] = yb[k] = 0.0f;
+    for (uint64_t i = 0; i < length; i++) {
+        const float phase = orc_fold_time(times[i], period, pdt_corr, 0);
+        uint64_t bin = sat_u64(phase * (float)num_bins);
+        if (bin > num_bins - 1) bin = num_bins - 1;
+        wb[bin] += iv[i];
+        yb[bin] += iyw[i];
+    }
+    wp[0] = 0.0f;
+    yp[0] = 0.0f;
+    for (uint32_t k = 0; k < num_bins; k++) {
+        wp[k + 1] = wp[k] + wb[k];
+        yp[k + 1] = yp[k] + yb[k];
+    }
+    const float w_total = wp[num_bins];
+    if (w_total <= 0.0f) return 0.0f;
+    float best = 0.0f;
+    for (uint64_t nb = nb_min; nb <= nb_max; nb++) {
+        for (uint64_t phi = 0; phi < num_bins; phi++) {
+            const uint64_t end = phi + nb;
+            float r, s;
+            if (end <= num_bins) {
+                r = wp[end] - wp[phi];
+                s = yp[end] - yp[phi];
+            } else {
+                const uint64_t wrap = end - num_bins;
+                r = (wp[num_bins] - wp[phi]) + wp[wrap];
+                s = (yp[num_bins] - yp[phi]) + yp[wrap];
+            }
+            const float r_frac = r / w_total;
+            if (r_frac > 0.0f && r_frac < 1.0f) {
+                const float v = (s * s) / (r * (w_total - r));
+                if (v > best) best = v;
+            }
+        }
+    }
+    return best;
+}
+
+/* rust/src/lib.rs:264-322 (calc_bls_batched): errs NULL means err = 1. */
+ORC_API void orc_bls_batched(const float* times, const float* mags, const float* errs,
+                             const int64_t* offsets, int64_t n_curves,
+                             const float* periods, int64_t n_per,
+                             const float* pdts, int64_t n_pdt, uint32_t num_bins,
+                             float qmin, float qmax, int n_threads, float* out) {
+    set_threads(n_threads);
+    const int64_t n_pts = n_curves > 0 ? offsets[n_curves] : 0;
+    float* iv = (float*)malloc((size_t)(n_pts > 0 ? n_pts : 1) * sizeof(float));
+    float* iyw = (float*)malloc((size_t)(n_pts > 0 ? n_pts : 1) * sizeof(float));
+    for (int64_t c = 0; c < n_curves; c++) {
+        float total_w = 0.0f, total_wy = 0.0f;
+        for (int64_t i = offsets[c]; i < offsets[c + 1]; i++) {
+            const float e = errs ? errs[i] : 1.0f;
+            iv[i] = 1.0f / (e * e);
+            total_w += iv[i];
+        }
+        for (int64_t i = offsets[c]; i < offsets[c + 1]; i++) total_wy += iv[i] * mags[i];
+        const float mean_y = total_w > 0.0f ? total_wy / total_w : 0.0f;
+        for (int64_t i = offsets[c]; i < offsets[c + 1]; i++) iyw[i] = iv[i] * (mags[i] - mean_y);
+    }
+    /* bls.rs:51-52 with Rust's saturating casts */
+    const uint64_t lo = sat_u64(floorf(qmin * (float)num_bins));
+    const uint64_t hi = sat_u64(ceilf(qmax * (float)num_bins));
+    const uint64_t nb_min = lo > 1 ? lo : 1;
+    const uint64_t nb_max = hi < (uint64_t)num_bins - 1 ? hi : (uint64_t)num_bins - 1;
+    const int64_t per_curve = n_per * n_pdt;
+    const int64_t total = n_curves * per_curve;
+#pragma omp parallel
+    {
+        float* wb = (float*)malloc((size_t)num_bins * sizeof(float));
+        float* yb = (float*)malloc((size_t)num_bins * sizeof(float));
+        float* wp = (float*)malloc((size_t)(num_bins + 1) * sizeof(float));
+        float* yp = (float*)malloc((size_t)(num_bins + 1) * sizeof(float));
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t k = 0; k < total; k++) {
+            int64_t c = k / per_curve, g = k % per_curve;
+            int64_t p = g / n_pdt, d = g % n_pdt;
+            const int64_t o = offsets[c];
+            out[k] = orc_bls_cell(times + o, iv + o, iyw + o, (uint64_t)(offsets[c + 1] - o),
+                                  periods[p], pdts[d], num_bins, nb_min, nb_max, wb, yb, wp, yp);
+        }
+        free(wb);
+        free(yb);
+        free(wp);
+        free(yp);
+    }
+    free(iv);
+    free(iyw);
+}
+
 /* ------------------------------------------------------------------ AOV */
 
 typedef struct {

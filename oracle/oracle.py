@@ -51,6 +51,9 @@ def _load():
     i64, u32, c_int = ctypes.c_int64, ctypes.c_uint32, ctypes.c_int
     lib.orc_ce_batched.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
                                    u32, u32, u32, u32, c_int, c_int, _f32p]
+    lib.orc_bls_batched.argtypes = [_f32p, _f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
+                                    ctypes.c_uint32, ctypes.c_float, ctypes.c_float, c_int,
+                                    _f32p]
     lib.orc_fpw_batched.argtypes = [_f32p, _f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
                                     ctypes.c_uint32, c_int, _f32p]
     lib.orc_aov_batched.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
@@ -133,6 +136,22 @@ def fpw(times, mags, periods, pdts, n_bins=10, errs=None, n_threads=0):
     lib.orc_fpw_batched(_ptr(t, _f32p), _ptr(m, _f32p), None if e is None else _ptr(e, _f32p),
                         _ptr(off, _i64p), len(off) - 1, _ptr(p, _f32p), len(p), _ptr(d, _f32p),
                         len(d), n_bins, n_threads, _ptr(out, _f32p))
+    return out
+
+
+def bls(times, mags, periods, pdts, n_bins=50, qmin=0.01, qmax=0.5, errs=None, n_threads=0):
+    """rust/src/bls.rs:19-134 batched as rust/src/lib.rs:264-322 (errs None:
+    unit uncertainties)."""
+    lib = _load()
+    t, m, off = pack(times, mags)
+    e = None
+    if errs is not None:
+        _, e, _ = pack(times, errs)
+    p, d = _grid(periods, pdts)
+    out = np.zeros((len(off) - 1, len(p), len(d)), np.float32)
+    lib.orc_bls_batched(_ptr(t, _f32p), _ptr(m, _f32p), None if e is None else _ptr(e, _f32p),
+                        _ptr(off, _i64p), len(off) - 1, _ptr(p, _f32p), len(p), _ptr(d, _f32p),
+                        len(d), n_bins, qmin, qmax, n_threads, _ptr(out, _f32p))
     return out
 
 
@@ -327,6 +346,8 @@ def _load_ref():
             "where the reference checkout exists)")
     lib = ctypes.CDLL(_REF_PATH)
     i64, u32 = ctypes.c_int64, ctypes.c_uint32
+    lib.pfref_bls.argtypes = [_f32p, _f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64, u32,
+                              ctypes.c_float, ctypes.c_float, _f32p]
     lib.pfref_fpw.argtypes = [_f32p, _f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64, u32,
                               _f32p]
     lib.pfref_ce.argtypes = [_f32p, _f32p, _i64p, i64, _f32p, i64, _f32p, i64,
@@ -354,6 +375,14 @@ def ref_cuda(algo, times, mags, periods, pdts, **kw):
                       _ptr(out, _f32p))
     elif algo == "ls":
         lib.pfref_ls(*args, _ptr(out, _f32p))
+    elif algo == "bls":
+        errs = kw.get("errs")
+        e = (np.ones(len(t), np.float32) if errs is None
+             else np.ascontiguousarray(np.concatenate(errs), np.float32))
+        lib.pfref_bls(_ptr(t, _f32p), _ptr(m, _f32p), _ptr(e, _f32p), _ptr(off, _i64p),
+                      len(off) - 1, _ptr(p, _f32p), len(p), _ptr(d, _f32p), len(d),
+                      kw.get("n_bins", 50), kw.get("qmin", 0.01), kw.get("qmax", 0.5),
+                      _ptr(out, _f32p))
     elif algo == "fpw":
         errs = kw.get("errs")
         e = (np.ones(len(t), np.float32) if errs is None

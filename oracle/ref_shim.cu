@@ -1,7 +1,7 @@
 // ref_shim.cu -- C entry points onto the reference's own CUDA host drivers.
 //
 // TEST INFRASTRUCTURE ONLY.  Linked (by oracle/Makefile, target `ref`) with
-// the reference's periodfind/cuda/{ce,aov,ls,fpw}.cu compiled from the reference
+// the reference's periodfind/cuda/{ce,aov,ls,fpw,bls}.cu compiled from the reference
 // checkout, it exposes exactly the calls the reference's Cython wrappers make
 // (periodfind/ce.pyx:183-187, aov.pyx:166-170, ls.pyx:150-154,
 // fpw.pyx:150-154), so tests can
@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "aov.h"
+#include "bls.h"
 #include "ce.h"
 #include "fpw.h"
 #include "ls.h"
@@ -87,6 +88,21 @@ int pfref_fpw(const float* times, const float* mags, const float* errs,
     for (int64_t c = 0; c < n_curves; c++) e[c] = const_cast<float*>(errs + offsets[c]);
     FPW fpw(n_bins);
     fpw.CalcFPWBatched(t, m, e, len, periods, pdts, (size_t)n_per, (size_t)n_pdt, out);
+    return 0;
+}
+
+// BLS(n_bins, qmin, qmax).CalcBLSBatched; errs packed like mags.
+int pfref_bls(const float* times, const float* mags, const float* errs,
+              const int64_t* offsets, int64_t n_curves, const float* periods,
+              int64_t n_per, const float* pdts, int64_t n_pdt, uint32_t n_bins, float qmin,
+              float qmax, float* out) {
+    std::vector<float*> t, m, e;
+    std::vector<size_t> len;
+    unpack(times, mags, offsets, n_curves, t, m, len);
+    e.resize(n_curves);
+    for (int64_t c = 0; c < n_curves; c++) e[c] = const_cast<float*>(errs + offsets[c]);
+    BLS bls(n_bins, qmin, qmax);
+    bls.CalcBLSBatched(t, m, e, len, periods, pdts, (size_t)n_per, (size_t)n_pdt, out);
     return 0;
 }
 

@@ -1,5 +1,6 @@
 """periodfind_b200: periodfind's batched periodograms (Conditional Entropy,
-Analysis of Variance, Lomb-Scargle, FPW) on NVIDIA B200 (sm_100a).
+Analysis of Variance, Lomb-Scargle, FPW, box least squares) on NVIDIA B200
+(sm_100a).
 
     from periodfind_b200.gpu import ConditionalEntropy, AOV, LombScargle, FPW
     ce = ConditionalEntropy(n_phase=10, n_mag=10)
@@ -14,12 +15,12 @@ absent or no B200 is visible.
 from .stats import Periodogram, Statistics
 
 __all__ = ["Statistics", "Periodogram", "ConditionalEntropy", "AOV", "LombScargle", "FPW",
-           "gpu"]
+           "BoxLeastSquares", "gpu"]
 __version__ = "0.1.0"
 
 
 def __getattr__(name):
-    if name in ("ConditionalEntropy", "AOV", "LombScargle", "FPW", "gpu"):
+    if name in ("ConditionalEntropy", "AOV", "LombScargle", "FPW", "BoxLeastSquares", "gpu"):
         import importlib
 
         gpu = importlib.import_module(__name__ + ".gpu")

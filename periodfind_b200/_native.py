@@ -39,6 +39,7 @@ _vp = ctypes.c_void_p
 _u64 = ctypes.c_uint64
 _u32 = ctypes.c_uint32
 _int = ctypes.c_int
+_f32 = ctypes.c_float
 
 # Every symbol the header declares, with its argument types.
 SIGNATURES = {
@@ -58,6 +59,10 @@ SIGNATURES = {
                      _vp], _int),
     "pf_wait": ([_vp], _int),
     "pf_prepare_mags_dev": ([_vp, _vp, _vp, _u64, _int, _vp, _vp], _int),
+    "pf_bls": ([_vp, _vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _f32, _f32, _int,
+                _vp], _int),
+    "pf_bls_peaks": ([_vp, _vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _f32, _f32,
+                      _u32, _u32, _int, _vp, _vp], _int),
     "pf_fpw": ([_vp, _vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _int, _vp], _int),
     "pf_fpw_peaks": ([_vp, _vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32,
                       _int, _vp, _vp], _int),

@@ -1000,11 +1000,18 @@ int ls_common_checks(pf_ctx* ctx, const float* d_times, const int64_t* offsets,
 // (iv = 1 / err^2, ivy = iv * m, errs absent = 1), packs them with the
 // times, and one launch covers every (curve, period derivative, period
 // tile); the peaks, when asked for, are found on the device.
+//
+// BLS (BLS::CalcBLSBatched, periodfind/cuda/bls.cu; calc_bls_batched /
+// calc_bls_peaks_batched, rust/src/lib.rs:264-322, 718-760) runs the same
+// way with the second weight w * (m - mean), mean = sum(w m) / sum(w) in
+// sequential f32 sums as both references compute it (bls.rs:36-48,
+// bls.cu:419-435), and the window search of the kernel.
 int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
             const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
             const float* periods, uint64_t n_per, const float* pdts, uint64_t n_pdt,
             uint32_t n_bins, int mode, float* out, bool peaks, uint32_t n_peaks,
-            uint32_t min_distance, int64_t* out_idx, float* out_val) {
+            uint32_t min_distance, int64_t* out_idx, float* out_val, bool bls = false,
+            float qmin = 0.0f, float qmax = 0.0f) {
     if (!ctx) return PF_EINVAL;
     Job j;
     j.algo = ALGO_LS;  // no bin-count checks of CE / AOV apply
@@ -1022,7 +1029,7 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
     int rc = validate_common(ctx, j);
     if (rc != PF_OK) return rc;
     if (mode & (PF_ASYNC | PF_TIMING))
-        return fail(ctx, PF_EINVAL, "PF_ASYNC and PF_TIMING do not apply to FPW");
+        return fail(ctx, PF_EINVAL, "PF_ASYNC and PF_TIMING do not apply to FPW / BLS");
     if (n_bins < 1 || n_bins > kFpwMaxBins)
         return fail(ctx, PF_EINVAL, "n_bins must be in [1, %u], got %u", kFpwMaxBins, n_bins);
     if (n_curves == 0) return PF_OK;
@@ -1068,16 +1075,27 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
                 const float* m = mags[c];
                 const float* e = errs ? errs[c] : nullptr;
                 const int64_t o = off[c];
+                // This unit is built without multiply-add contraction.
+                float mean_y = 0.0f;
+                if (bls) {
+                    float total_w = 0.0f, total_wy = 0.0f;
+                    for (uint32_t i = 0; i < len[c]; i++) {
+                        const float err = e ? e[i] : 1.0f;
+                        const float w_i = 1.0f / (err * err);
+                        total_w += w_i;
+                        total_wy += w_i * m[i];
+                    }
+                    mean_y = total_w > 0.0f ? total_wy / total_w : 0.0f;
+                }
                 for (uint32_t i = 0; i < len[c]; i++) {
                     const float x = t[i];
                     if (!std::isfinite(x)) bad[w] = 1;
                     tmx[w] = std::max(tmx[w], std::fabs(x));
                     ht[o + i] = x;
                     const float err = e ? e[i] : 1.0f;
-                    // This unit is built without multiply-add contraction.
                     const float w_i = 1.0f / (err * err);
                     hiv[o + i] = w_i;
-                    hivy[o + i] = w_i * m[i];
+                    hivy[o + i] = bls ? w_i * (m[i] - mean_y) : w_i * m[i];
                 }
             }
         };
@@ -1114,8 +1132,21 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
     p.n_per = n_per;
     p.n_pdt = (uint32_t)n_pdt;
     p.n_bins = n_bins;
-    // FPW::FPW (fpw.cu:19-22): 1.0 / (float)n_bins in double, stored as float.
-    p.bin_size = (float)(1.0 / (double)(float)n_bins);
+    // FPW::FPW (fpw.cu:19-22): 1.0 / (float)n_bins in double, stored as
+    // float; BLS::BLS (bls.cu:20-25): 1.0f / (float)n_bins.
+    p.bin_size = bls ? 1.0f / (float)n_bins : (float)(1.0 / (double)(float)n_bins);
+    p.bls = bls ? 1 : 0;
+    if (bls) {
+        // Window widths (bls.rs:51-52): max(floor(qmin nb), 1) and
+        // min(ceil(qmax nb), nb - 1), with Rust's saturating float casts.
+        auto sat = [](float x) -> uint64_t {
+            if (!(x > 0.0f)) return 0;
+            if (x >= 18446744073709551616.0f) return UINT64_MAX;
+            return (uint64_t)x;
+        };
+        p.nb_min = (uint32_t)std::max<uint64_t>(sat(std::floor(qmin * (float)n_bins)), 1);
+        p.nb_max = (uint32_t)std::min<uint64_t>(sat(std::ceil(qmax * (float)n_bins)), n_bins - 1);
+    }
     p.out = (float*)ctx->d_out.p;
     p.tmax = tmax;
     p.edge_d = edge_guard(n_bins);
@@ -1123,7 +1154,7 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
     PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
     PF_CUDA((mode & PF_SEM_CPU) ? launch_fpw_cpusem(p, exact, n_curves, s)
                                 : launch_fpw_cudasem(p, exact, n_curves, s),
-            "FPW kernel launch");
+            "FPW / BLS kernel launch");
     PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
     ctx->timed_pending = true;
     ctx->launches++;
@@ -1665,6 +1696,24 @@ int pf_prepare_mags_dev(pf_ctx* ctx, const float* d_mags, const int64_t* offsets
     ctx->prep_pending = true;
     ctx->launches++;
     return PF_OK;
+}
+
+int pf_bls(pf_ctx* ctx, const float* const* times, const float* const* mags,
+           const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
+           const float* periods, uint64_t n_per, const float* period_dts, uint64_t n_pdt,
+           uint32_t n_bins, float qmin, float qmax, int mode, float* out) {
+    return run_fpw(ctx, times, mags, errs, lengths, n_curves, periods, n_per, period_dts, n_pdt,
+                   n_bins, mode, out, false, 0, 0, nullptr, nullptr, true, qmin, qmax);
+}
+
+int pf_bls_peaks(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                 const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
+                 const float* periods, uint64_t n_per, const float* period_dts, uint64_t n_pdt,
+                 uint32_t n_bins, float qmin, float qmax, uint32_t n_peaks,
+                 uint32_t min_distance, int mode, int64_t* out_idx, float* out_val) {
+    return run_fpw(ctx, times, mags, errs, lengths, n_curves, periods, n_per, period_dts, n_pdt,
+                   n_bins, mode, nullptr, true, n_peaks, min_distance, out_idx, out_val, true,
+                   qmin, qmax);
 }
 
 int pf_wait(pf_ctx* ctx) {

@@ -1,4 +1,4 @@
-// pf_fpw.cuh -- FPW (fast phase-folding weighted) periodogram, included by
+// pf_fpw.cuh -- FPW (fast phase-folding weighted) and BLS periodograms, included by
 // each arithmetic unit after pf_fold.cuh and pf_bin.cuh.
 //
 // Statistic (rust/src/fpw.rs:12-66; periodfind/cuda/fpw.cu:45-224): each
@@ -46,16 +46,23 @@ __device__ __forceinline__ uint32_t fpw_ref_bin(float folded, const FpwParams& p
     return min(b, p.n_bins - 1u);
 }
 
-template <int BLOCK, bool CHOSEN>
+// BLS (Box Least Squares, rust/src/bls.rs:19-134; periodfind/cuda/bls.cu:
+// 56-308) shares the binning: the second sum is w * (m - weighted mean), the
+// bins sit one row down so that row 0 holds the zero of the prefix sums, and
+// the value is the best s^2 / (r (W - r)) over the windows of nb_min ..
+// nb_max consecutive bins (wrapping) whose weight fraction r / W lies in
+// (0, 1); 0 when W <= 0.
+template <int BLOCK, bool CHOSEN, bool BLS>
 __global__ void __launch_bounds__(BLOCK)
     fpw_kernel(const FpwParams p, uint32_t tiles_per_row) {
     using TT = typename std::conditional<CHOSEN, double, float>::type;
+    constexpr uint32_t kRow0 = BLS ? 1u : 0u;  // rows before bin 0
     extern __shared__ __align__(16) unsigned char fsm[];
     TT* st = reinterpret_cast<TT*>(fsm);
     float* siv = reinterpret_cast<float*>(st + kFpwTile);
     float* sivy = siv + kFpwTile;
-    float* bv = sivy + kFpwTile;          // [n_bins][BLOCK]
-    float* by = bv + p.n_bins * BLOCK;    // [n_bins][BLOCK]
+    float* bv = sivy + kFpwTile;                   // [kRow0 + n_bins][BLOCK]
+    float* by = bv + (p.n_bins + kRow0) * BLOCK;   // [kRow0 + n_bins][BLOCK]
     __shared__ double warp_min[BLOCK / 32];
 
     const uint64_t cta = blockIdx.x;
@@ -70,7 +77,7 @@ __global__ void __launch_bounds__(BLOCK)
     const int64_t off = p.off[c];
     const uint32_t n = p.len[c];
     const uint32_t nb = p.n_bins;
-    for (uint32_t k = 0; k < nb; k++) {
+    for (uint32_t k = 0; k < nb + kRow0; k++) {
         bv[k * BLOCK + tid] = 0.0f;
         by[k * BLOCK + tid] = 0.0f;
     }
@@ -138,17 +145,50 @@ __global__ void __launch_bounds__(BLOCK)
             } else {
                 bin = fpw_ref_bin(fold_ref(st[i], s), p);
             }
-            bv[bin * BLOCK + tid] += siv[i];
-            by[bin * BLOCK + tid] += sivy[i];
+            bv[(bin + kRow0) * BLOCK + tid] += siv[i];
+            by[(bin + kRow0) * BLOCK + tid] += sivy[i];
         }
     }
     if (!active) return;
     float acc = 0.0f;
-    for (uint32_t k = 0; k < nb; k++) {
-        const float v = bv[k * BLOCK + tid];
-        if (v > 0.0f) {
-            const float y = by[k * BLOCK + tid];
-            acc += y * y / (2.0f * v);
+    if constexpr (BLS) {
+        // Prefix sums in place, in the reference's order (bls.rs:83-89):
+        // row k + 1 becomes row k + row k + 1.
+        for (uint32_t k = 0; k < nb; k++) {
+            bv[(k + 1) * BLOCK + tid] = bv[k * BLOCK + tid] + bv[(k + 1) * BLOCK + tid];
+            by[(k + 1) * BLOCK + tid] = by[k * BLOCK + tid] + by[(k + 1) * BLOCK + tid];
+        }
+        const float w_total = bv[nb * BLOCK + tid];
+        if (w_total > 0.0f) {
+            const float y_total = by[nb * BLOCK + tid];
+            for (uint32_t nbw = p.nb_min; nbw <= p.nb_max; nbw++) {
+                for (uint32_t phi = 0; phi < nb; phi++) {
+                    const uint32_t end = phi + nbw;
+                    const float w_phi = bv[phi * BLOCK + tid], y_phi = by[phi * BLOCK + tid];
+                    float r, sy;
+                    if (end <= nb) {
+                        r = bv[end * BLOCK + tid] - w_phi;
+                        sy = by[end * BLOCK + tid] - y_phi;
+                    } else {
+                        const uint32_t wrap = end - nb;
+                        r = (w_total - w_phi) + bv[wrap * BLOCK + tid];
+                        sy = (y_total - y_phi) + by[wrap * BLOCK + tid];
+                    }
+                    const float r_frac = r / w_total;
+                    if (r_frac > 0.0f && r_frac < 1.0f) {
+                        const float bls = (sy * sy) / (r * (w_total - r));
+                        if (bls > acc) acc = bls;
+                    }
+                }
+            }
+        }
+    } else {
+        for (uint32_t k = 0; k < nb; k++) {
+            const float v = bv[k * BLOCK + tid];
+            if (v > 0.0f) {
+                const float y = by[k * BLOCK + tid];
+                acc += y * y / (2.0f * v);
+            }
         }
     }
     p.out[(uint64_t)c * (p.n_per * p.n_pdt) + pi * p.n_pdt + d] = acc;

@@ -60,7 +60,7 @@ cudaError_t launch_binaux_cpusem(const float* m, void* aux, const CurveDesc* cur
                                  uint32_t n_curves, uint32_t n_mag, float mag_bin_size,
                                  int block, int cnt16, cudaStream_t s);
 
-// FPW (pf_fpw.cuh): per point t, inverse variance iv = 1 / err^2 and
+// FPW and BLS (pf_fpw.cuh): per point t, inverse variance iv = 1 / err^2 and
 // ivy = iv * m, packed per curve at off[c] with len[c] points; out is
 // [curve][period][pdt].  bin_size = 1 / n_bins as the reference rounds it.
 struct FpwParams {
@@ -78,6 +78,8 @@ struct FpwParams {
     float* out;
     double tmax;      // max |t| over the batch (the chosen form's range guard)
     uint32_t edge_d;  // bin-edge guard, units of 2^-20 bin (as the CE / AOV bin kernels)
+    int bls;          // BLS instead of FPW (ivy then holds w * (m - weighted mean))
+    uint32_t nb_min, nb_max;  // BLS: window widths searched, in bins
 };
 constexpr uint32_t kFpwMaxBins = 128;
 // exact: the chosen form (fast bins with the reference sequence near bin

@@ -509,12 +509,19 @@ class FPW(_Periodogram):
                     f"errs[{i}] and times[{i}] have different lengths: {len(e)} vs {len(t)}")
         return errs
 
+    # The native calls and the statistic's own arguments after n_bins.
+    _pgram_fn, _peaks_fn = "pf_fpw", "pf_fpw_peaks"
+
+    def _stat_args(self):
+        return (self.n_bins,)
+
     def _call(self, ctx, fn, times, mags, errs, periods, pdts, *tail):
         b = nat.CurveBatch(times, mags)
         eptr, keep = (None, None) if errs is None else nat.host_pointers(errs, b.lengths)
         tptr, mptr, lens, n = b.args()
         rc = fn(ctx.handle, tptr, mptr, None if eptr is None else eptr.ctypes.data, lens, n,
-                nat.ptr(periods), len(periods), nat.ptr(pdts), len(pdts), self.n_bins, *tail)
+                nat.ptr(periods), len(periods), nat.ptr(pdts), len(pdts), *self._stat_args(),
+                *tail)
         del keep
         return rc
 
@@ -523,8 +530,8 @@ class FPW(_Periodogram):
         ctx = nat.default_context(self.device)
         out = np.empty((len(times), len(periods), len(period_dts)), dtype=np.float32)
         with ctx.lock:
-            ctx.check(self._call(ctx, ctx.lib.pf_fpw, times, mags, errs, periods, period_dts,
-                                 self._flags, nat.ptr(out)))
+            ctx.check(self._call(ctx, getattr(ctx.lib, self._pgram_fn), times, mags, errs,
+                                 periods, period_dts, self._flags, nat.ptr(out)))
         return out
 
     def peaks(self, times, mags, periods, period_dts, n_peaks=N_PEAKS_DEFAULT,
@@ -537,15 +544,15 @@ class FPW(_Periodogram):
         idx = np.full((len(times), n_peaks), -1, dtype=np.int64)
         val = np.zeros((len(times), n_peaks), dtype=np.float32)
         with ctx.lock:
-            ctx.check(self._call(ctx, ctx.lib.pf_fpw_peaks, times, mags, errs, periods,
-                                 period_dts, n_peaks, int(min_distance), self._flags,
+            ctx.check(self._call(ctx, getattr(ctx.lib, self._peaks_fn), times, mags, errs,
+                                 periods, period_dts, n_peaks, int(min_distance), self._flags,
                                  nat.ptr(idx), nat.ptr(val)))
         return idx, val
 
     def calc(self, times, mags, periods, period_dts, errs=None, output="stats",
              normalize=False, center=False, n_stats=1, significance_type="stdmean",
              n_peaks=N_PEAKS_DEFAULT, min_distance=MIN_DISTANCE_DEFAULT):
-        """Compute the FPW periodogram of every light curve.
+        """Compute the periodogram of every light curve.
 
         Returns a list of Statistics (output='stats'; lists of them when
         n_stats > 1), a list of Periodogram (output='periodogram'), or a list
@@ -571,6 +578,30 @@ class FPW(_Periodogram):
                     data[i], [periods, period_dts], True, n=n_stats,
                     significance_type=significance_type) for i in range(len(times))]
             return [Periodogram(d, [periods, period_dts], True) for d in data]
+
+
+class BoxLeastSquares(FPW):
+    """Box least squares (BLS, Kovacs, Zucker & Mazeh 2002) transit search,
+    maximum is best (periodfind/bls.pyx:36-181; the CPU class
+    periodfind/cpu/__init__.py:525-640, whose 'peaks' output it also has).
+
+    Per point an inverse variance w = 1 / err^2 weights the magnitude minus
+    the curve's weighted mean; the phase bins' sums are searched for the
+    window of qmin .. qmax of the period (in bins, wrapping) with the best
+    s^2 / (r (W - r)).  `errs` None means unit uncertainties; `normalize`
+    and `center` are accepted and unused, as in the reference.
+    """
+
+    _pgram_fn, _peaks_fn = "pf_bls", "pf_bls_peaks"
+
+    def __init__(self, n_bins=50, qmin=0.01, qmax=0.5, *, mode="chosen", semantics="cuda",
+                 device=0):
+        super().__init__(n_bins, mode=mode, semantics=semantics, device=device)
+        self.qmin = float(qmin)
+        self.qmax = float(qmax)
+
+    def _stat_args(self):
+        return (self.n_bins, self.qmin, self.qmax)
 
 
 def find_top_peaks_batched(data, n_peaks, min_distance, use_max, device=0):

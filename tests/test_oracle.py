@@ -184,3 +184,75 @@ def test_fpw_known_period(oracle, case):
                     errs=None if e is None else [e])[0, :, 0]
     best = P[int(np.argmax(pg))]
     assert abs(best - case["period"]) / case["period"] < 0.05, best
+
+
+def _bls_numpy(t, m, e, periods, pdts, n_bins, qmin, qmax):
+    """BLS from numpy: the fold and f32 bin rule of rust/src/bls.rs:75-80, the
+    weighted mean, bin sums, prefix sums and window search in float64."""
+    t64 = t.astype(np.float64)
+    w = (1.0 / (e.astype(np.float64) ** 2)) if e is not None else np.ones(len(t))
+    yw = w * (m.astype(np.float64) - np.sum(w * m) / np.sum(w))
+    lo = max(int(np.floor(np.float32(qmin) * np.float32(n_bins))), 1)
+    hi = min(int(np.ceil(np.float32(qmax) * np.float32(n_bins))), n_bins - 1)
+    out = np.zeros((len(periods), len(pdts)))
+    for pi, P in enumerate(periods):
+        for di, dt in enumerate(pdts):
+            corr = np.float32(np.float32(dt) / np.float32(P)) / np.float32(2.0)
+            r = (t64 - np.float64(corr) * t64 * t64) / np.float64(P)
+            phase = np.abs(r - np.floor(r)).astype(np.float32)
+            b = np.minimum((phase * np.float32(n_bins)).astype(np.int64), n_bins - 1)
+            W = np.concatenate([[0.0], np.cumsum(np.bincount(b, weights=w, minlength=n_bins))])
+            Y = np.concatenate([[0.0], np.cumsum(np.bincount(b, weights=yw, minlength=n_bins))])
+            best = 0.0
+            for nb in range(lo, hi + 1):
+                for phi in range(n_bins):
+                    end = phi + nb
+                    if end <= n_bins:
+                        rr, ss = W[end] - W[phi], Y[end] - Y[phi]
+                    else:
+                        rr = W[n_bins] - W[phi] + W[end - n_bins]
+                        ss = Y[n_bins] - Y[phi] + Y[end - n_bins]
+                    if 0 < rr / W[n_bins] < 1:
+                        best = max(best, ss * ss / (rr * (W[n_bins] - rr)))
+            out[pi, di] = best
+    return out
+
+
+def test_bls_matches_numpy_restatement(oracle):
+    """The oracle's BLS (f32 sums in point order, as rust/src/bls.rs) is close
+    to the same statistic in float64 (window sums difference-cancel, so the
+    tolerance is looser than FPW's)."""
+    rng = np.random.default_rng(5)
+    t = lc.uniform_times(rng, 600, 200.0)
+    m = lc.noisy(rng, lc.box_eclipse(t, 2.7, depth=0.3, duty=0.08) + 15.0, 0.02)
+    e = rng.uniform(0.02, 0.2, 600).astype(np.float32)
+    P = lc.trial_periods(2.7, n=40)
+    D = np.array([0.0, 1e-4], np.float32)
+    for errs, nb, q in ((None, 50, (0.01, 0.5)), ([e], 30, (0.02, 0.3)), ([e], 64, (0.0, 1.0))):
+        got = oracle.bls([t], [m], P, D, nb, q[0], q[1], errs=errs)[0]
+        want = _bls_numpy(t, m, None if errs is None else e, P, D, nb, *q)
+        np.testing.assert_allclose(got, want, rtol=2e-3, atol=1e-6 * want.max())
+
+
+@pytest.mark.parametrize("case", [
+    dict(kind="eclipse", period=2.5, n=800, span=200.0, noise=0.02, qmax=0.3, errs=None),
+    dict(kind="sine", period=5.0, n=800, span=200.0, noise=0.02, qmax=0.5, errs=None),
+    dict(kind="eclipse", period=3.0, n=600, span=150.0, noise=0.05, qmax=0.3, errs=0.05),
+    dict(kind="eclipse", period=2.0, n=500, span=100.0, noise=0.03, qmax=0.3, errs=None),
+])
+def test_bls_known_period(oracle, case):
+    """Known-answer cases of the reference's CPU BLS tests
+    (tests/test_cpu_standalone.py:555-640): the best period is the injected
+    one, its half or its double, to 5%."""
+    rng = np.random.default_rng(42)
+    t = lc.uniform_times(rng, case["n"], case["span"])
+    y = (lc.v_eclipse(t, case["period"]) if case["kind"] == "eclipse"
+         else lc.sinusoid(t, case["period"]))
+    m = lc.noisy(rng, y, case["noise"])
+    e = None if case["errs"] is None else [np.full(case["n"], case["errs"], np.float32)]
+    P = lc.trial_periods(case["period"], n=500)
+    pg = oracle.bls([t], [m], P, np.zeros(1, np.float32), 50, 0.01, case["qmax"],
+                    errs=e)[0, :, 0]
+    best = float(P[int(np.argmax(pg))])
+    assert any(abs(best - c) / c < 0.05 for c in (case["period"], case["period"] / 2,
+                                                  case["period"] * 2)), best
