@@ -34,7 +34,7 @@
 namespace pfk {
 namespace PF_KNS {
 
-constexpr uint32_t kFpwTile = 1024;
+constexpr uint32_t kFpwTile = 256;
 
 // The reference's bin of a folded phase, with this unit's arithmetic.
 __device__ __forceinline__ uint32_t fpw_ref_bin(float folded, const FpwParams& p) {
