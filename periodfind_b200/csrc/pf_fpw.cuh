@@ -56,13 +56,16 @@ template <int BLOCK, bool CHOSEN, bool BLS>
 __global__ void __launch_bounds__(BLOCK)
     fpw_kernel(const FpwParams p, uint32_t tiles_per_row) {
     using TT = typename std::conditional<CHOSEN, double, float>::type;
+    // One 16-byte record per staged point: a single 128-bit shared load.
+    struct alignas(16) Point {
+        TT t;
+        float iv, ivy;
+    };
     constexpr uint32_t kRow0 = BLS ? 1u : 0u;  // rows before bin 0
     extern __shared__ __align__(16) unsigned char fsm[];
-    TT* st = reinterpret_cast<TT*>(fsm);
-    float* siv = reinterpret_cast<float*>(st + kFpwTile);
-    float* sivy = siv + kFpwTile;
-    float* bv = sivy + kFpwTile;                   // [kRow0 + n_bins][BLOCK]
-    float* by = bv + (p.n_bins + kRow0) * BLOCK;   // [kRow0 + n_bins][BLOCK]
+    Point* st = reinterpret_cast<Point*>(fsm);
+    float* bv = reinterpret_cast<float*>(st + kFpwTile);  // [kRow0 + n_bins][BLOCK]
+    float* by = bv + (p.n_bins + kRow0) * BLOCK;          // [kRow0 + n_bins][BLOCK]
     __shared__ double warp_min[BLOCK / 32];
 
     const uint64_t cta = blockIdx.x;
@@ -112,18 +115,16 @@ __global__ void __launch_bounds__(BLOCK)
     for (uint32_t base = 0; base < n; base += kFpwTile) {
         const uint32_t cnt = min(kFpwTile, n - base);
         __syncthreads();
-        for (uint32_t i = tid; i < cnt; i += BLOCK) {
-            st[i] = (TT)p.t[off + base + i];
-            siv[i] = p.iv[off + base + i];
-            sivy[i] = p.ivy[off + base + i];
-        }
+        for (uint32_t i = tid; i < cnt; i += BLOCK)
+            st[i] = Point{(TT)p.t[off + base + i], p.iv[off + base + i], p.ivy[off + base + i]};
         __syncthreads();
         if (!active) continue;
 #pragma unroll 4
         for (uint32_t i = 0; i < cnt; i++) {
+            const Point pt = st[i];
             uint32_t bin;
             if constexpr (CHOSEN) {
-                const double td = st[i];
+                const double td = pt.t;
                 if (fast) {
                     const double a = has_pdt ? td - s.c * td * td : td;
                     const double qh = __dmul_rn(a, s.yhi);
@@ -143,10 +144,10 @@ __global__ void __launch_bounds__(BLOCK)
                                               : fold_exact<false>(td, s), p);
                 }
             } else {
-                bin = fpw_ref_bin(fold_ref(st[i], s), p);
+                bin = fpw_ref_bin(fold_ref(pt.t, s), p);
             }
-            bv[(bin + kRow0) * BLOCK + tid] += siv[i];
-            by[(bin + kRow0) * BLOCK + tid] += sivy[i];
+            bv[(bin + kRow0) * BLOCK + tid] += pt.iv;
+            by[(bin + kRow0) * BLOCK + tid] += pt.ivy;
         }
     }
     if (!active) return;
