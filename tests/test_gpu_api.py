@@ -266,8 +266,12 @@ def test_stats_on_device_equal_numpy(gpu, algo, n_stats):
         D = np.array(pdts, np.float32)
         got = obj.calc(ts, ms, P, D, output="stats", n_stats=n_stats)
         pgs = obj.calc(ts, ms, P, D, output="periodogram")
-        want = [Statistics.statistics_from_data(pg.data, [P, D], obj._use_max, n=n_stats)
-                for pg in pgs]
+        with warnings.catch_warnings():
+            # numpy's std of an AOV row holding inf (a curve shorter than
+            # its bins) warns; the device statistics carry the same NaN.
+            warnings.simplefilter("ignore", RuntimeWarning)
+            want = [Statistics.statistics_from_data(pg.data, [P, D], obj._use_max, n=n_stats)
+                    for pg in pgs]
         for g, w, pg in zip(got, want, pgs):
             _stats_equal(g, w, pg.data, (P, D))
 
