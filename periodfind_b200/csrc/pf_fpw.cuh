@@ -52,7 +52,7 @@ __device__ __forceinline__ uint32_t fpw_ref_bin(float folded, const FpwParams& p
 // the value is the best s^2 / (r (W - r)) over the windows of nb_min ..
 // nb_max consecutive bins (wrapping) whose weight fraction r / W lies in
 // (0, 1); 0 when W <= 0.
-template <int BLOCK, bool CHOSEN, bool BLS>
+template <int BLOCK, bool CHOSEN, bool BLS, int GROUP>
 __global__ void __launch_bounds__(BLOCK)
     fpw_kernel(const FpwParams p, uint32_t tiles_per_row) {
     using TT = typename std::conditional<CHOSEN, double, float>::type;
@@ -112,6 +112,30 @@ __global__ void __launch_bounds__(BLOCK)
     const uint32_t edge_add = p.edge_d << 12;
     const uint32_t edge_lim = (2u * p.edge_d) << 12;
 
+    // The reference's bin of point time t (the fast bin when the CTA's
+    // bound allows, the reference sequence near an edge or otherwise).
+    auto bin_of = [&](TT t) -> uint32_t {
+        if constexpr (CHOSEN) {
+            const double td = t;
+            if (fast) {
+                const double a = has_pdt ? td - s.c * td * td : td;
+                const double qh = __dmul_rn(a, s.yhi);
+                const double r = __dadd_rd(qh, kMagic15);
+                const double y = __fma_rd(qh, nd20, kMagic15);
+                const uint32_t ylo = (uint32_t)__double2loint(y);
+                const uint32_t yhi = (uint32_t)__double2hiint(y);
+                // floor(q' n_bins) - n_bins floor(q'), biased by 2^31 by the
+                // magic constant's top mantissa bit.
+                const uint32_t b = __funnelshift_r(ylo, yhi, 20) +
+                                   (uint32_t)__double2loint(r) * n_neg - 0x80000000u;
+                if (ylo * 4096u + edge_add >= edge_lim) return b;
+            }
+            return fpw_ref_bin(has_pdt ? fold_exact<true>(td, s) : fold_exact<false>(td, s), p);
+        } else {
+            return fpw_ref_bin(fold_ref(t, s), p);
+        }
+    };
+
     for (uint32_t base = 0; base < n; base += kFpwTile) {
         const uint32_t cnt = min(kFpwTile, n - base);
         __syncthreads();
@@ -119,33 +143,32 @@ __global__ void __launch_bounds__(BLOCK)
             st[i] = Point{(TT)p.t[off + base + i], p.iv[off + base + i], p.ivy[off + base + i]};
         __syncthreads();
         if (!active) continue;
-#pragma unroll 4
-        for (uint32_t i = 0; i < cnt; i++) {
-            const Point pt = st[i];
-            uint32_t bin;
-            if constexpr (CHOSEN) {
-                const double td = pt.t;
-                if (fast) {
-                    const double a = has_pdt ? td - s.c * td * td : td;
-                    const double qh = __dmul_rn(a, s.yhi);
-                    const double r = __dadd_rd(qh, kMagic15);
-                    const double y = __fma_rd(qh, nd20, kMagic15);
-                    const uint32_t ylo = (uint32_t)__double2loint(y);
-                    const uint32_t yhi = (uint32_t)__double2hiint(y);
-                    // floor(q' n_bins) - n_bins floor(q'), biased by 2^31 by
-                    // the magic constant's top mantissa bit.
-                    bin = __funnelshift_r(ylo, yhi, 20) + (uint32_t)__double2loint(r) * n_neg -
-                          0x80000000u;
-                    if (ylo * 4096u + edge_add < edge_lim)
-                        bin = fpw_ref_bin(has_pdt ? fold_exact<true>(td, s)
-                                                  : fold_exact<false>(td, s), p);
-                } else {
-                    bin = fpw_ref_bin(has_pdt ? fold_exact<true>(td, s)
-                                              : fold_exact<false>(td, s), p);
+        uint32_t i = 0;
+        if constexpr (GROUP > 1) {
+            // GROUP points are read and binned before the first of their
+            // read-modify-writes: the staged tile and the bins share one
+            // shared-memory array, so a point read cannot move above an
+            // earlier bin store, and one point at a time would chain the
+            // point read, the bin arithmetic and the bin update per point.
+            // The updates stay in point order (same bin, same rounding).
+            for (; i + GROUP <= cnt; i += GROUP) {
+                Point q[GROUP];
+                uint32_t b[GROUP];
+#pragma unroll
+                for (int k = 0; k < GROUP; k++) q[k] = st[i + k];
+#pragma unroll
+                for (int k = 0; k < GROUP; k++) b[k] = bin_of(q[k].t);
+#pragma unroll
+                for (int k = 0; k < GROUP; k++) {
+                    bv[(b[k] + kRow0) * BLOCK + tid] += q[k].iv;
+                    by[(b[k] + kRow0) * BLOCK + tid] += q[k].ivy;
                 }
-            } else {
-                bin = fpw_ref_bin(fold_ref(pt.t, s), p);
             }
+        }
+#pragma unroll 4
+        for (; i < cnt; i++) {
+            const Point pt = st[i];
+            const uint32_t bin = bin_of(pt.t);
             bv[(bin + kRow0) * BLOCK + tid] += pt.iv;
             by[(bin + kRow0) * BLOCK + tid] += pt.ivy;
         }
