@@ -64,8 +64,25 @@ __global__ void __launch_bounds__(BLOCK)
     constexpr uint32_t kRow0 = BLS ? 1u : 0u;  // rows before bin 0
     extern __shared__ __align__(16) unsigned char fsm[];
     Point* st = reinterpret_cast<Point*>(fsm);
-    float* bv = reinterpret_cast<float*>(st + kFpwTile);  // [kRow0 + n_bins][BLOCK]
-    float* by = bv + (p.n_bins + kRow0) * BLOCK;          // [kRow0 + n_bins][BLOCK]
+    // Per-thread bins, row k (bin k - kRow0) of thread tid: the chosen form
+    // keeps (V, Y) pairs, [row][BLOCK] float2, so a bin update is one 8-byte
+    // load and store; the plain form keeps V rows then Y rows.
+    float* bins = reinterpret_cast<float*>(st + kFpwTile);
+    const uint32_t rows = p.n_bins + kRow0;
+    auto ld = [&](uint32_t k) -> float2 {
+        if constexpr (CHOSEN)
+            return reinterpret_cast<const float2*>(bins)[k * BLOCK + threadIdx.x];
+        else
+            return make_float2(bins[k * BLOCK + threadIdx.x], bins[(rows + k) * BLOCK + threadIdx.x]);
+    };
+    auto put = [&](uint32_t k, float2 x) {
+        if constexpr (CHOSEN) {
+            reinterpret_cast<float2*>(bins)[k * BLOCK + threadIdx.x] = x;
+        } else {
+            bins[k * BLOCK + threadIdx.x] = x.x;
+            bins[(rows + k) * BLOCK + threadIdx.x] = x.y;
+        }
+    };
     __shared__ double warp_min[BLOCK / 32];
 
     const uint64_t cta = blockIdx.x;
@@ -80,10 +97,7 @@ __global__ void __launch_bounds__(BLOCK)
     const int64_t off = p.off[c];
     const uint32_t n = p.len[c];
     const uint32_t nb = p.n_bins;
-    for (uint32_t k = 0; k < nb + kRow0; k++) {
-        bv[k * BLOCK + tid] = 0.0f;
-        by[k * BLOCK + tid] = 0.0f;
-    }
+    for (uint32_t k = 0; k < rows; k++) put(k, make_float2(0.0f, 0.0f));
     const float period = p.periods[active ? pi : (uint64_t)tile * BLOCK];
     const float period_dt = p.pdts[d];
     Cell s;
@@ -160,8 +174,10 @@ __global__ void __launch_bounds__(BLOCK)
                 for (int k = 0; k < GROUP; k++) b[k] = bin_of(q[k].t);
 #pragma unroll
                 for (int k = 0; k < GROUP; k++) {
-                    bv[(b[k] + kRow0) * BLOCK + tid] += q[k].iv;
-                    by[(b[k] + kRow0) * BLOCK + tid] += q[k].ivy;
+                    float2 x = ld(b[k] + kRow0);
+                    x.x += q[k].iv;
+                    x.y += q[k].ivy;
+                    put(b[k] + kRow0, x);
                 }
             }
         }
@@ -169,8 +185,10 @@ __global__ void __launch_bounds__(BLOCK)
         for (; i < cnt; i++) {
             const Point pt = st[i];
             const uint32_t bin = bin_of(pt.t);
-            bv[(bin + kRow0) * BLOCK + tid] += pt.iv;
-            by[(bin + kRow0) * BLOCK + tid] += pt.ivy;
+            float2 x = ld(bin + kRow0);
+            x.x += pt.iv;
+            x.y += pt.ivy;
+            put(bin + kRow0, x);
         }
     }
     if (!active) return;
@@ -178,26 +196,30 @@ __global__ void __launch_bounds__(BLOCK)
     if constexpr (BLS) {
         // Prefix sums in place, in the reference's order (bls.rs:83-89):
         // row k + 1 becomes row k + row k + 1.
+        float2 prev = ld(0);
         for (uint32_t k = 0; k < nb; k++) {
-            bv[(k + 1) * BLOCK + tid] = bv[k * BLOCK + tid] + bv[(k + 1) * BLOCK + tid];
-            by[(k + 1) * BLOCK + tid] = by[k * BLOCK + tid] + by[(k + 1) * BLOCK + tid];
+            float2 x = ld(k + 1);
+            x.x = prev.x + x.x;
+            x.y = prev.y + x.y;
+            put(k + 1, x);
+            prev = x;
         }
-        const float w_total = bv[nb * BLOCK + tid];
+        const float w_total = prev.x, y_total = prev.y;
         if (w_total > 0.0f) {
-            const float y_total = by[nb * BLOCK + tid];
-            for (uint32_t nbw = p.nb_min; nbw <= p.nb_max; nbw++) {
-                for (uint32_t phi = 0; phi < nb; phi++) {
+            // Every (phase, width) window, phase-major: the window's start
+            // row is read once per phase.  The sums are the reference's:
+            // end <= nb gives row[end] - row[phi] (x - y is x + (-y)
+            // exactly), a wrapping window (total - row[phi]) + row[end - nb];
+            // the maximum does not depend on the order of the windows.
+            for (uint32_t phi = 0; phi < nb; phi++) {
+                const float2 a = ld(phi);
+                const float w_rest = w_total - a.x, y_rest = y_total - a.y;
+                for (uint32_t nbw = p.nb_min; nbw <= p.nb_max; nbw++) {
                     const uint32_t end = phi + nbw;
-                    const float w_phi = bv[phi * BLOCK + tid], y_phi = by[phi * BLOCK + tid];
-                    float r, sy;
-                    if (end <= nb) {
-                        r = bv[end * BLOCK + tid] - w_phi;
-                        sy = by[end * BLOCK + tid] - y_phi;
-                    } else {
-                        const uint32_t wrap = end - nb;
-                        r = (w_total - w_phi) + bv[wrap * BLOCK + tid];
-                        sy = (y_total - y_phi) + by[wrap * BLOCK + tid];
-                    }
+                    const bool wrap = end > nb;
+                    const float2 e = ld(wrap ? end - nb : end);
+                    const float r = e.x + (wrap ? w_rest : -a.x);
+                    const float sy = e.y + (wrap ? y_rest : -a.y);
                     const float r_frac = r / w_total;
                     if (r_frac > 0.0f && r_frac < 1.0f) {
                         const float bls = (sy * sy) / (r * (w_total - r));
@@ -208,11 +230,8 @@ __global__ void __launch_bounds__(BLOCK)
         }
     } else {
         for (uint32_t k = 0; k < nb; k++) {
-            const float v = bv[k * BLOCK + tid];
-            if (v > 0.0f) {
-                const float y = by[k * BLOCK + tid];
-                acc += y * y / (2.0f * v);
-            }
+            const float2 x = ld(k);
+            if (x.x > 0.0f) acc += x.y * x.y / (2.0f * x.x);
         }
     }
     p.out[(uint64_t)c * (p.n_per * p.n_pdt) + pi * p.n_pdt + d] = acc;
