@@ -54,7 +54,8 @@
  *                  form's divide-free one (agreeing to ~1e-6): values are then
  *                  bit-identical to the plain form exactly when the bin
  *                  occupancies are, which is how occupancy parity is tested.
- *  PF_ASYNC        (pf_ce_peaks / pf_aov_peaks / pf_ls_peaks only) enqueue
+ *  PF_ASYNC        (pf_ce_peaks / pf_aov_peaks / pf_ls_peaks / pf_fpw_peaks /
+ *                  pf_bls_peaks only) enqueue
  *                  and return: the inputs are packed into the context's
  *                  staging block and the work is queued on the context's
  *                  stream, but out_idx / out_val are written later, by the
@@ -173,7 +174,7 @@ int pf_ls_peaks(pf_ctx* ctx, const float* const* times,
  * sum over bins with V > 0 of Y^2 / (2 V).  Maximum is best.  n_bins in
  * [1, 128].  Magnitudes are used as given.  PF_MODE_CHOSEN folds without a
  * divide (same values); PF_SEM_CPU takes the Rust path's bin rule and IEEE
- * arithmetic.  PF_ASYNC and PF_TIMING are refused. */
+ * arithmetic.  PF_TIMING is refused; PF_ASYNC applies to pf_fpw_peaks. */
 int pf_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
            const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
            const float* periods, uint64_t n_per, const float* period_dts, uint64_t n_pdt,
@@ -193,7 +194,7 @@ int pf_fpw_peaks(pf_ctx* ctx, const float* const* times, const float* const* mag
  * over windows of nb_min .. nb_max consecutive bins (wrapping; nb_min =
  * max(floor(qmin n_bins), 1), nb_max = min(ceil(qmax n_bins), n_bins - 1))
  * whose weight fraction r / W_total lies in (0, 1).  Maximum is best.
- * n_bins in [1, 128]; modes as pf_fpw. */
+ * n_bins in [1, 128]; modes as pf_fpw (PF_ASYNC: pf_bls_peaks). */
 int pf_bls(pf_ctx* ctx, const float* const* times, const float* const* mags,
            const float* const* errs, const uint64_t* lengths, uint64_t n_curves,
            const float* periods, uint64_t n_per, const float* period_dts, uint64_t n_pdt,

@@ -1028,14 +1028,20 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
     j.out = out;
     int rc = validate_common(ctx, j);
     if (rc != PF_OK) return rc;
-    if (mode & (PF_ASYNC | PF_TIMING))
-        return fail(ctx, PF_EINVAL, "PF_ASYNC and PF_TIMING do not apply to FPW / BLS");
+    if (mode & PF_TIMING) return fail(ctx, PF_EINVAL, "PF_TIMING does not apply to FPW / BLS");
+    const bool async = (mode & PF_ASYNC) != 0;
+    if (async) {
+        if (!peaks) return fail(ctx, PF_EINVAL, "PF_ASYNC applies to the peak calls only");
+        if (ctx->pend_count == pf_ctx::kMaxPending)
+            return fail(ctx, PF_EINVAL, "%d PF_ASYNC calls are pending; collect one with pf_wait",
+                        pf_ctx::kMaxPending);
+    }
     if (n_bins < 1 || n_bins > kFpwMaxBins)
         return fail(ctx, PF_EINVAL, "n_bins must be in [1, %u], got %u", kFpwMaxBins, n_bins);
-    if (n_curves == 0) return PF_OK;
+    if (n_curves == 0) return async ? push_pending(ctx, j, 0, false, nullptr) : PF_OK;
     if (!times || !mags || !lengths) return fail(ctx, PF_EINVAL, "times/mags/lengths is NULL");
     const uint64_t n_cells = n_per * n_pdt;
-    if (n_cells == 0) return PF_OK;
+    if (n_cells == 0) return async ? push_pending(ctx, j, 0, false, nullptr) : PF_OK;
     if ((rc = check_grid_host(ctx, j)) != PF_OK) return rc;
     std::vector<int64_t> off(n_curves);
     std::vector<uint32_t> len(n_curves);
@@ -1167,11 +1173,23 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
                                  (int64_t*)ctx->d_pidx.p, (float*)ctx->d_pval.p, s),
                     "peak search launch");
             ctx->launches++;
-            PF_CUDA(cudaMemcpyAsync(out_idx, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
+            // PF_ASYNC: into this call's pending slot (free: its last user
+            // was collected), copied out by pf_wait.
+            char* hr = nullptr;
+            if (async) {
+                pf_ctx::Pending& q =
+                    ctx->pend[(ctx->pend_head + ctx->pend_count) % pf_ctx::kMaxPending];
+                if ((rc = ensure_pinned(ctx, q.res, pk * 12)) != PF_OK) return rc;
+                hr = (char*)q.res.p;
+            }
+            PF_CUDA(cudaMemcpyAsync(async ? (void*)hr : (void*)out_idx, ctx->d_pidx.p, pk * 8,
+                                    cudaMemcpyDeviceToHost, s),
                     "D2H peak indices");
-            PF_CUDA(cudaMemcpyAsync(out_val, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s),
+            PF_CUDA(cudaMemcpyAsync(async ? (void*)(hr + pk * 8) : (void*)out_val, ctx->d_pval.p,
+                                    pk * 4, cudaMemcpyDeviceToHost, s),
                     "D2H peak values");
         }
+        if (async) return push_pending(ctx, j, (size_t)n_curves * n_peaks, true, s);
     } else {
         PF_CUDA(cudaMemcpyAsync(out, p.out, out_bytes, cudaMemcpyDeviceToHost, s),
                 "D2H periodogram");

@@ -187,20 +187,19 @@ class _Periodogram:
     # so is the last, whose result building nothing overlaps.
     _CHUNK_EDGES = (0.0, 0.1, 0.37, 0.64, 0.9, 1.0)
 
-    def _peaks_overlapped(self, times, mags, periods, period_dts, n_peaks, min_distance,
-                          center=False, normalize=False):
-        """'peaks' output, with the magnitudes prepared here (centre or
-        normalise).  Large batches run as a few consecutive chunks in a
-        pipeline: each chunk's native call only queues its work (PF_ASYNC)
-        and returns, so the next chunk is prepared, packed and queued while
-        the GPU runs this one, and a chunk's result objects are built while
-        the GPU runs the next.  Results are identical to one call."""
-        n = len(times)
+    @staticmethod
+    def _pipelined(times, periods, period_dts):
+        """Whether a 'peaks' batch is large enough to run in chunks."""
         points = sum(len(t) for t in times)
-        if not (n >= 64 and points * len(periods) * len(period_dts) >= 2e10):
-            mags = prepare_magnitudes(mags, center, normalize)
-            idx, val = self.peaks(times, mags, periods, period_dts, n_peaks, min_distance)
-            return unravel_peaks(idx, val, periods, period_dts, n_peaks)
+        return len(times) >= 64 and points * len(periods) * len(period_dts) >= 2e10
+
+    def _chunked_peaks(self, n, periods, period_dts, n_peaks, issue):
+        """'peaks' output of n curves as a few consecutive chunks in a
+        pipeline.  issue(ctx, a, e, idx, val) makes the native peak call for
+        curves [a, e) with PF_ASYNC: it packs and queues the chunk and
+        returns, so the next chunk is prepared, packed and queued while the
+        GPU runs this one, and a chunk's result objects are built while the
+        GPU runs the next.  Results are identical to one call."""
         n_peaks = int(n_peaks)
         if n_peaks < 0:
             raise ValueError("n_peaks must be >= 0")
@@ -212,11 +211,9 @@ class _Periodogram:
         with ctx.lock:
             def queue(k):
                 a, e = bounds[k], bounds[k + 1]
-                b = nat.CurveBatch(times[a:e], prepare_magnitudes(mags[a:e], center, normalize))
-                idx = np.full((b.n, n_peaks), -1, dtype=np.int64)
-                val = np.zeros((b.n, n_peaks), dtype=np.float32)
-                ctx.check(self._native_peaks(ctx, b, periods, period_dts, n_peaks,
-                                             int(min_distance), idx, val, nat.PF_ASYNC))
+                idx = np.full((e - a, n_peaks), -1, dtype=np.int64)
+                val = np.zeros((e - a, n_peaks), dtype=np.float32)
+                ctx.check(issue(ctx, a, e, idx, val))
                 outs.append((idx, val))
 
             collected = 0
@@ -235,6 +232,22 @@ class _Periodogram:
                 for _ in range(len(outs) - collected):
                     ctx.lib.pf_wait(ctx.handle)
         return res
+
+    def _peaks_overlapped(self, times, mags, periods, period_dts, n_peaks, min_distance,
+                          center=False, normalize=False):
+        """'peaks' output, with the magnitudes prepared here (centre or
+        normalise) per chunk of a pipelined batch (_chunked_peaks)."""
+        if not self._pipelined(times, periods, period_dts):
+            mags = prepare_magnitudes(mags, center, normalize)
+            idx, val = self.peaks(times, mags, periods, period_dts, n_peaks, min_distance)
+            return unravel_peaks(idx, val, periods, period_dts, n_peaks)
+
+        def issue(ctx, a, e, idx, val):
+            b = nat.CurveBatch(times[a:e], prepare_magnitudes(mags[a:e], center, normalize))
+            return self._native_peaks(ctx, b, periods, period_dts, idx.shape[1],
+                                      int(min_distance), idx, val, nat.PF_ASYNC)
+
+        return self._chunked_peaks(len(times), periods, period_dts, n_peaks, issue)
 
     def _stats_on_device(self, times, mags, periods, period_dts, n_stats, significance_type):
         """The 'stats' output with the statistics computed on the device
@@ -569,8 +582,19 @@ class FPW(_Periodogram):
         periods = _grid(periods, "periods")
         period_dts = _grid(period_dts, "period_dts")
         if output == "peaks":
-            idx, val = self.peaks(times, mags, periods, period_dts, n_peaks, min_distance, errs)
-            return unravel_peaks(idx, val, periods, period_dts, int(n_peaks))
+            if not self._pipelined(times, periods, period_dts):
+                idx, val = self.peaks(times, mags, periods, period_dts, n_peaks, min_distance,
+                                      errs)
+                return unravel_peaks(idx, val, periods, period_dts, int(n_peaks))
+            fn = self._peaks_fn
+
+            def issue(ctx, a, e, idx, val):
+                return self._call(ctx, getattr(ctx.lib, fn), times[a:e], mags[a:e],
+                                  None if errs is None else errs[a:e], periods, period_dts,
+                                  idx.shape[1], int(min_distance), self._flags | nat.PF_ASYNC,
+                                  nat.ptr(idx), nat.ptr(val))
+
+            return self._chunked_peaks(len(times), periods, period_dts, n_peaks, issue)
         data = self.periodograms(times, mags, periods, period_dts, errs)
         with gc_paused():
             if output == "stats":

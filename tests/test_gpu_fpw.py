@@ -156,3 +156,49 @@ def test_fpw_fast_bins_exact_on_long_baselines(gpu, oracle, semantics):
         np.testing.assert_array_equal(a, b)
         if semantics == "cpu":
             np.testing.assert_array_equal(b, oracle.fpw(ts, ms, P, D, nb, errs=es))
+
+
+def test_fpw_bls_pipelined_peaks_equal_one_call(gpu):
+    """A large 'peaks' request of FPW or BLS runs as PF_ASYNC chunks (packing
+    the next chunk and building the last one's results while the GPU runs);
+    the result equals one synchronous native call's peak for peak, with and
+    without uncertainties.  PF_ASYNC is refused on the periodogram calls
+    and after two uncollected calls."""
+    from periodfind_b200 import _native as nat
+    from periodfind_b200.gpu import unravel_peaks
+
+    rng = np.random.default_rng(12)
+    ts = [lc.uniform_times(rng, int(rng.integers(3000, 4097)), 1500.0) for _ in range(80)]
+    ms = [lc.noisy(rng, 15.0 + lc.box_eclipse(t, float(rng.uniform(0.5, 10)), depth=0.3,
+                                               duty=0.05), 0.05) for t in ts]
+    es = [rng.uniform(0.02, 0.3, len(t)).astype(np.float32) for t in ts]
+    P = np.exp(np.linspace(np.log(0.2), np.log(60.0), 45000)).astype(np.float32)
+    D = np.array([0.0, 1e-6], np.float32)
+    assert gpu.FPW._pipelined(ts, P, D)
+    for obj in (gpu.FPW(10), gpu.BoxLeastSquares(30, 0.02, 0.3)):
+        for e in (es, None):
+            got = obj.calc(ts, ms, P, D, errs=e, output="peaks", n_peaks=8, min_distance=3)
+            idx, val = obj.peaks(ts, ms, P, D, 8, 3, errs=e)
+            want = unravel_peaks(idx, val, P, D, 8)
+            assert len(got) == len(want) == len(ts)
+            for g, w in zip(got, want):
+                assert [(s.params, s.value) for s in g] == [(s.params, s.value) for s in w]
+    ctx = nat.default_context(0)
+    obj = gpu.FPW(10)
+    out = np.empty((2, 50, 1), np.float32)
+    P2, Z = np.linspace(1.0, 5.0, 50).astype(np.float32), np.zeros(1, np.float32)
+    with ctx.lock:
+        assert obj._call(ctx, ctx.lib.pf_fpw, ts[:2], ms[:2], None, P2, Z,
+                         obj._flags | nat.PF_ASYNC, nat.ptr(out)) == nat.PF_EINVAL
+        idx = np.full((2, 4), -1, np.int64)
+        val = np.zeros((2, 4), np.float32)
+        for _ in range(2):
+            assert obj._call(ctx, ctx.lib.pf_fpw_peaks, ts[:2], ms[:2], None, P2, Z, 4, 1,
+                             obj._flags | nat.PF_ASYNC, nat.ptr(idx), nat.ptr(val)) == nat.PF_OK
+        assert obj._call(ctx, ctx.lib.pf_fpw_peaks, ts[:2], ms[:2], None, P2, Z, 4, 1,
+                         obj._flags | nat.PF_ASYNC, nat.ptr(idx), nat.ptr(val)) == nat.PF_EINVAL
+        for _ in range(2):
+            ctx.check(ctx.lib.pf_wait(ctx.handle))
+    want_idx, want_val = obj.peaks(ts[:2], ms[:2], P2, Z, 4, 1)
+    np.testing.assert_array_equal(idx, want_idx)
+    np.testing.assert_array_equal(val, want_val)
