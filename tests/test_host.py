@@ -261,3 +261,67 @@ def test_curve_pointers_address_the_curves():
         np.testing.assert_array_equal(read(bc.mptr[0], sizes[0]), norm[0])
     with pytest.raises(ValueError):
         nat.CurveBatch([np.zeros(3, np.float32)], [np.zeros(4, np.float32)])
+
+
+def test_chunked_peaks_pipeline_order_and_error_cleanup(monkeypatch):
+    """The 'peaks' pipeline (gpu._Periodogram._chunked_peaks) against a fake
+    context: chunks cover the curves in order, at most two calls are
+    pending when one is collected, results come back in curve order, and a
+    failing call still has every queued call collected, so the context is
+    left with nothing pending."""
+    import threading
+
+    from periodfind_b200 import gpu
+
+    class FakeLib:
+        def __init__(self, ctx):
+            self.ctx = ctx
+
+        def pf_wait(self, handle):
+            assert self.ctx.pending > 0
+            self.ctx.pending -= 1
+            return 0
+
+    class FakeCtx:
+        lock = threading.Lock()
+        handle = None
+
+        def __init__(self):
+            self.pending = 0
+            self.max_pending = 0
+            self.lib = FakeLib(self)
+
+        def check(self, rc):
+            if rc != 0:
+                raise RuntimeError(f"native call failed: {rc}")
+            return rc
+
+    ctx = FakeCtx()
+    monkeypatch.setattr(gpu.nat, "default_context", lambda device=0: ctx)
+    P = np.linspace(1.0, 2.0, 5).astype(np.float32)
+    D = np.zeros(1, np.float32)
+    chunks = []
+
+    def issue(c, a, e, idx, val, fail_at=None):
+        if fail_at is not None and len(chunks) == fail_at:
+            return -2
+        chunks.append((a, e))
+        c.pending += 1
+        c.max_pending = max(c.max_pending, c.pending)
+        idx[:, 0] = np.arange(a, e) % len(P)  # peak k of curve i at cell i mod 5
+        val[:, 0] = np.arange(a, e)
+        return 0
+
+    obj = gpu.AOV()
+    res = obj._chunked_peaks(200, P, D, 1, issue)
+    assert chunks[0][0] == 0 and chunks[-1][1] == 200
+    assert all(x[1] == y[0] for x, y in zip(chunks, chunks[1:]))
+    assert ctx.pending == 0 and ctx.max_pending == 2
+    assert [r[0].value for r in res] == list(range(200))
+    assert [r[0].params[0] for r in res] == [P[i % 5] for i in range(200)]
+    chunks.clear()
+    with pytest.raises(RuntimeError):
+        obj._chunked_peaks(200, P, D, 1, lambda *a: issue(*a, fail_at=3))
+    assert len(chunks) == 3 and ctx.pending == 0
+    with pytest.raises(ValueError):
+        obj._chunked_peaks(200, P, D, -1, issue)
