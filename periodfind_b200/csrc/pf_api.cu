@@ -771,6 +771,30 @@ int push_pending(pf_ctx* ctx, const Job& j, size_t n, bool work, cudaStream_t s)
     return PF_OK;
 }
 
+// Copy a peak call's results (d_pidx / d_pval, n_curves x n_peaks) back:
+// into the caller's arrays, or with PF_ASYNC into the next pending slot's
+// pinned block (free: its last user was collected, so no copy into it is
+// in flight) and register the call for pf_wait.
+int copy_peaks_back(pf_ctx* ctx, const Job& j, bool async, cudaStream_t s) {
+    const size_t pk = (size_t)j.n_curves * j.n_peaks;
+    void* hi = j.out_idx;
+    void* hv = j.out_val;
+    if (async && pk > 0) {
+        pf_ctx::Pending& q = ctx->pend[(ctx->pend_head + ctx->pend_count) % pf_ctx::kMaxPending];
+        const int rc = ensure_pinned(ctx, q.res, pk * 12);
+        if (rc != PF_OK) return rc;
+        hi = q.res.p;
+        hv = (char*)q.res.p + pk * 8;
+    }
+    if (pk > 0) {
+        PF_CUDA(cudaMemcpyAsync(hi, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
+                "D2H peak indices");
+        PF_CUDA(cudaMemcpyAsync(hv, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s),
+                "D2H peak values");
+    }
+    return async ? push_pending(ctx, j, pk, true, s) : PF_OK;
+}
+
 // The whole pipeline for host-pointer inputs.
 int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* const* mags,
              const uint64_t* lengths) {
@@ -863,30 +887,11 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
     } else if (!j.peaks) {
         PF_CUDA(cudaMemcpyAsync(j.out, ctx->d_out.p, out_bytes, cudaMemcpyDeviceToHost, s),
                 "D2H periodogram");
-    } else if (j.n_peaks > 0 && !async) {
-        const size_t pk = (size_t)j.n_curves * j.n_peaks;
-        PF_CUDA(cudaMemcpyAsync(j.out_idx, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
-                "D2H peak indices");
-        PF_CUDA(cudaMemcpyAsync(j.out_val, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s),
-                "D2H peak values");
-    }
-    if (async) {
-        // The peaks go to this call's pinned block (a free slot: its last
-        // user was collected, so no copy into it is in flight), and the
-        // call returns with its work queued.  The staging block stays
-        // marked in use until the H2D copy above has finished.
-        const size_t pk = (size_t)j.n_curves * j.n_peaks;
-        if (pk > 0) {
-            pf_ctx::Pending& q =
-                ctx->pend[(ctx->pend_head + ctx->pend_count) % pf_ctx::kMaxPending];
-            if ((rc = ensure_pinned(ctx, q.res, pk * 12)) != PF_OK) return rc;
-            char* hr = (char*)q.res.p;
-            PF_CUDA(cudaMemcpyAsync(hr, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
-                    "D2H peak indices");
-            PF_CUDA(cudaMemcpyAsync(hr + pk * 8, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s),
-                    "D2H peak values");
-        }
-        return push_pending(ctx, j, pk, true, s);
+    } else {
+        if ((rc = copy_peaks_back(ctx, j, async, s)) != PF_OK) return rc;
+        // PF_ASYNC: the call returns with its work queued.  The staging
+        // block stays marked in use until the H2D copy above has finished.
+        if (async) return PF_OK;
     }
     PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
     ctx->staged_pending = false;
@@ -1173,23 +1178,9 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
                                  (int64_t*)ctx->d_pidx.p, (float*)ctx->d_pval.p, s),
                     "peak search launch");
             ctx->launches++;
-            // PF_ASYNC: into this call's pending slot (free: its last user
-            // was collected), copied out by pf_wait.
-            char* hr = nullptr;
-            if (async) {
-                pf_ctx::Pending& q =
-                    ctx->pend[(ctx->pend_head + ctx->pend_count) % pf_ctx::kMaxPending];
-                if ((rc = ensure_pinned(ctx, q.res, pk * 12)) != PF_OK) return rc;
-                hr = (char*)q.res.p;
-            }
-            PF_CUDA(cudaMemcpyAsync(async ? (void*)hr : (void*)out_idx, ctx->d_pidx.p, pk * 8,
-                                    cudaMemcpyDeviceToHost, s),
-                    "D2H peak indices");
-            PF_CUDA(cudaMemcpyAsync(async ? (void*)(hr + pk * 8) : (void*)out_val, ctx->d_pval.p,
-                                    pk * 4, cudaMemcpyDeviceToHost, s),
-                    "D2H peak values");
         }
-        if (async) return push_pending(ctx, j, (size_t)n_curves * n_peaks, true, s);
+        if ((rc = copy_peaks_back(ctx, j, async, s)) != PF_OK) return rc;
+        if (async) return PF_OK;
     } else {
         PF_CUDA(cudaMemcpyAsync(out, p.out, out_bytes, cudaMemcpyDeviceToHost, s),
                 "D2H periodogram");
