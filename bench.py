@@ -56,7 +56,7 @@ METRIC = "curve*period*point evals/s on 1 B200, chosen vs plain, at stated error
 def make_workload(n_curves=N_CURVES, seed=SEED):
     from tests import lightcurves as lc
 
-    ts, ms = lc.batch_config2(n_curves, N_POINTS, seed)
+    ts, ms = lc.mixed_signal_batch(n_curves, N_POINTS, seed)
     periods = np.exp(np.linspace(np.log(0.1), np.log(100.0), N_PERIODS)).astype(np.float32)
     pdts = np.array(PDTS, np.float32)
     return ts, ms, periods, pdts

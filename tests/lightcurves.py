@@ -85,7 +85,7 @@ def center(m):
     return m - np.mean(m)
 
 
-def batch_config2(n_curves, n_points, seed, t_span=2000.0):
+def mixed_signal_batch(n_curves, n_points, seed, t_span=2000.0):
     """Curves shaped like the 1000 x 4096 benchmark batch: half sinusoids,
     a quarter sawtooth, a quarter box eclipses (depth 0.5, duty 0.05),
     N(0, 0.05^2) noise, periods log-uniform in [0.1, 100] days."""

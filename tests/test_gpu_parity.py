@@ -155,7 +155,7 @@ def test_bin_kernel_occupancy_exact_at_scale(gpu, pdts):
     histograms, including long baselines (MJD-like times, short periods)."""
     from tests import lightcurves as lc2
 
-    ts, ms = lc2.batch_config2(48, 4096, 1234)
+    ts, ms = lc2.mixed_signal_batch(48, 4096, 1234)
     rng = np.random.default_rng(5)
     for k in range(8):  # long-baseline curves: t ~ 5.9e4 days
         t = np.sort(rng.uniform(58000.0, 60000.0, 4096)).astype(np.float32)
