@@ -929,8 +929,9 @@ def main():
 # path: t * RN(1/P) (DMUL), floor (DADD.RD), bin with fraction bits
 # (DFMA.RD), plus DMUL + DFMA for t - c t^2 on the period-derivative cells.
 FP64_OPS_PER_EVAL = 3 + 2 * sum(1 for d in PDTS if d != 0.0) / len(PDTS)
-# DRAM bytes (read + write) of one full-size CE bin_kernel launch, from the
-# ncu capture summarised in profiles/bin_kernel_ce_aov_10x4096.md.
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
+# full-size CE bin_kernel launch (1000 curves x 4096 points x 2e4 cells),
+# from one ncu capture of this benchmark.
 CE_TRAFFIC_BYTES = 52514048 + 28131328
 
 if __name__ == "__main__":
