@@ -8,9 +8,12 @@
 //
 // Decomposition: a CTA per (curve, period derivative, tile of BLOCK trial
 // periods); thread j owns one period for the whole curve and keeps its own
-// V and Y in shared memory ([bin][thread], so a warp's updates hit 32
-// banks), adding the points in curve order -- the Rust path's order, so the
-// sums round as it does.  The curve streams through shared memory in tiles.
+// V and Y in shared memory ([bin][thread], so a warp's updates touch
+// consecutive words: the chosen form as (V, Y) float2 pairs, one 8-byte
+// access per update; the plain form as V rows then Y rows), adding the
+// points in curve order -- the Rust path's order, so the sums round as it
+// does.  The curve streams through shared memory in 16-byte point records,
+// 256 points per tile.
 //
 // The bin is the reference's for the unit's semantics:
 //   CUDA build: (size_t)(folded / bin_size), clamped to n_bins - 1
