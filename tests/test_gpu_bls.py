@@ -146,3 +146,23 @@ def test_bls_detects_eclipsing_binary(gpu, errs):
     r = gpu.BoxLeastSquares(50, 0.01, 0.3).calc([t], [m], P, np.zeros(1, np.float32), errs=e)
     best = float(r[0].params[0])
     assert any(abs(best - c) / c < 0.05 for c in (2.5, 1.25, 5.0)), best
+
+
+@pytest.mark.parametrize("mode", ["plain", "chosen"])
+def test_bls_degenerate_windows_score_zero(gpu, oracle, mode):
+    """No admissible window: one bin, qmin above qmax, an empty curve, a
+    single point.  In the Rust path's arithmetic those cells are 0, as the
+    oracle's (rust/src/bls.rs:51-52, 93-120)."""
+    rng = np.random.default_rng(9)
+    t = lc.uniform_times(rng, 300, 100.0)
+    m = lc.noisy(rng, lc.box_eclipse(t, 3.1, depth=0.3) + 15.0, 0.02)
+    P = lc.trial_periods(3.1, n=30)
+    D = np.array([0.0, 1e-4], np.float32)
+    e0 = np.zeros(0, np.float32)
+    ts, ms = [e0, t[:1].copy(), t], [e0, m[:1].copy(), m]
+    for nb, qmin, qmax in ((1, 0.01, 0.5), (50, 0.5, 0.1), (20, 0.05, 0.5)):
+        got = gpu.BoxLeastSquares(nb, qmin, qmax, mode=mode, semantics="cpu").periodograms(
+            ts, ms, P, D)
+        want = oracle.bls(ts, ms, P, D, nb, qmin, qmax)
+        np.testing.assert_array_equal(got, want)
+        assert not got[0].any() and not got[1].any()

@@ -256,3 +256,21 @@ def test_bls_known_period(oracle, case):
     best = float(P[int(np.argmax(pg))])
     assert any(abs(best - c) / c < 0.05 for c in (case["period"], case["period"] / 2,
                                                   case["period"] * 2)), best
+
+
+def test_bls_degenerate_windows_score_zero(oracle):
+    """BLS cells with no admissible window score 0 (rust/src/bls.rs:51-52,
+    93-120): one bin (no width between 1 and n_bins - 1), qmin above qmax,
+    an empty curve (no weight), and a single point (every window holds all
+    of the weight or none of it)."""
+    rng = np.random.default_rng(9)
+    t = lc.uniform_times(rng, 300, 100.0)
+    m = lc.noisy(rng, lc.box_eclipse(t, 3.1, depth=0.3) + 15.0, 0.02)
+    P = lc.trial_periods(3.1, n=30)
+    D = np.zeros(1, np.float32)
+    assert not oracle.bls([t], [m], P, D, 1, 0.01, 0.5).any()
+    assert not oracle.bls([t], [m], P, D, 50, 0.5, 0.1).any()
+    e0 = np.zeros(0, np.float32)
+    one_t, one_m = t[:1].copy(), m[:1].copy()
+    out = oracle.bls([e0, one_t, t], [e0, one_m, m], P, D, 20, 0.05, 0.5)
+    assert not out[0].any() and not out[1].any() and out[2].max() > 0
