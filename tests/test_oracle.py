@@ -161,6 +161,25 @@ def test_fpw_matches_numpy_restatement(oracle):
         np.testing.assert_allclose(got, want, rtol=2e-5)
 
 
+def test_fpw_one_bin_and_empty_curve(oracle):
+    """One phase bin holds every point: the value is (sum w m)^2 / (2 sum w)
+    at every trial period (rust/src/fpw.rs:46-63); an empty curve has no
+    non-empty bin and scores 0."""
+    rng = np.random.default_rng(4)
+    t = lc.uniform_times(rng, 400, 100.0)
+    m = lc.noisy(rng, lc.sinusoid(t, 2.2, amp=0.3, offset=15.0), 0.05)
+    e = rng.uniform(0.05, 0.2, 400).astype(np.float32)
+    P = lc.trial_periods(2.2, n=25)
+    D = np.array([0.0, 1e-4], np.float32)
+    got = oracle.fpw([t, np.zeros(0, np.float32)], [m, np.zeros(0, np.float32)], P, D, 1,
+                     errs=[e, np.zeros(0, np.float32)])
+    w = 1.0 / e.astype(np.float64) ** 2
+    want = np.sum(w * m) ** 2 / (2.0 * np.sum(w))
+    np.testing.assert_allclose(got[0], want, rtol=1e-5)
+    assert np.all(got[0] == got[0, 0, 0])
+    assert not got[1].any()
+
+
 @pytest.mark.parametrize("case", [
     dict(period=5.0, n=800, noise=0.02, span=200.0, n_bins=20, errs=None),
     dict(period=3.0, n=600, noise=0.05, span=150.0, n_bins=15, errs="const"),
