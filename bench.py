@@ -1,35 +1,52 @@
 """Benchmark: curve x period x point evaluations per second on B200.
 
-Workload (one "step"): Conditional Entropy (10 x 10 bins) and AOV (15 bins)
-periodograms plus the top-32 peak search, over 1000 light curves x 4096
-points, 10000 trial periods log-spaced in [0.1, 100] days and period
-derivatives [0, 1e-6] -- 2 x 8.19e10 evaluations per step.  Synthetic
-curves (seeded): half sinusoids, a quarter sawtooth, a quarter box eclipses
-(depth 0.5, duty 0.05) with N(0, 0.05^2) noise, times uniform over 2000 days.
+Default workload (one "step"): the mixed ragged batch -- 100 000 light
+curves with lengths lognormal (median 300, sigma 0.8) clipped to [20, 2000]
+(4.07e7 points), seasonal cadence over 2500 days, a third sinusoids, a third
+box eclipses, a third pure noise -- searched by Conditional Entropy (10 x 10
+bins), AOV (15 bins) and Lomb-Scargle over 20 000 log-spaced trial periods
+in [0.05, 500] days (one period derivative, 0), each followed by the top-32
+peak search: 3 x 8.14e11 evaluations per step.  Seeded synthetic curves with
+the configuration's shapes (no public dataset is named by the reference).
 
 Reported (one JSON line on rank 0):
-  value     evals/s of the chosen form, inputs resident in HBM, device-timed
-            with CUDA events around each step (max over ranks); L2 is
-            flushed (256 MB write) between timed steps, outside the events.
-  e2e       the same metric through the public API (gpu.ConditionalEntropy /
-            gpu.AOV .calc(..., output='peaks')) with host numpy inputs: the
-            timed region includes magnitude preparation, the H2D copy of the
-            step's inputs and the D2H copy of the peaks.
-  plain     the plain form (the reference's fold, op for op) on the same
-            device-resident workload, for the chosen-vs-plain ratio.
-  roofline  the dominant fold kernel against the measured FP64-pipe peak
-            (this path is FP64/XU issue bound; HBM traffic is given too).
-  cpu_baseline  the oracle (C/OpenMP restatement of the reference's Rust
-            CPU path) on all host cores over a bounded sample of curves.
+  value       evals/s of the chosen form: per step, the magnitudes are
+              prepared on the device (CE normalised, LS centred, numpy's
+              values) and the three batch plans (CUDA graphs of the queue
+              kernels per length class + peak search) are replayed; inputs
+              resident in HBM, CUDA events around each step, max over ranks.
+  plain       the same step with the plain form (the reference's fold op for
+              op, one launch per algorithm) and its ratio chosen / plain.
+  e2e         the same metric through the C ABI with host buffers: per step
+              host magnitude preparation, pf_{ce,aov,ls}_peaks from per-curve
+              host arrays (H2D copy of every curve inside each call), peaks
+              back to host memory; the calls are pipelined (PF_ASYNC).
+  e2e_calc    once per algorithm, the public Python path
+              calc(list of numpy, output='peaks'), which also builds the
+              3.2e6 result objects per algorithm.
+  latency     per-curve device latency p50 / p99 (PF_TIMING stamps), chosen
+              and plain.
+  roofline    the kernel with the most time in the step, against the
+              measured rate of the pipe that bounds it (pipe_peaks.cu probe).
+  ls_peak_frequency_error  Newton-refined LS peaks of the chosen form on a
+              sample of curves, checked by one FP64 Newton step.
+  cpu_baseline / reference_cuda  the C/OpenMP restatement of the reference's
+              Rust CPU path on the host cores, and the reference's own CUDA
+              drivers built from its sources, each on a stated curve sample.
+  batch_4096  secondary: CE(10x10) + AOV(15) + peaks over 1000 curves x 4096
+              points x 10000 periods x pdts [0, 1e-6], chosen vs plain.
 
---impl reference runs that CPU restatement (the reference's CPU
-implementation is Rust; no Rust toolchain exists on these machines) as the
-reference arm, on rank 0 only.
+--impl reference runs the CPU restatement of the reference's path (the
+reference's CPU implementation is Rust; no Rust toolchain exists on these
+machines) as the reference arm, on rank 0 only.  --workload selects the
+separate reports of the other configurations (bench_reports.py).
 """
 
 from __future__ import annotations
 
 import argparse
+import contextlib
+import ctypes
 import json
 import os
 import statistics
@@ -43,38 +60,49 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+import lightcurves as lc  # noqa: E402
+
+METRIC = "curve*period*point evals/s on 1 B200, chosen vs plain, at stated error"
+SEED = 20261205
+N_PEAKS = 32
+ALGOS = ("ce", "aov", "ls")
+
+# The mixed ragged batch.
+RAGGED_CURVES = 100000
+RAGGED_PERIODS = 20000
+RAGGED_WORKLOAD = ("mixed ragged batch: 100000 curves, lengths lognormal(median 300, sigma 0.8) "
+                   "clipped to [20, 2000], seasonal cadence 2500 d, 1/3 sinusoid, 1/3 box "
+                   "eclipse, 1/3 noise; CE(10x10) + AOV(15) + LS over 20000 log periods "
+                   "[0.05, 500] d, period_dts [0], top-32 peaks each")
+
+# The 1000 x 4096 batch (secondary line; --workload batch / fpw / bls / device).
 N_CURVES = 1000
 N_POINTS = 4096
 N_PERIODS = 10000
 PDTS = (0.0, 1e-6)
-N_PEAKS = 32
-SEED = 20261205
-WORKLOAD = "CE(10x10)+AOV(15)+top32 peaks, 1000 curves x 4096 pts, 10000 log periods [0.1,100] d x pdts [0,1e-6]"
-METRIC = "curve*period*point evals/s on 1 B200, chosen vs plain, at stated error"
+
+
+def ragged_grid():
+    periods = np.exp(np.linspace(np.log(0.05), np.log(500.0), RAGGED_PERIODS)).astype(np.float32)
+    return periods, np.zeros(1, np.float32)
 
 
 def make_workload(n_curves=N_CURVES, seed=SEED):
-    from tests import lightcurves as lc
-
     ts, ms = lc.mixed_signal_batch(n_curves, N_POINTS, seed)
     periods = np.exp(np.linspace(np.log(0.1), np.log(100.0), N_PERIODS)).astype(np.float32)
-    pdts = np.array(PDTS, np.float32)
-    return ts, ms, periods, pdts
-
-
-def evals_per_step(n_curves):
-    return 2 * n_curves * N_POINTS * N_PERIODS * len(PDTS)
+    return ts, ms, periods, np.array(PDTS, np.float32)
 
 
 # ----------------------------------------------------------------- clocks
 
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) while the timed region runs."""
+    """nvidia-smi samples (200 ms) while a timed region runs."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device_index):
         self.idx = device_index
@@ -90,9 +118,10 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (FileNotFoundError, OSError):
             self.proc = None
-            return
+            return self
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        return self
 
     def _read(self):
         for line in self.proc.stdout:
@@ -100,7 +129,8 @@ class ClockSampler:
 
     def stop(self):
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"],
+                    "samples": 0}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -108,33 +138,65 @@ class ClockSampler:
             self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
-        mhz, mx, reasons, power = [], None, set(), []
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                mhz.append(float(parts[1]))
-                mx = float(parts[2])
-                power.append(float(parts[3]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(mhz),
-                "power_w_max": max(power) if power else None}
+        return summarise_clocks(self.lines)
+
+
+def summarise_clocks(lines):
+    """Median SM clock, max clock, throttle reasons seen active, samples."""
+    mhz, mx, reasons, power = [], None, set(), []
+    for ln in lines:
+        parts = [p.strip() for p in ln.split(",")]
+        if len(parts) < 9:
+            continue
+        try:
+            mhz.append(float(parts[1]))
+            mx = float(parts[2])
+            power.append(float(parts[3]))
+        except ValueError:
+            continue
+        for nm, v in zip(ClockSampler.REASONS, parts[5:9]):
+            if v.lower() == "active":
+                reasons.add(nm)
+    return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+            "reasons": sorted(reasons), "samples": len(mhz),
+            "power_w_max": max(power) if power else None}
+
+
+class Clocks:
+    """A clock record per timed region (one nvidia-smi sampler each) and
+    their union."""
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.regions = {}
+        self._lines = []
+
+    @contextlib.contextmanager
+    def region(self, name):
+        s = ClockSampler(self.idx).start()
+        try:
+            yield
+        finally:
+            self.regions[name] = s.stop()
+            self._lines.extend(s.lines)
+
+    def union(self):
+        return summarise_clocks(self._lines)
 
 
 # -------------------------------------------------------------- pipe peaks
 
 
 def measure_pipes():
-    import ctypes
+    """Per-pipe throughput measured now on this GPU (pipe_peaks.cu beside
+    this file, built on first use): the roofline denominators."""
+    so = os.path.join(ROOT, "pipe_peaks.so")
+    src = os.path.join(ROOT, "pipe_peaks.cu")
+    if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        from periodfind_b200.build import ARCH, COMMON, nvcc
 
-    lib = ctypes.CDLL(os.path.join(ROOT, "periodfind_b200", "libpfpeaks.so"))
+        subprocess.run([nvcc()] + COMMON + ARCH + ["-shared", "-o", so, src], check=True)
+    lib = ctypes.CDLL(so)
 
     class R(ctypes.Structure):
         _fields_ = [("name", ctypes.c_char * 32), ("ops_per_clk_per_sm", ctypes.c_double),
@@ -147,689 +209,536 @@ def measure_pipes():
                                    "mhz": arr[i].sm_mhz} for i in range(max(k, 0))}
 
 
-# ----------------------------------------------------------- device step
+# The pipe that bounds each kernel of the ragged step, and its algorithmic
+# operations per evaluation (no period derivative):
+#   CE bin kernel   FP64: t * RN(1/P) (DMUL), floor (DADD.RD), bin with
+#                   fraction bits (DFMA.RD); one shared reduction.
+#   AOV bin kernel  two shared reductions (count, fixed-point sum); 3 FP64.
+#   LS fold kernel  MUFU sine and cosine.
+ROOFLINE = {
+    "ce": {"kernel": "bin_kernel<CE> (chosen)", "bound": "fp64", "pipe": "dfma", "ops": 3.0,
+           "views": {"shared_atomic": ("atoms_u32_private", 1.0)}},
+    "aov": {"kernel": "bin_kernel<AOV> (chosen)", "bound": "shared-atomic",
+            "pipe": "atoms_u32_private", "ops": 2.0, "views": {"fp64": ("dfma", 3.0)}},
+    "ls": {"kernel": "fold_kernel<LS, split-precision> (chosen)", "bound": "mufu",
+           "pipe": "mufu_sin+cos", "ops": 2.0, "views": {}},
+}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the class
+# kernels of one algorithm over the whole ragged batch, from one ncu capture
+# of a curve sample of the batch scaled by its evaluations (the traffic is
+# the curve points and the periodogram, both proportional).  None where no
+# capture has been made.
+RAGGED_TRAFFIC = {"ce": None, "aov": None, "ls": None}
 
 
-class DeviceStep:
-    """CE + AOV + peaks on device-resident packed curves via the C ABI."""
+# ------------------------------------------------------------ ragged step
 
-    def __init__(self, ts, ms, periods, pdts, mode_flags, torch, device=0):
+
+class RaggedStep:
+    """The ragged batch resident on the device, its three batch plans
+    (chosen) and the plain form's direct calls, on the current stream."""
+
+    def __init__(self, t, m, off, periods, pdts, torch, device):
         from periodfind_b200 import _native as nat
-        from tests import lightcurves as lc
+        from periodfind_b200.plan import BatchPlan
 
-        self.nat = nat
-        self.torch = torch
-        self.ctx = nat.default_context(device)
-        self.flags = mode_flags
-        off = np.zeros(len(ts) + 1, np.int64)
-        np.cumsum([len(t) for t in ts], out=off[1:])
-        self.off = off
-        dev = "cuda"
-        self.t = torch.from_numpy(np.concatenate(ts)).to(dev)
-        self.m_ce = torch.from_numpy(np.concatenate([lc.normalize(m) for m in ms])).to(dev)
-        self.m_aov = torch.from_numpy(np.concatenate(ms)).to(dev)
-        self.P = torch.from_numpy(periods).to(dev)
-        self.D = torch.from_numpy(pdts).to(dev)
-        n = len(ts)
-        self.n = n
-        cells = len(periods) * len(pdts)
-        self.cells = cells
-        self.pg_ce = torch.empty((n, cells), dtype=torch.float32, device=dev)
-        self.pg_aov = torch.empty((n, cells), dtype=torch.float32, device=dev)
-        self.pk_idx = torch.empty((2, n, N_PEAKS), dtype=torch.int64, device=dev)
-        self.pk_val = torch.empty((2, n, N_PEAKS), dtype=torch.float32, device=dev)
-        self.np_ = len(periods)
-        self.nd = len(pdts)
+        self.nat, self.torch = nat, torch
+        self.off = np.ascontiguousarray(off, np.int64)
+        self.n = len(off) - 1
+        dev = torch.device("cuda", device)
+        self.d_t = torch.from_numpy(t).to(dev)
+        self.d_m = torch.from_numpy(m).to(dev)
+        self.mags = {"ce": torch.empty_like(self.d_m), "aov": self.d_m,
+                     "ls": torch.empty_like(self.d_m)}
+        self.d_p = torch.from_numpy(periods).to(dev)
+        self.d_d = torch.from_numpy(pdts).to(dev)
+        self.n_per, self.n_pdt = len(periods), len(pdts)
+        self.cells = self.n_per * self.n_pdt
+        self.pg = torch.empty((self.n, self.cells), dtype=torch.float32, device=dev)
+        self.pk_i = torch.empty((3, self.n, N_PEAKS), dtype=torch.int64, device=dev)
+        self.pk_v = torch.empty((3, self.n, N_PEAKS), dtype=torch.float32, device=dev)
+        # Magnitude preparation and the plain calls each on a context of
+        # their own (a context serialises the reuse of its offsets copy).
+        self.prep_ctx = {k: nat.Context(device) for k in ("ce", "ls")}
+        self.ctx = nat.Context(device)
+        self.stream = torch.cuda.current_stream(dev)
+        self.s = self.stream.cuda_stream
+        self.prepare()
+        self.plans = {}
+        for k, algo in enumerate(ALGOS):
+            self.plans[algo] = BatchPlan(
+                algo, self.d_t, self.mags[algo], self.off, self.d_p, self.d_d, self.pg,
+                n_phase=10 if algo == "ce" else 15, n_mag=10, flags=nat.PF_MODE_CHOSEN,
+                n_peaks=N_PEAKS, peak_idx=self.pk_i[k], peak_val=self.pk_v[k], device=device)
+        self.plan_kernels = sum(int(nat.load().pf_plan_kernel_count(p.handle))
+                                for p in self.plans.values())
 
-    def run(self, stream):
-        c, lib, h, nat = self.ctx, self.ctx.lib, self.ctx.handle, self.nat
-        c.check(lib.pf_ce_dev(h, self.t.data_ptr(), self.m_ce.data_ptr(), self.off.ctypes.data,
-                              self.n, self.P.data_ptr(), self.np_, self.D.data_ptr(), self.nd,
-                              10, 10, 1, 1, self.flags, self.pg_ce.data_ptr(), stream))
-        c.check(lib.pf_find_peaks_dev(h, self.pg_ce.data_ptr(), self.n, self.cells, N_PEAKS, 1,
-                                      0, self.pk_idx[0].data_ptr(), self.pk_val[0].data_ptr(),
-                                      stream))
-        c.check(lib.pf_aov_dev(h, self.t.data_ptr(), self.m_aov.data_ptr(), self.off.ctypes.data,
-                               self.n, self.P.data_ptr(), self.np_, self.D.data_ptr(), self.nd,
-                               15, 1, self.flags, self.pg_aov.data_ptr(), stream))
-        c.check(lib.pf_find_peaks_dev(h, self.pg_aov.data_ptr(), self.n, self.cells, N_PEAKS, 1,
-                                      1, self.pk_idx[1].data_ptr(), self.pk_val[1].data_ptr(),
-                                      stream))
+    def prepare(self):
+        nat = self.nat
+        for algo, kind in (("ce", nat.PF_PREP_NORMALIZE), ("ls", nat.PF_PREP_CENTER)):
+            c = self.prep_ctx[algo]
+            c.check(c.lib.pf_prepare_mags_dev(c.handle, self.d_m.data_ptr(), self.off.ctypes.data,
+                                              self.n, kind, self.mags[algo].data_ptr(), self.s))
+
+    def chosen(self):
+        self.prepare()
+        for algo in ALGOS:
+            self.plans[algo].launch(self.stream)
+
+    def direct(self, algo, flags, peaks=True):
+        c, lib, h = self.ctx, self.ctx.lib, self.ctx.handle
+        common = (h, self.d_t.data_ptr(), self.mags[algo].data_ptr(), self.off.ctypes.data,
+                  self.n, self.d_p.data_ptr(), self.n_per, self.d_d.data_ptr(), self.n_pdt)
+        if algo == "ce":
+            c.check(lib.pf_ce_dev(*common, 10, 10, 1, 1, flags, self.pg.data_ptr(), self.s))
+        elif algo == "aov":
+            c.check(lib.pf_aov_dev(*common, 15, 1, flags, self.pg.data_ptr(), self.s))
+        else:
+            c.check(lib.pf_ls_dev(*common, flags, self.pg.data_ptr(), self.s))
+        if peaks:
+            k = ALGOS.index(algo)
+            c.check(lib.pf_find_peaks_dev(h, self.pg.data_ptr(), self.n, self.cells, N_PEAKS, 1,
+                                          0 if algo == "ce" else 1, self.pk_i[k].data_ptr(),
+                                          self.pk_v[k].data_ptr(), self.s))
+
+    def plain(self):
+        self.prepare()
+        for algo in ALGOS:
+            self.direct(algo, self.nat.PF_MODE_PLAIN)
+
+    def close(self):
+        for p in self.plans.values():
+            p.close()
 
 
-def time_device(step, steps, warmup, torch, flush):
-    stream = torch.cuda.current_stream()
-    s = stream.cuda_stream
+def time_steps(fn, steps, warmup, torch, flush, stream):
+    """Mean CUDA-event time (ms) of `steps` calls of fn after `warmup`
+    untimed ones; L2 flushed (a 256 MB write) before each timed call,
+    outside the events."""
     for _ in range(warmup):
-        step.run(s)
+        fn()
     torch.cuda.synchronize()
-    launches0 = step.ctx.launches
-    total = 0.0
+    per = []
     for _ in range(steps):
-        flush.zero_()  # evict L2 between timed steps (outside the events)
+        flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        step.run(s)
+        fn()
         e1.record(stream)
         e1.synchronize()
-        total += e0.elapsed_time(e1)
+        per.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
-    return total / steps, step.ctx.launches - launches0
+    return float(np.mean(per)), per
 
 
-def time_kernels(step, torch, reps=3):
-    """Average duration of the CE and AOV fold kernels (their own events)."""
-    s = torch.cuda.current_stream().cuda_stream
-    ce, aov = [], []
-    c, lib, h = step.ctx, step.ctx.lib, step.ctx.handle
-    for _ in range(reps):
-        c.check(lib.pf_ce_dev(h, step.t.data_ptr(), step.m_ce.data_ptr(), step.off.ctypes.data,
-                              step.n, step.P.data_ptr(), step.np_, step.D.data_ptr(), step.nd,
-                              10, 10, 1, 1, step.flags, step.pg_ce.data_ptr(), s))
-        torch.cuda.synchronize()
-        ce.append(c.last_kernel_ms)
-        c.check(lib.pf_aov_dev(h, step.t.data_ptr(), step.m_aov.data_ptr(), step.off.ctypes.data,
-                               step.n, step.P.data_ptr(), step.np_, step.D.data_ptr(), step.nd,
-                               15, 1, step.flags, step.pg_aov.data_ptr(), s))
-        torch.cuda.synchronize()
-        aov.append(c.last_kernel_ms)
-    return float(np.mean(ce)), float(np.mean(aov))
+def curve_latency(step, algo, flags):
+    """Per-curve device latency (ms) of one stamped direct call: last end
+    minus first start of the CTAs that computed the curve."""
+    nat = step.nat
+    step.direct(algo, flags | nat.PF_TIMING, peaks=False)
+    lat = np.zeros(step.n)
+    step.ctx.check(step.ctx.lib.pf_curve_latency(step.ctx.handle, step.n, lat.ctypes.data))
+    return {"p50_ms": float(np.percentile(lat, 50)) / 1e6,
+            "p99_ms": float(np.percentile(lat, 99)) / 1e6}
 
 
-def time_e2e(ts, ms, periods, pdts, steps, warmup, device=0):
+# ---------------------------------------------------------- end to end
+
+
+class HostBatch:
+    """The ragged batch as per-curve host arrays (views of two flat float32
+    arrays) with the per-curve pointers the C ABI takes."""
+
+    def __init__(self, t, m, off):
+        self.t, self.m, self.off = t, m, off
+        self.n = len(off) - 1
+        self.lens = np.diff(off).astype(np.uint64)
+        self.tptr = self.ptrs(t)
+        self.mptr = self.ptrs(m)
+        self.m_ce = np.empty_like(m)
+        self.m_ls = np.empty_like(m)
+        self.ceptr = self.ptrs(self.m_ce)
+        self.lsptr = self.ptrs(self.m_ls)
+
+    def ptrs(self, a):
+        return (np.uint64(a.ctypes.data)
+                + np.uint64(4) * self.off[:-1].astype(np.uint64)).astype(np.uintp)
+
+
+def e2e_cabi(hb, periods, pdts, steps, warmup, device):
+    """Wall time per step of CE + AOV + LS peaks through the C ABI from host
+    buffers: host magnitude preparation (pf_normalize_mags /
+    pf_center_mags), and the peak calls -- each packs its curves into pinned
+    staging, copies them to the GPU, runs the kernels and the peak search
+    and copies the peaks back -- pipelined with PF_ASYNC so that host work
+    overlaps the GPU.  Returns (s per step, H2D bytes, D2H bytes, kernel
+    launches per step)."""
+    from periodfind_b200 import _native as nat
+
+    ctx = nat.Context(device)
+    lib, h = ctx.lib, ctx.handle
+    n = hb.n
+    idx = np.empty((3, n, N_PEAKS), np.int64)
+    val = np.empty((3, n, N_PEAKS), np.float32)
+    flags = nat.PF_MODE_CHOSEN | nat.PF_ASYNC
+    grid = (periods.ctypes.data, len(periods), pdts.ctypes.data, len(pdts))
+
+    def peaks(algo, mptr, k):
+        args = (h, hb.tptr.ctypes.data, mptr.ctypes.data, hb.lens.ctypes.data, n) + grid
+        out = (flags, idx[k].ctypes.data, val[k].ctypes.data)
+        if algo == "ce":
+            rc = lib.pf_ce_peaks(*args, 10, 10, 1, 1, N_PEAKS, 1, *out)
+        elif algo == "aov":
+            rc = lib.pf_aov_peaks(*args, 15, 1, N_PEAKS, 1, *out)
+        else:
+            rc = lib.pf_ls_peaks(*args, N_PEAKS, 1, *out)
+        ctx.check(rc)
+
+    def step():
+        ctx.check(lib.pf_normalize_mags(hb.mptr.ctypes.data, hb.lens.ctypes.data, n,
+                                        hb.ceptr.ctypes.data))
+        peaks("ce", hb.ceptr, 0)
+        peaks("aov", hb.mptr, 1)
+        # Centring for LS runs on the host while the GPU works.
+        ctx.check(lib.pf_center_mags(hb.mptr.ctypes.data, hb.lens.ctypes.data, n,
+                                     hb.lsptr.ctypes.data))
+        ctx.check(lib.pf_wait(h))
+        peaks("ls", hb.lsptr, 2)
+        ctx.check(lib.pf_wait(h))
+        ctx.check(lib.pf_wait(h))
+
+    for _ in range(warmup):
+        step()
+    l0 = ctx.launches
+    w = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        step()
+        w.append(time.perf_counter() - t0)
+    launches = (ctx.launches - l0) // max(steps, 1)
+    h2d = 3 * (hb.t.nbytes + hb.m.nbytes + periods.nbytes + pdts.nbytes)
+    d2h = idx.nbytes + val.nbytes
+    ctx.close()
+    return float(np.mean(w)), int(h2d), int(d2h), int(launches)
+
+
+def e2e_calc(t, m, off, periods, pdts, device):
+    """Seconds of one calc(list of numpy arrays, output='peaks') per
+    algorithm through the public Python classes (result objects built)."""
     from periodfind_b200 import gpu
 
-    ce = gpu.ConditionalEntropy(10, 10, device=device)
-    aov = gpu.AOV(15, device=device)
-    for _ in range(warmup):
-        ce.calc(ts, ms, periods, pdts, output="peaks", n_peaks=N_PEAKS)
-        aov.calc(ts, ms, periods, pdts, output="peaks", n_peaks=N_PEAKS)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        a = ce.calc(ts, ms, periods, pdts, output="peaks", n_peaks=N_PEAKS)
-        b = aov.calc(ts, ms, periods, pdts, output="peaks", n_peaks=N_PEAKS)
-    dt = (time.perf_counter() - t0) / steps
-    assert len(a) == len(ts) and len(b) == len(ts)
-    return dt
+    ts, ms = lc.split_csr(t, off), lc.split_csr(m, off)
+    out = {}
+    for algo, obj in (("ce", gpu.ConditionalEntropy(10, 10, device=device)),
+                      ("aov", gpu.AOV(15, device=device)),
+                      ("ls", gpu.LombScargle(device=device))):
+        t0 = time.perf_counter()
+        res = obj.calc(ts, ms, periods, pdts, output="peaks", n_peaks=N_PEAKS)
+        out[algo] = time.perf_counter() - t0
+        assert len(res) == len(ts)
+        del res
+    return out
 
 
-# ------------------------------------------------------------ CPU baseline
+# ------------------------------------------------------- LS peak precision
 
 
-def cpu_baseline(ts, ms, periods, pdts, target_s=12.0):
-    """The oracle (C/OpenMP restatement of the reference's Rust path) on all
-    host cores over the first k curves, k sized for ~target_s of work."""
+def _ls_power_f64(t, y, w):
+    """The reference's tau-form LS power (periodfind/cuda/ls.cu:107-134) in
+    FP64 for one curve at the angular frequencies w."""
+    th = np.outer(w, t)
+    c, s = np.cos(th), np.sin(th)
+    yc, ys = c @ y, s @ y
+    cc = (c * c).sum(1)
+    cs = (c * s).sum(1)
+    ss = len(t) - cc
+    tau = 0.5 * np.arctan2(2.0 * cs, cc - ss)
+    ct, st = np.cos(tau), np.sin(tau)
+    a = ct * yc + st * ys
+    b = ct * ys - st * yc
+    dl = ct * ct * cc + 2 * ct * st * cs + st * st * ss
+    dr = ct * ct * ss - 2 * ct * st * cs + st * st * cc
+    return 0.5 * (a * a / dl + b * b / dr)
+
+
+def ls_peak_error(step, periods, n_sample, torch, seed=SEED + 9):
+    """Refine the chosen LS periodogram's top-32 grid peaks of a random sample
+    of curves by 5 Newton steps on the GPU (pf_ls_refine_dev), then take one
+    FP64 Newton step from each refined frequency (derivatives by central
+    differences of the FP64 power, h = 1e-7 relative): its size relative to
+    the frequency is the refined peak's distance from the FP64 maximum."""
+    from periodfind_b200 import ls_grad
+
+    rng = np.random.default_rng(seed)
+    cur = np.sort(rng.choice(step.n, n_sample, replace=False))
+    idx = step.pk_i[2].cpu().numpy()[cur]
+    off = step.off
+    t_all = step.d_t.cpu().numpy()
+    y_all = step.mags["ls"].cpu().numpy()
+    ts = [t_all[off[c]:off[c + 1]] for c in cur]
+    ys = [y_all[off[c]:off[c + 1]] for c in cur]
+    sub_off = np.zeros(n_sample + 1, np.int64)
+    np.cumsum([len(x) for x in ts], out=sub_off[1:])
+    grid = 2.0 * np.pi / periods.astype(np.float64)
+    valid = idx >= 0
+    i = np.where(valid, idx, 0)
+    w0 = grid[i]
+    hw = np.maximum(np.abs(grid[np.maximum(i - 1, 0)] - w0),
+                    np.abs(grid[np.minimum(i + 1, len(grid) - 1)] - w0))
+    dev = step.d_t.device
+    w, _ = ls_grad.refine_peaks(torch.from_numpy(np.concatenate(ts)).to(dev),
+                                torch.from_numpy(np.concatenate(ys)).to(dev),
+                                torch.from_numpy(w0).to(dev), torch.from_numpy(hw).to(dev),
+                                sub_off, n_steps=5)
+    w = w.cpu().numpy()
+    errs = []
+    for k in range(n_sample):
+        t = ts[k].astype(np.float64)
+        y = ys[k].astype(np.float64)
+        wk = w[k][valid[k]]
+        if len(t) < 16 or wk.size == 0:
+            continue
+        h = 1e-7 * wk
+        p0 = _ls_power_f64(t, y, wk)
+        pp = _ls_power_f64(t, y, wk + h)
+        pm = _ls_power_f64(t, y, wk - h)
+        d1 = (pp - pm) / (2 * h)
+        d2 = (pp - 2 * p0 + pm) / (h * h)
+        ok = d2 < 0  # at a maximum of the FP64 power
+        errs.extend((np.abs(d1[ok] / d2[ok]) / wk[ok]).tolist())
+    errs = np.array(errs) if errs else np.zeros(1)
+    return {"peaks": int(errs.size), "curves": n_sample, "max_rel": float(errs.max()),
+            "median_rel": float(np.median(errs)), "target": 1e-7,
+            "method": "5 GPU Newton steps from the chosen periodogram's top-32 grid peaks; "
+                      "error = one FP64 Newton step (central differences of the FP64 power)"}
+
+
+# ------------------------------------------------------------ baselines
+
+
+def _sample_curves(off, k, seed):
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(len(off) - 1, min(k, len(off) - 1), replace=False))
+
+
+def _subset(t, m, off, cur):
+    return ([t[off[c]:off[c + 1]] for c in cur], [m[off[c]:off[c + 1]] for c in cur])
+
+
+def oracle_ragged(O, ts, ms, periods, pdts, cores):
+    """CE + AOV + LS with peaks by the CPU restatement of the Rust path
+    (rust/src/lib.rs:31-199, 508-677), magnitudes prepared as the
+    reference's classes prepare them."""
+    msn = [lc.normalize(m) for m in ms]
+    msc = [lc.center(m) for m in ms]
+    for pg, use_max in ((O.ce(ts, msn, periods, pdts, 10, 10, n_threads=cores), False),
+                        (O.aov(ts, ms, periods, pdts, 15, n_threads=cores), True),
+                        (O.ls(ts, msc, periods, pdts, n_threads=cores), True)):
+        O.find_top_peaks_batched(pg, N_PEAKS, 1, use_max, n_threads=cores)
+
+
+def cpu_baseline(t, m, off, periods, pdts, target_s=12.0):
+    """The oracle on all host cores over a random sample of curves (the
+    batch's length distribution) sized for about target_s of work."""
     from oracle import oracle as O
-    from tests import lightcurves as lc
 
     cores = os.cpu_count() or 1
-    k = 1
+    cur = _sample_curves(off, 100, SEED + 7)
+    ts, ms = _subset(t, m, off, cur)
     t0 = time.perf_counter()
-    O.ce(ts[:k], [lc.normalize(m) for m in ms[:k]], periods, pdts, 10, 10, n_threads=cores)
-    O.aov(ts[:k], ms[:k], periods, pdts, 15, n_threads=cores)
+    oracle_ragged(O, ts, ms, periods, pdts, cores)
     one = time.perf_counter() - t0
-    k = int(max(1, min(len(ts), target_s / max(one, 1e-3))))
+    k = int(max(50, min(len(off) - 1, 100 * target_s / max(one, 1e-3))))
+    cur = _sample_curves(off, k, SEED + 7)
+    ts, ms = _subset(t, m, off, cur)
     t0 = time.perf_counter()
-    O.ce(ts[:k], [lc.normalize(m) for m in ms[:k]], periods, pdts, 10, 10, n_threads=cores)
-    O.aov(ts[:k], ms[:k], periods, pdts, 15, n_threads=cores)
+    oracle_ragged(O, ts, ms, periods, pdts, cores)
     dt = time.perf_counter() - t0
-    value = evals_per_step(k) / dt
-    return {"value": value, "unit": "evals/s", "cores": cores, "kind": "port",
-            "sample": f"{k} of {len(ts)} curves (CE 10x10 + AOV 15, full 10000x2 grid), "
-                      f"{dt:.1f} s on {cores} threads"}
+    ev = 3 * sum(len(x) for x in ts) * len(periods) * len(pdts)
+    return {"value": ev / dt, "unit": "evals/s", "cores": cores, "kind": "port",
+            "sample": f"{len(cur)} random curves of {len(off) - 1} (CE + AOV + LS periodograms "
+                      f"and top-32 peaks over the full 20000-period grid), {dt:.1f} s on "
+                      f"{cores} threads; C/OpenMP restatement of the reference's Rust path"}
+
+
+def reference_cuda(t, m, off, periods, pdts, clocks, n_sample=1000):
+    """The reference's own CUDA drivers (CalcCEValsBatched, CalcAOVValsBatched,
+    CalcLSBatched; periodfind/cuda/{ce,aov,ls}.cu) built from its sources,
+    on a random curve sample of the batch: periodograms only (the
+    reference's GPU path has no peak search), with its per-call device
+    allocation, per-curve copies and launches, as its Python classes call
+    it.  A reported comparator beside the plain form."""
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return {"unavailable": "oracle/_ref/libpfref.so is not built"}
+    cur = _sample_curves(off, n_sample, SEED + 8)
+    ts, ms = _subset(t, m, off, cur)
+    msn = [lc.normalize(x) for x in ms]
+    msc = [lc.center(x) for x in ms]
+    O.ref_cuda("ce", ts[:8], msn[:8], periods, pdts, n_phase=10, n_mag=10)  # load, warm up
+    out = {}
+    with clocks.region("reference_cuda"):
+        for algo, mm, kw in (("ce", msn, {"n_phase": 10, "n_mag": 10}),
+                             ("aov", ms, {"n_phase": 15}), ("ls", msc, {})):
+            t0 = time.perf_counter()
+            O.ref_cuda(algo, ts, mm, periods, pdts, **kw)
+            out[algo] = time.perf_counter() - t0
+    ev = sum(len(x) for x in ts) * len(periods) * len(pdts)
+    return {"value": 3 * ev / sum(out.values()), "unit": "evals/s",
+            "per_algo_evals_per_s": {a: ev / s for a, s in out.items()},
+            "sample": f"{len(cur)} random curves of {len(off) - 1}, full grid, wall time of the "
+                      "reference's Calc*Batched host drivers, periodograms only",
+            "clocks": clocks.regions.get("reference_cuda")}
 
 
 def reference_arm(args):
+    """The reference arm: the CPU restatement of the reference's Rust path on
+    all host cores, each step a fixed random sample of the ragged batch."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    ts, ms, periods, pdts = make_workload()
     from oracle import oracle as O
-    from tests import lightcurves as lc
 
+    n_curves = args.curves or RAGGED_CURVES
+    t, m, off = lc.ragged_batch(n_curves, SEED + 5)
+    periods, pdts = ragged_grid()
     cores = os.cpu_count() or 1
-    k = 2
-    sub_t, sub_m = ts[:k], ms[:k]
-    run = lambda: (O.ce(sub_t, [lc.normalize(m) for m in sub_m], periods, pdts, 10, 10,
-                        n_threads=cores),
-                   O.aov(sub_t, sub_m, periods, pdts, 15, n_threads=cores))
+    k = 60
+    cur = _sample_curves(off, k, SEED + 7)
+    ts, ms = _subset(t, m, off, cur)
+    ev = 3 * sum(len(x) for x in ts) * len(periods) * len(pdts)
     for _ in range(args.warmup):
-        run()
+        oracle_ragged(O, ts, ms, periods, pdts, cores)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        run()
+        oracle_ragged(O, ts, ms, periods, pdts, cores)
         times.append(time.perf_counter() - t0)
     per_step = float(np.mean(times))
-    value = evals_per_step(k) / per_step
+    value = ev / per_step
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 fold, f32 statistics", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_curves_per_step": k},
+        "config": {"workload": RAGGED_WORKLOAD, "sample_curves_per_step": k},
         "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "port",
-                         "sample": f"{k} of {N_CURVES} curves per step, full grid, "
-                                   f"C/OpenMP restatement of the reference's Rust CPU path"},
+                         "sample": f"{k} random curves of {n_curves} per step (CE + AOV + LS "
+                                   "periodograms and top-32 peaks, full grid); C/OpenMP "
+                                   "restatement of the reference's Rust CPU path"},
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-# ------------------------------------------------------------ ragged batch
+# ------------------------------------------------- 1000 x 4096 secondary
 
 
-def make_ragged(n_curves=100000, seed=SEED + 5, n_periods=20000):
-    """Mixed ragged batch: lengths lognormal (median 300, sigma 0.8) clipped to
-    [20, 2000]; seasonal cadence over 2500 days (125-day seasons); 1/3
-    sinusoids, 1/3 box eclipses (depth 0.5, duty 0.05), 1/3 pure noise; noise
-    sigma U[0.02, 0.1]; 20000 periods log-spaced in [0.05, 500] days."""
-    rng = np.random.default_rng(seed)
-    lens = np.clip(np.round(rng.lognormal(np.log(300.0), 0.8, n_curves)), 20, 2000).astype(np.int64)
-    cid = np.repeat(np.arange(n_curves), lens)
-    n_years = int(np.ceil(2500.0 / 365.25))
-    t = rng.integers(0, n_years, cid.size) * 365.25 + rng.uniform(0.0, 125.25, cid.size)
-    t = np.minimum(t, 2500.0)
-    order = np.lexsort((t, cid))
-    t = t[order].astype(np.float32)
-    period = np.exp(rng.uniform(np.log(0.05), np.log(500.0), n_curves))[cid]
-    phase = rng.uniform(0, 1, n_curves)[cid]
-    kind = (np.arange(n_curves) % 3)[cid]
-    sigma = rng.uniform(0.02, 0.1, n_curves)[cid]
-    ph = np.mod(t / period + phase, 1.0)
-    y = np.where(kind == 0, 0.3 * np.sin(2 * np.pi * ph),
-                 np.where(kind == 1, np.where(ph < 0.05, -0.5, 0.0), 0.0))
-    m = (15.0 + y + rng.normal(0.0, 1.0, cid.size) * sigma).astype(np.float32)
-    off = np.zeros(n_curves + 1, np.int64)
-    np.cumsum(lens, out=off[1:])
-    periods = np.exp(np.linspace(np.log(0.05), np.log(500.0), n_periods)).astype(np.float32)
-    return t, m, off, periods, np.zeros(1, np.float32)
+class BatchStep:
+    """CE + AOV + peaks on the device-resident 1000 x 4096 batch."""
+
+    def __init__(self, ts, ms, periods, pdts, flags, torch, device):
+        from periodfind_b200 import _native as nat
+
+        self.ctx = nat.Context(device)
+        self.flags = flags
+        off = np.zeros(len(ts) + 1, np.int64)
+        np.cumsum([len(t) for t in ts], out=off[1:])
+        self.off = off
+        dev = torch.device("cuda", device)
+        self.t = torch.from_numpy(np.concatenate(ts)).to(dev)
+        self.m_ce = torch.from_numpy(np.concatenate([lc.normalize(m) for m in ms])).to(dev)
+        self.m_aov = torch.from_numpy(np.concatenate(ms)).to(dev)
+        self.P = torch.from_numpy(periods).to(dev)
+        self.D = torch.from_numpy(pdts).to(dev)
+        self.n = len(ts)
+        self.cells = len(periods) * len(pdts)
+        self.pg = torch.empty((2, self.n, self.cells), dtype=torch.float32, device=dev)
+        self.pk_i = torch.empty((2, self.n, N_PEAKS), dtype=torch.int64, device=dev)
+        self.pk_v = torch.empty((2, self.n, N_PEAKS), dtype=torch.float32, device=dev)
+        self.np_, self.nd = len(periods), len(pdts)
+        self.s = torch.cuda.current_stream(dev).cuda_stream
+
+    def run(self):
+        c, lib, h = self.ctx, self.ctx.lib, self.ctx.handle
+        for k, m in enumerate((self.m_ce, self.m_aov)):
+            common = (h, self.t.data_ptr(), m.data_ptr(), self.off.ctypes.data, self.n,
+                      self.P.data_ptr(), self.np_, self.D.data_ptr(), self.nd)
+            if k == 0:
+                c.check(lib.pf_ce_dev(*common, 10, 10, 1, 1, self.flags, self.pg[0].data_ptr(),
+                                      self.s))
+            else:
+                c.check(lib.pf_aov_dev(*common, 15, 1, self.flags, self.pg[1].data_ptr(),
+                                       self.s))
+            c.check(lib.pf_find_peaks_dev(h, self.pg[k].data_ptr(), self.n, self.cells, N_PEAKS,
+                                          1, k, self.pk_i[k].data_ptr(), self.pk_v[k].data_ptr(),
+                                          self.s))
 
 
-def ragged_arm(args):
+def batch_secondary(torch, device, flush, clocks, steps=3):
+    """The 1000 x 4096 batch: chosen and plain device steps (CUDA events, L2
+    flushed between steps)."""
+    from periodfind_b200 import _native as nat
+
+    ts, ms, periods, pdts = make_workload()
+    ev = 2 * N_CURVES * N_POINTS * N_PERIODS * len(PDTS)
+    stream = torch.cuda.current_stream(device)
+    out = {"workload": "CE(10x10) + AOV(15) + top-32 peaks, 1000 curves x 4096 points x "
+                       "10000 log periods [0.1, 100] d x pdts [0, 1e-6]", "evals": ev}
+    for mode, flags, k in (("chosen", nat.PF_MODE_CHOSEN, steps),
+                           ("plain", nat.PF_MODE_PLAIN, 1)):
+        st = BatchStep(ts, ms, periods, pdts, flags, torch, device)
+        with clocks.region(f"batch_4096_{mode}"):
+            ms_, _ = time_steps(st.run, k, 1, torch, flush, stream)
+        out[mode] = {"ms_per_step": ms_, "value": ev / (ms_ * 1e-3)}
+        st.ctx.close()
+    out["chosen_over_plain"] = out["plain"]["ms_per_step"] / out["chosen"]["ms_per_step"]
+    return out
+
+
+# ------------------------------------------------------------------ main
+
+
+def _roofline(kernel_ms, evals_algo, pipes, off, periods, pdts):
+    """Roofline of the kernel with the most time, and each kernel's
+    fraction of its own bound."""
+    dom = max(kernel_ms, key=kernel_ms.get)
+    rf = ROOFLINE[dom]
+
+    def frac(pipe, ops, ms):
+        pk = pipes.get(pipe, {}).get("per_s", float("nan"))
+        a = evals_algo * ops / (ms * 1e-3)
+        return a, pk, (a / pk if pk == pk else None)
+
+    achieved, peak, f = frac(rf["pipe"], rf["ops"], kernel_ms[dom])
+    views = {}
+    for name, (pipe, ops) in rf["views"].items():
+        a, pk, fv = frac(pipe, ops, kernel_ms[dom])
+        views[name] = {"achieved_gops": a / 1e9, "peak_gops": pk / 1e9, "ops_per_eval": ops,
+                       "frac": fv}
+    per_kernel = {a: {"kernel": ROOFLINE[a]["kernel"], "ms": kernel_ms[a],
+                      "bound": ROOFLINE[a]["bound"],
+                      "frac": frac(ROOFLINE[a]["pipe"], ROOFLINE[a]["ops"], kernel_ms[a])[2]}
+                  for a in kernel_ms}
+    in_bytes = int(off[-1]) * 8 + len(periods) * 4
+    out_bytes = (len(off) - 1) * len(periods) * len(pdts) * 4
+    hbm_gbs = (in_bytes + out_bytes) / (kernel_ms[dom] * 1e-3) / 1e9
+    return {"bound": rf["bound"], "kernel": rf["kernel"], "achieved": achieved / 1e9,
+            "peak": peak / 1e9, "unit": "Gop/s", "frac": f, "ops_per_eval": rf["ops"],
+            "kernel_ms": kernel_ms[dom],
+            "peak_source": f"measured on this GPU (pipe_peaks.cu, {rf['pipe']})",
+            "traffic": RAGGED_TRAFFIC[dom], "views": views, "per_kernel": per_kernel,
+            "hbm_view": {"achieved_gbs": hbm_gbs, "peak_gbs": 6453.7, "frac": hbm_gbs / 6453.7}}
+
+
+def ragged_main(args):
     import torch
 
     from periodfind_b200 import _native as nat
-
-    torch.cuda.set_device(0)
-    n_curves = args.curves if args.curves != N_CURVES else 100000
-    t, m, off, periods, pdts = make_ragged(n_curves)
-    lens = np.diff(off)
-    ctx = nat.default_context(0)
-    dev = "cuda"
-    d_t = torch.from_numpy(t).to(dev)
-    # Per-curve magnitude preparation as the reference does it: normalise for
-    # CE (periodfind/_utils.py:39-45), centre for LS, raw for AOV.
-    seg_min = np.minimum.reduceat(m, off[:-1])
-    seg_max = np.maximum.reduceat(m, off[:-1])
-    cid = np.repeat(np.arange(n_curves), lens)
-    m_ce = (((m - seg_min[cid]) / (seg_max[cid] - seg_min[cid])) * np.float32(0.999)
-            + np.float32(5e-4)).astype(np.float32)
-    seg_mean = (np.add.reduceat(m.astype(np.float64), off[:-1]) / lens).astype(np.float32)
-    m_ls = (m - seg_mean[cid]).astype(np.float32)
-    mags = {"ce": torch.from_numpy(m_ce).to(dev), "aov": torch.from_numpy(m).to(dev),
-            "ls": torch.from_numpy(m_ls).to(dev)}
-    d_p = torch.from_numpy(periods).to(dev)
-    d_d = torch.from_numpy(pdts).to(dev)
-    cells = len(periods) * len(pdts)
-    pg = torch.empty((n_curves, cells), dtype=torch.float32, device=dev)
-    pk_i = torch.empty((n_curves, N_PEAKS), dtype=torch.int64, device=dev)
-    pk_v = torch.empty((n_curves, N_PEAKS), dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream()
-    s = stream.cuda_stream
-    evals = int(lens.sum()) * cells
-
-    def step(algo, flags):
-        h, lib = ctx.handle, ctx.lib
-        common = (h, d_t.data_ptr(), mags[algo].data_ptr(), off.ctypes.data, n_curves,
-                  d_p.data_ptr(), len(periods), d_d.data_ptr(), len(pdts))
-        if algo == "ce":
-            ctx.check(lib.pf_ce_dev(*common, 10, 10, 1, 1, flags, pg.data_ptr(), s))
-        elif algo == "aov":
-            ctx.check(lib.pf_aov_dev(*common, 15, 1, flags, pg.data_ptr(), s))
-        else:
-            ctx.check(lib.pf_ls_dev(*common, flags, pg.data_ptr(), s))
-        ctx.check(lib.pf_find_peaks_dev(h, pg.data_ptr(), n_curves, cells, N_PEAKS, 1,
-                                        0 if algo == "ce" else 1, pk_i.data_ptr(),
-                                        pk_v.data_ptr(), s))
-
-    out = {"workload": f"ragged: {n_curves} curves, lengths lognormal(median 300, sigma 0.8) "
-                       f"in [20, 2000] (mean {lens.mean():.0f}), seasonal cadence 2500 d, "
-                       f"{len(periods)} log periods [0.05, 500] d, top-{N_PEAKS} peaks",
-           "evals_per_algo": evals, "algos": {}}
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    from periodfind_b200.plan import BatchPlan
-
-    for algo in ("ce", "aov", "ls"):
-        row = {}
-        # The chosen form runs as a batch plan: the pipeline (packing,
-        # preparation, per-length-class tuned queue launches, peaks) captured
-        # once as a CUDA graph; the plain form as direct calls per step.
-        plan = BatchPlan(algo, d_t, mags[algo], off, d_p, d_d, pg, n_phase=10 if algo == "ce"
-                         else 15, n_mag=10, flags=nat.PF_MODE_CHOSEN, n_peaks=N_PEAKS,
-                         peak_idx=pk_i, peak_val=pk_v)
-        for mode, flags in (("chosen", nat.PF_MODE_CHOSEN), ("plain", nat.PF_MODE_PLAIN)):
-            run = (lambda: plan.launch(stream)) if mode == "chosen" else (
-                lambda flags=flags: step(algo, flags))
-            run()
-            torch.cuda.synchronize()
-            ts_ = []
-            for _ in range(max(1, args.steps)):
-                flush.zero_()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                run()
-                e1.record(stream)
-                e1.synchronize()
-                ts_.append(e0.elapsed_time(e1))
-            ms_ = float(np.median(ts_))
-            # Per-curve device latency from a separate, stamped run.
-            step(algo, flags | nat.PF_TIMING)
-            lat = np.zeros(n_curves)
-            ctx.check(ctx.lib.pf_curve_latency(ctx.handle, n_curves, lat.ctypes.data))
-            row[mode] = {"ms": ms_, "evals_per_s": evals / (ms_ * 1e-3),
-                         "curve_latency_ms_p50": float(np.percentile(lat, 50)) / 1e6,
-                         "curve_latency_ms_p99": float(np.percentile(lat, 99)) / 1e6}
-        row["chosen_over_plain"] = row["plain"]["ms"] / row["chosen"]["ms"]
-        row["chosen"]["launch"] = "batch plan (CUDA graph replay)"
-        plan.close()
-        out["algos"][algo] = row
-    tc = sum(out["algos"][a]["chosen"]["ms"] for a in out["algos"])
-    tp = sum(out["algos"][a]["plain"]["ms"] for a in out["algos"])
-    out["all_three"] = {"chosen_evals_per_s": 3 * evals / (tc * 1e-3),
-                        "plain_evals_per_s": 3 * evals / (tp * 1e-3),
-                        "chosen_over_plain": tp / tc}
-    out["tuning"] = ctx.tuning_report().strip().splitlines()
-    print(json.dumps(out), flush=True)
-
-
-# ------------------------------------------------------------------ FPW
-
-
-def fpw_arm(args, bls=False):
-    """FPW(10) -- or, with bls, BoxLeastSquares(50, 0.01, 0.5) -- over the
-    benchmark batch (1000 curves x 4096 points, 10000 log periods in
-    [0.1, 100] d x pdts [0, 1e-6]) with per-point uncertainties U[0.02, 0.1]:
-    device time of the chosen and plain forms (the kernel, CUDA events),
-    end-to-end calc(output='peaks') from numpy lists, and the oracle (the
-    Rust path's restatement) on all host cores over a sample."""
-    from periodfind_b200 import gpu
-
-    ts, ms, periods, pdts = make_workload(args.curves)
-    rng = np.random.default_rng(SEED + 6)
-    es = [rng.uniform(0.02, 0.1, len(t)).astype(np.float32) for t in ts]
-    evals = sum(len(t) for t in ts) * len(periods) * len(pdts)
-    label = "BLS(50, qmin 0.01, qmax 0.5)" if bls else "FPW(10)"
-    out = {"workload": f"{label}, {len(ts)} curves x {N_POINTS} pts, {N_PERIODS} log periods "
-                       f"[0.1,100] d x pdts {list(PDTS)}, errs U[0.02,0.1]", "evals": evals}
-    from periodfind_b200 import _native as nat
-
-    ctx = nat.default_context(0)
-    for mode in ("chosen", "plain"):
-        obj = gpu.BoxLeastSquares(50, 0.01, 0.5, mode=mode) if bls else gpu.FPW(10, mode=mode)
-        obj.periodograms(ts, ms, periods, pdts, errs=es)
-        k = []
-        for _ in range(max(1, args.steps)):
-            obj.periodograms(ts, ms, periods, pdts, errs=es)
-            k.append(ctx.lib.pf_last_kernel_ms(ctx.handle))
-        kms = float(np.median(k))
-        obj.calc(ts, ms, periods, pdts, errs=es, output="peaks", n_peaks=N_PEAKS)
-        w = []
-        for _ in range(max(1, min(args.steps, 3))):
-            t0 = time.perf_counter()
-            obj.calc(ts, ms, periods, pdts, errs=es, output="peaks", n_peaks=N_PEAKS)
-            w.append(time.perf_counter() - t0)
-        out[mode] = {"kernel_ms": kms, "evals_per_s": evals / (kms * 1e-3),
-                     "e2e_ms": float(np.median(w)) * 1e3,
-                     "e2e_evals_per_s": evals / float(np.median(w))}
-    out["chosen_over_plain"] = out["plain"]["kernel_ms"] / out["chosen"]["kernel_ms"]
-    if not args.no_cpu:
-        from oracle import oracle as O
-
-        cores = os.cpu_count() or 1
-        k = 20
-        t0 = time.perf_counter()
-        if bls:
-            O.bls(ts[:k], ms[:k], periods, pdts, 50, 0.01, 0.5, errs=es[:k], n_threads=cores)
-        else:
-            O.fpw(ts[:k], ms[:k], periods, pdts, 10, errs=es[:k], n_threads=cores)
-        dt = time.perf_counter() - t0
-        out["cpu_baseline"] = {"value": k * N_POINTS * N_PERIODS * len(PDTS) / dt,
-                               "unit": "evals/s", "cores": cores, "kind": "port",
-                               "sample": f"{k} of {len(ts)} curves, {dt:.1f} s"}
-    print(json.dumps(out), flush=True)
-
-
-# ---------------------------------------------------- device-resident I/O
-
-
-def device_arm(args):
-    """CE(10x10) and AOV(15) periodograms of the benchmark batch (1000 curves x
-    4096 points x 10000 periods x 2 pdts) from curves already on the GPU,
-    left on the GPU (periodograms_device: magnitude preparation on the
-    device, no host copy), against the public host path
-    calc(output='periodogram') from numpy lists, which returns the 80 MB
-    periodogram per algorithm to the host.  Wall time per step, synchronised."""
-    import torch
-
-    from periodfind_b200 import gpu
-
-    torch.cuda.set_device(0)
-    ts, ms, periods, pdts = make_workload(args.curves)
-    off = np.zeros(len(ts) + 1, np.int64)
-    np.cumsum([len(t) for t in ts], out=off[1:])
-    d_t = torch.from_numpy(np.concatenate(ts)).cuda()
-    d_m = torch.from_numpy(np.concatenate(ms)).cuda()
-    evals = 2 * int(off[-1]) * len(periods) * len(pdts)
-    ce, aov = gpu.ConditionalEntropy(10, 10), gpu.AOV(15)
-
-    def dev_step():
-        a = ce.periodograms_device(d_t, d_m, off, periods, pdts)
-        b = aov.periodograms_device(d_t, d_m, off, periods, pdts)
-        torch.cuda.synchronize()
-        return a, b
-
-    def host_step():
-        return (ce.calc(ts, ms, periods, pdts, output="periodogram"),
-                aov.calc(ts, ms, periods, pdts, output="periodogram"))
-
-    out = {"workload": f"CE(10x10) + AOV(15) periodograms, {len(ts)} curves x {N_POINTS} pts x "
-                       f"{N_PERIODS} periods x {len(PDTS)} pdts", "evals": evals}
-    for name, fn in (("device_resident", dev_step), ("host_calc_periodogram", host_step)):
-        for _ in range(2):
-            fn()
-        w = []
-        for _ in range(max(3, args.steps)):
-            t0 = time.perf_counter()
-            fn()
-            w.append(time.perf_counter() - t0)
-        ms_ = float(np.median(w)) * 1e3
-        out[name] = {"ms": ms_, "evals_per_s": evals / (ms_ * 1e-3)}
-    print(json.dumps(out), flush=True)
-
-
-# ------------------------------------------------------ small CE batch
-
-
-def small_arm(args):
-    """CE 10 x 10 on 100 curves x 1024 points (times uniform in [0, 1000] d,
-    15 + 0.3 sin(2 pi t / P + phi) + N(0, 0.05^2), P ~ U[0.5, 10] d) over
-    1000 periods linspace(0.5, 10) d, period_dts [0], output 'stats'.
-    Device time of the chosen and plain forms, end-to-end calc() time, bin
-    agreement of the two forms, and the CPU port on all host cores."""
-    import torch
-
-    from periodfind_b200 import _native as nat
-    from periodfind_b200 import gpu
-
-    torch.cuda.set_device(0)
-    rng = np.random.default_rng(SEED + 1)
-    n_curves, n_pts = 100, 1024
-    ts, ms = [], []
-    for _ in range(n_curves):
-        t = np.sort(rng.uniform(0.0, 1000.0, n_pts)).astype(np.float32)
-        per, ph = rng.uniform(0.5, 10.0), rng.uniform(0.0, 2 * np.pi)
-        m = 15.0 + 0.3 * np.sin(2 * np.pi * t.astype(np.float64) / per + ph)
-        ts.append(t)
-        ms.append((m + rng.normal(0.0, 0.05, n_pts)).astype(np.float32))
-    periods = np.linspace(0.5, 10.0, 1000).astype(np.float32)
-    pdts = np.zeros(1, np.float32)
-    evals = n_curves * n_pts * len(periods)
-    msn = [((m - m.min()) / (m.max() - m.min()) * np.float32(0.999) + np.float32(5e-4))
-           .astype(np.float32) for m in ms]
-    off = np.arange(n_curves + 1, dtype=np.int64) * n_pts
-    d_t = torch.from_numpy(np.concatenate(ts)).cuda()
-    d_m = torch.from_numpy(np.concatenate(msn)).cuda()
-    d_p = torch.from_numpy(periods).cuda()
-    d_d = torch.from_numpy(pdts).cuda()
-    pg = torch.empty((n_curves, len(periods)), device="cuda")
-    ctx = nat.default_context(0)
-    s = torch.cuda.current_stream().cuda_stream
-    out = {"workload": "CE 10x10 stats, 100 curves x 1024 points x 1000 periods "
-                       "linspace(0.5, 10) d, period_dts [0]", "evals": evals}
-    for mode, flags in (("chosen", nat.PF_MODE_CHOSEN), ("plain", nat.PF_MODE_PLAIN)):
-        def run(flags=flags):
-            ctx.check(ctx.lib.pf_ce_dev(ctx.handle, d_t.data_ptr(), d_m.data_ptr(),
-                                        off.ctypes.data, n_curves, d_p.data_ptr(), len(periods),
-                                        d_d.data_ptr(), 1, 10, 10, 1, 1, flags, pg.data_ptr(), s))
-        for _ in range(3):
-            run()
-        torch.cuda.synchronize()
-        k = []
-        for _ in range(max(3, args.steps)):
-            run()
-            torch.cuda.synchronize()
-            k.append(ctx.lib.pf_last_kernel_ms(ctx.handle))
-        obj = gpu.ConditionalEntropy(10, 10, mode=mode)
-        obj.calc(ts, ms, periods, pdts, output="stats")
-        w = []
-        for _ in range(max(3, args.steps)):
-            t0 = time.perf_counter()
-            obj.calc(ts, ms, periods, pdts, output="stats")
-            w.append(time.perf_counter() - t0)
-        kms, ws = float(np.median(k)), float(np.median(w))
-        out[mode] = {"kernel_ms": kms, "evals_per_s": evals / (kms * 1e-3),
-                     "e2e_ms": ws * 1e3, "e2e_evals_per_s": evals / ws}
-    a = gpu.ConditionalEntropy(mode="plain").periodograms(ts, msn, periods, pdts)
-    b = gpu.ConditionalEntropy(mode="chosen", reference_stats=True).periodograms(
-        ts, msn, periods, pdts)
-    out["bins_identical_chosen_vs_plain"] = bool(np.array_equal(a, b))
-    out["chosen_over_plain"] = out["plain"]["kernel_ms"] / out["chosen"]["kernel_ms"]
-    if not args.no_cpu:
-        from oracle import oracle as O
-
-        cores = os.cpu_count() or 1
-        t0 = time.perf_counter()
-        O.ce(ts, msn, periods, pdts, 10, 10, n_threads=cores)
-        dt = time.perf_counter() - t0
-        out["cpu_baseline"] = {"value": evals / dt, "unit": "evals/s", "cores": cores,
-                               "kind": "port", "sample": f"all {n_curves} curves, {dt:.2f} s"}
-    print(json.dumps(out), flush=True)
-
-
-# ------------------------------------------------- LS derivatives and study
-
-
-def _seasonal_ls_batch(lengths, seed, baseline=3000.0):
-    """LS study curves: seasonal cadence over `baseline` days (240-day annual
-    gap), 15 + A sin(2 pi f t) + N(0, sigma^2) with A ~ U[0.01, 0.5],
-    sigma ~ U[0.01, 0.1], f ~ U[0.01, 20] / day; magnitudes centred.
-    Returns CSR (times, mags, offsets)."""
-    rng = np.random.default_rng(seed)
-    lengths = np.asarray(lengths, np.int64)
-    n_curves = len(lengths)
-    cid = np.repeat(np.arange(n_curves), lengths)
-    n_years = int(np.ceil(baseline / 365.25))
-    t = rng.integers(0, n_years, cid.size) * 365.25 + rng.uniform(0.0, 125.25, cid.size)
-    t = np.minimum(t, baseline)
-    t = t[np.lexsort((t, cid))].astype(np.float32)
-    amp = rng.uniform(0.01, 0.5, n_curves)[cid]
-    sig = rng.uniform(0.01, 0.1, n_curves)[cid]
-    f = rng.uniform(0.01, 20.0, n_curves)[cid]
-    ph = rng.uniform(0, 2 * np.pi, n_curves)[cid]
-    m = 15.0 + amp * np.sin(2 * np.pi * f * t.astype(np.float64) + ph)
-    m = m + rng.normal(0.0, 1.0, cid.size) * sig
-    off = np.zeros(n_curves + 1, np.int64)
-    np.cumsum(lengths, out=off[1:])
-    mean = np.add.reduceat(m, off[:-1]) / lengths
-    return t, (m - mean[cid]).astype(np.float32), off
-
-
-def _event_ms(torch, fn, reps, flush):
-    ts_ = []
-    for _ in range(reps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        fn()
-        e1.record()
-        e1.synchronize()
-        ts_.append(e0.elapsed_time(e1))
-    return float(np.median(ts_))
-
-
-def lsgrad_arm(args):
-    """2000 curves x 2048 points over 3000 days; 20000 log-spaced frequencies
-    in [0.01, 20] / day.  Times the LS grid periodogram + top-32 peaks, the
-    autograd forward (power, dP/domega, coefficients) and backward
-    (dP/dy and dL/domega) over the grid, and 5 Newton steps on the top-32
-    peaks of every curve."""
-    import torch
-
-    from periodfind_b200 import _native as nat
-    from periodfind_b200 import ls_grad
-
-    torch.cuda.set_device(0)
-    n_curves, n_pts, n_freq = 2000, 2048, 20000
-    t, m, off = _seasonal_ls_batch(np.full(n_curves, n_pts), SEED + 4)
-    freqs = np.exp(np.linspace(np.log(0.01), np.log(20.0), n_freq))
-    periods = (1.0 / freqs[::-1]).astype(np.float32)
-    dev = "cuda"
-    d_t, d_m = torch.from_numpy(t).to(dev), torch.from_numpy(m).to(dev)
-    d_p = torch.from_numpy(periods).to(dev)
-    d_d = torch.zeros(1, dtype=torch.float32, device=dev)
-    pg = torch.empty((n_curves, n_freq), dtype=torch.float32, device=dev)
-    pk_i = torch.empty((n_curves, N_PEAKS), dtype=torch.int64, device=dev)
-    pk_v = torch.empty((n_curves, N_PEAKS), dtype=torch.float32, device=dev)
-    ctx = nat.default_context(0)
-    s = torch.cuda.current_stream().cuda_stream
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    reps = max(1, args.steps)
-
-    def grid_peaks():
-        ctx.check(ctx.lib.pf_ls_dev(ctx.handle, d_t.data_ptr(), d_m.data_ptr(), off.ctypes.data,
-                                    n_curves, d_p.data_ptr(), n_freq, d_d.data_ptr(), 1,
-                                    nat.PF_MODE_CHOSEN, pg.data_ptr(), s))
-        ctx.check(ctx.lib.pf_find_peaks_dev(ctx.handle, pg.data_ptr(), n_curves, n_freq, N_PEAKS,
-                                            1, 1, pk_i.data_ptr(), pk_v.data_ptr(), s))
-
-    w_grid = torch.from_numpy(2 * np.pi / periods.astype(np.float64)).to(dev)
-    y = d_m.clone().requires_grad_(True)
-    w = w_grid.clone().requires_grad_(True)
-    holder = {}
-
-    def forward():
-        holder["P"] = ls_grad.ls_power(d_t, y, w, off)
-
-    def backward():
-        holder["P"].backward(holder["g"])
-
-    grid_peaks()
-    forward()
-    holder["g"] = torch.ones_like(holder["P"])
-    backward()
-    torch.cuda.synchronize()
-    out = {"workload": f"LS derivatives: {n_curves} curves x {n_pts} points, seasonal cadence "
-                       f"3000 d, {n_freq} log-spaced frequencies [0.01, 20] / d, top-{N_PEAKS} "
-                       "peaks refined by 5 Newton steps"}
-    ev = n_curves * n_pts * n_freq
-    ms_grid = _event_ms(torch, grid_peaks, reps, flush)
-    ms_fwd = _event_ms(torch, forward, reps, flush)
-    ms_bwd = []
-    for _ in range(reps):
-        forward()
-        torch.cuda.synchronize()
-        ms_bwd.append(_event_ms(torch, backward, 1, flush))
-    ms_bwd = float(np.median(ms_bwd))
-    # Newton refinement of the grid peaks.
-    idx = pk_i.clamp(min=0)
-    wg = w_grid
-    w0 = wg[idx]
-    hw = torch.maximum((wg[(idx - 1).clamp(min=0)] - w0).abs(),
-                       (wg[(idx + 1).clamp(max=n_freq - 1)] - w0).abs()).contiguous()
-    w0 = w0.contiguous()
-
-    def refine():
-        holder["ref"] = ls_grad.refine_peaks(d_t, d_m, w0, hw, off, n_steps=5)
-
-    refine()
-    ms_ref = _event_ms(torch, refine, reps, flush)
-    ev_ref = n_curves * n_pts * N_PEAKS * 6
-    out["grid_periodogram_peaks"] = {"ms": ms_grid, "evals_per_s": ev / (ms_grid * 1e-3)}
-    out["autograd_forward"] = {"ms": ms_fwd, "evals_per_s": ev / (ms_fwd * 1e-3)}
-    out["autograd_backward"] = {"ms": ms_bwd, "evals_per_s": ev / (ms_bwd * 1e-3)}
-    out["newton_refine_5_steps"] = {"ms": ms_ref, "evals_per_s": ev_ref / (ms_ref * 1e-3),
-                                    "peaks": n_curves * N_PEAKS}
-    print(json.dumps(out), flush=True)
-
-
-def precision_arm(args):
-    """10000 curves, lengths log-uniform in [64, 16384], seasonal cadence over
-    3000 days; 50000 frequencies uniform in [0.01, 20] / day.  Times the LS
-    periodogram with each fold: plain (the reference's FP64-divide fold),
-    chosen split-precision, chosen exact, and the all-FP32 fold."""
-    import torch
-
-    from periodfind_b200 import _native as nat
-
-    torch.cuda.set_device(0)
-    rng = np.random.default_rng(SEED + 3)
-    n_curves = args.curves if args.curves != N_CURVES else 10000
-    lengths = np.exp(rng.uniform(np.log(64), np.log(16384), n_curves)).astype(np.int64)
-    t, m, off = _seasonal_ls_batch(lengths, SEED + 3)
-    n_freq = 50000
-    periods = (1.0 / np.linspace(0.01, 20.0, n_freq)[::-1]).astype(np.float32)
-    dev = "cuda"
-    d_t, d_m = torch.from_numpy(t).to(dev), torch.from_numpy(m).to(dev)
-    d_p = torch.from_numpy(periods).to(dev)
-    d_d = torch.zeros(1, dtype=torch.float32, device=dev)
-    pg = torch.empty((n_curves, n_freq), dtype=torch.float32, device=dev)
-    ctx = nat.default_context(0)
-    s = torch.cuda.current_stream().cuda_stream
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    ev = int(lengths.sum()) * n_freq
-    out = {"workload": f"LS precision study: {n_curves} curves, lengths log-uniform [64, 16384] "
-                       f"(mean {lengths.mean():.0f}), seasonal cadence 3000 d, {n_freq} "
-                       "frequencies uniform in [0.01, 20] / d", "evals": ev, "folds": {}}
-    for name, flags in (("plain (reference fold)", nat.PF_MODE_PLAIN),
-                        ("chosen split-precision", nat.PF_MODE_CHOSEN),
-                        ("chosen exact", nat.PF_MODE_CHOSEN | nat.PF_FOLD_EXACT),
-                        ("all-FP32", nat.PF_MODE_CHOSEN | nat.PF_FOLD_F32)):
-        def run(flags=flags):
-            ctx.check(ctx.lib.pf_ls_dev(ctx.handle, d_t.data_ptr(), d_m.data_ptr(),
-                                        off.ctypes.data, n_curves, d_p.data_ptr(), n_freq,
-                                        d_d.data_ptr(), 1, flags, pg.data_ptr(), s))
-        run()
-        ms_ = _event_ms(torch, run, max(1, args.steps), flush)
-        out["folds"][name] = {"ms": ms_, "evals_per_s": ev / (ms_ * 1e-3)}
-    print(json.dumps(out), flush=True)
-
-
-# ------------------------------------------------------------------- main
-
-
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--curves", type=int, default=N_CURVES)
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--workload", default="batch",
-                    choices=["batch", "small", "ragged", "lsgrad", "precision", "fpw", "bls",
-                             "device"],
-                    help="'small': CE stats on 100 x 1024; 'ragged': the mixed ragged batch; "
-                         "'lsgrad': LS derivatives and "
-                         "Newton refinement; 'precision': LS folds on the precision-study "
-                         "batch; 'fpw' / 'bls': FPW / BLS on the benchmark batch; 'device': "
-                         "periodograms of "
-                         "device-resident curves left on the GPU (separate reports, 1 GPU)")
-    args = ap.parse_args()
-    if args.impl == "reference":
-        reference_arm(args)
-        return
-    if args.workload != "batch":
-        {"small": small_arm, "ragged": ragged_arm, "lsgrad": lsgrad_arm,
-         "precision": precision_arm, "fpw": fpw_arm, "bls": lambda a: fpw_arm(a, bls=True),
-         "device": device_arm}[args.workload](args)
-        return
-
-    import torch
+    from periodfind_b200.distributed import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -841,98 +750,142 @@ def main():
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    # Each rank processes its own batch of curves (weak scaling, no exchange).
-    ts, ms, periods, pdts = make_workload(args.curves, SEED + rank)
-    from periodfind_b200 import _native as nat
-    from periodfind_b200.distributed import max_over_ranks
-
+    # Each rank searches its own batch of curves (weak scaling, no exchange).
+    n_curves = args.curves or RAGGED_CURVES
+    t, m, off = lc.ragged_batch(n_curves, SEED + 5 + rank)
+    periods, pdts = ragged_grid()
+    evals_algo = int(off[-1]) * len(periods) * len(pdts)
+    clocks = Clocks(local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-
     pipes = measure_pipes() if rank == 0 else {}
 
-    chosen = DeviceStep(ts, ms, periods, pdts, nat.PF_MODE_CHOSEN, torch, local)
-    clocks = ClockSampler(local)
+    step = RaggedStep(t, m, off, periods, pdts, torch, local)
+    stream = step.stream
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks.start()
-    ms_step, launches = time_device(chosen, args.steps, args.warmup, torch, flush)
-    clock_info = clocks.stop()
+    with clocks.region("chosen"):
+        ms_step, _ = time_steps(step.chosen, args.steps, args.warmup, torch, flush, stream)
+    if dist:
+        dist.barrier()
     ms_step = max_over_ranks(ms_step, device="cuda")
-    ce_ms, aov_ms = time_kernels(chosen, torch)
+    launches = args.steps * (step.plan_kernels + 2)  # + the two preparation kernels
 
-    plain = DeviceStep(ts, ms, periods, pdts, nat.PF_MODE_PLAIN, torch, local)
-    plain_ms, _ = time_device(plain, max(1, min(args.steps, 3)), 1, torch, flush)
+    with clocks.region("plain"):
+        plain_ms, _ = time_steps(step.plain, max(1, min(args.steps, 3)), 1, torch, flush,
+                                 stream)
     plain_ms = max_over_ranks(plain_ms, device="cuda")
-    del plain
 
-    e2e_s = time_e2e(ts, ms, periods, pdts, max(1, min(args.steps, 3)), 1, local)
+    # Per algorithm: the plan's replay (CUDA events), the fold / bin kernels
+    # alone (the library's events around the class launches of a direct
+    # chosen call, tuned by its first call), per-curve latency.
+    algo_ms, kernel_ms, latency = {}, {}, {}
+    for algo in ALGOS:
+        plan = step.plans[algo]
+        algo_ms[algo], _ = time_steps(lambda: plan.launch(stream), 3, 1, torch, flush, stream)
+        step.direct(algo, nat.PF_MODE_CHOSEN, peaks=False)
+        ks = []
+        for _ in range(3):
+            step.direct(algo, nat.PF_MODE_CHOSEN, peaks=False)
+            torch.cuda.synchronize()
+            ks.append(step.ctx.last_kernel_ms)
+        kernel_ms[algo] = float(np.mean(ks))
+        latency[algo] = {"chosen": curve_latency(step, algo, nat.PF_MODE_CHOSEN),
+                         "plain": curve_latency(step, algo, nat.PF_MODE_PLAIN)}
+    step.chosen()  # the chosen peaks back in pk_i / pk_v for the precision check
+    torch.cuda.synchronize()
+
+    hb = HostBatch(t, m, off)
+    with clocks.region("e2e"):
+        e2e_s, h2d, d2h, e2e_launches = e2e_cabi(hb, periods, pdts, max(1, min(args.steps, 3)),
+                                                 1, local)
     e2e_s = max_over_ranks(e2e_s, device="cuda")
     if dist:
         dist.barrier()
 
-    n_eval = evals_per_step(args.curves) * world
-    value = n_eval / (ms_step * 1e-3)
+    n_eval = 3 * evals_algo * world
     if rank == 0:
-        # Roofline of the dominant kernel (CE fold): FP64-pipe operations.
-        evals_ce = args.curves * N_POINTS * N_PERIODS * len(PDTS)
-        fp64_per_eval = FP64_OPS_PER_EVAL
-        achieved = evals_ce * fp64_per_eval / (ce_ms * 1e-3) / 1e9
-        peak = pipes.get("dfma", {}).get("per_s", float("nan")) / 1e9
-        in_bytes = args.curves * N_POINTS * 8 + N_PERIODS * 4
-        out_bytes = args.curves * N_PERIODS * len(PDTS) * 4
-        hbm_gbs = (in_bytes + out_bytes) / (ce_ms * 1e-3) / 1e9
-        cpu = None if args.no_cpu else cpu_baseline(ts, ms, periods, pdts)
-        h2d = 2 * sum(t.nbytes + m.nbytes for t, m in zip(ts, ms)) + 2 * (periods.nbytes + pdts.nbytes)
-        d2h = 2 * args.curves * N_PEAKS * 12
+        prec = ls_peak_error(step, periods, 64, torch)
+        calc_s = None if args.no_calc else e2e_calc(t, m, off, periods, pdts, local)
+        cpu = None if args.no_cpu else cpu_baseline(t, m, off, periods, pdts)
+        ref_cuda = None if args.no_cpu else reference_cuda(t, m, off, periods, pdts, clocks)
+        secondary = batch_secondary(torch, local, flush, clocks)
+        lens = np.diff(off)
         line = {
-            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "metric": METRIC, "value": n_eval / (ms_step * 1e-3), "unit": "evals/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 fold (exact), f32/fixed-point statistics", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "curves_per_gpu": args.curves,
-                       "points": N_POINTS, "periods": N_PERIODS, "pdts": list(PDTS),
-                       "l2": "flushed (256 MB write) between timed steps",
+            "dtype": "f64 bin fold (CE, AOV), split-precision f32 phase (LS), f32 / "
+                     "fixed-point statistics",
+            "data": "synthetic",
+            "config": {"workload": RAGGED_WORKLOAD, "curves_per_gpu": n_curves,
+                       "points_per_gpu": int(off[-1]), "mean_length": float(lens.mean()),
+                       "periods": len(periods), "pdts": [0.0], "evals_per_step": n_eval,
+                       "l2": "inputs (326 MB) and periodogram (8 GB) larger than L2; L2 also "
+                             "flushed (256 MB write) between timed steps",
                        "parallelism": f"{world} independent replicas (curves sharded)"},
             "plain": {"value": n_eval / (plain_ms * 1e-3), "ms_per_step": plain_ms,
                       "chosen_over_plain": plain_ms / ms_step},
-            "e2e": {"value": n_eval / e2e_s, "unit": "evals/s",
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "ms_per_step": e2e_s * 1e3,
-                    "path": "gpu.ConditionalEntropy/AOV.calc(list of numpy, output='peaks')"},
-            "roofline": {"bound": "fp64", "kernel": "CE fold (chosen)",
-                         "achieved": achieved, "peak": peak, "unit": "Gop/s",
-                         "frac": achieved / peak if peak == peak else None,
-                         "ops_per_eval": fp64_per_eval, "kernel_ms": ce_ms,
-                         "peak_source": "measured DFMA rate (periodfind_b200/csrc/pipe_peaks.cu)",
-                         "traffic": CE_TRAFFIC_BYTES,
-                         "shared_atomic_view": {
-                             "achieved_gops": evals_ce / (ce_ms * 1e-3) / 1e9,
-                             "peak_gops": pipes.get("atoms_u32_private", {}).get("per_s", float("nan")) / 1e9,
-                             "ops_per_eval": 1},
-                         "hbm_view": {"achieved_gbs": hbm_gbs, "peak_gbs": 6453.7,
-                                      "frac": hbm_gbs / 6453.7}},
-            "kernels_ms": {"ce_fold": ce_ms, "aov_fold": aov_ms},
+            "chosen_over_plain": plain_ms / ms_step,
+            "e2e": {"value": n_eval / e2e_s, "unit": "evals/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
+                    "path": "C ABI pf_ce_peaks / pf_aov_peaks / pf_ls_peaks from per-curve host "
+                            "arrays (PF_ASYNC pipeline), host magnitude preparation "
+                            "(pf_normalize_mags / pf_center_mags) inside the step"},
+            "e2e_calc": None if calc_s is None else {
+                "s_per_algo": calc_s, "value": n_eval / sum(calc_s.values()),
+                "path": "gpu.ConditionalEntropy / AOV / LombScargle .calc(list of numpy, "
+                        "output='peaks'), 3.2e6 Statistics objects per algorithm"},
+            "algo_ms": algo_ms, "kernels_ms": kernel_ms,
+            "latency_per_curve": latency,
+            "ls_peak_frequency_error": prec,
+            "roofline": _roofline(kernel_ms, evals_algo, pipes, off, periods, pdts),
             "pipes": {k: round(v["per_s"] / 1e12, 3) for k, v in pipes.items()},
             "cpu_baseline": cpu,
-            "clocks": clock_info,
+            "reference_cuda": ref_cuda,
+            "batch_4096": secondary,
+            "clocks": clocks.regions["chosen"],
+            "clocks_regions": clocks.regions,
             "gpu_launches": int(launches),
+            "e2e_gpu_launches_per_step": e2e_launches,
         }
         print(json.dumps(line), flush=True)
+    step.close()
     if dist:
         dist.destroy_process_group()
 
 
-# FP64-pipe operations per evaluation in the chosen CE bin kernel's fast
-# path: t * RN(1/P) (DMUL), floor (DADD.RD), bin with fraction bits
-# (DFMA.RD), plus DMUL + DFMA for t - c t^2 on the period-derivative cells.
-FP64_OPS_PER_EVAL = 3 + 2 * sum(1 for d in PDTS if d != 0.0) / len(PDTS)
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
-# full-size CE bin_kernel launch (1000 curves x 4096 points x 2e4 cells),
-# from one ncu capture of this benchmark.
-CE_TRAFFIC_BYTES = 52514048 + 28131328
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--curves", type=int, default=0,
+                    help="curves per GPU (default: the workload's own count)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU and reference baselines")
+    ap.add_argument("--no-calc", action="store_true", help="skip the Python calc() path")
+    ap.add_argument("--workload", default="ragged",
+                    choices=["ragged", "batch", "small", "lsgrad", "precision", "fpw", "bls",
+                             "device"],
+                    help="'ragged' (default): the mixed ragged batch; separate reports on 1 "
+                         "GPU: 'batch' CE + AOV on 1000 x 4096, 'small' CE stats on 100 x "
+                         "1024, 'lsgrad' LS derivatives and Newton refinement, 'precision' LS "
+                         "folds on the precision-study batch, 'fpw' / 'bls' on the 1000 x 4096 "
+                         "batch, 'device' device-resident periodograms")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    if args.workload == "ragged":
+        ragged_main(args)
+        return
+    from bench_reports import ARMS
+
+    ARMS[args.workload](args)
+
 
 if __name__ == "__main__":
     main()

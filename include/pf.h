@@ -343,6 +343,9 @@ int pf_plan_launch(pf_plan* plan, void* stream);
  * pf_plan_create on this thread. */
 const char* pf_plan_error(const pf_plan* plan);
 void pf_plan_destroy(pf_plan* plan);
+/* Number of kernel launches one pf_plan_launch replays (kernel nodes of the
+ * plan's graph); 0 for NULL. */
+uint64_t pf_plan_kernel_count(const pf_plan* plan);
 
 /* Per-curve device latency of the last PF_TIMING launch on this context:
  * out_ns[c] = last end - first start (ns) over the CTAs that computed curve
@@ -408,6 +411,15 @@ int pf_ls_refine_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
  * PF_EINVAL (numpy raises for them). */
 int pf_normalize_mags(const float* const* mags, const uint64_t* lengths, uint64_t n_curves,
                       float* const* out);
+
+/* The reference's center=True magnitude preparation
+ * (periodfind/_utils.py:35-37): out[c][i] = m[i] - np.mean(m) per curve in
+ * float32, bit-identical to numpy (its pairwise float32 sum, divided by the
+ * length, then one subtraction per point).  Host arrays; several host
+ * threads for large batches.  Empty curves are PF_EINVAL (numpy's mean of
+ * an empty array is NaN with a warning; callers keep that path). */
+int pf_center_mags(const float* const* mags, const uint64_t* lengths, uint64_t n_curves,
+                   float* const* out);
 
 /* The autotuner's decisions on this context, one line per (computation,
  * length class): the launch shape kept and the sample times of the fastest

@@ -1,4 +1,4 @@
-"""Seeded synthetic light curves for the tests and the benchmark.
+"""Seeded synthetic light curves for the tests and the benchmark (bench.py).
 
 Signal shapes follow what the reference's tests exercise (sinusoids,
 eclipsing binaries, sawtooth RR Lyrae-like curves, seasonal survey cadence:
@@ -127,3 +127,62 @@ def ls_study_curves(n_curves, seed, lengths=None, baseline=3000.0):
         fs.append(f)
         ss.append(s)
     return ts, ms, np.array(fs), np.array(ss)
+
+
+def ragged_batch(n_curves, seed, baseline=2500.0):
+    """The mixed ragged batch: lengths lognormal (median 300, sigma 0.8)
+    rounded and clipped to [20, 2000]; seasonal cadence over `baseline` days
+    (125.25-day seasons, a 240-day annual gap); a third sinusoids
+    (amplitude 0.3), a third box eclipses (depth 0.5, duty 0.05), a third
+    pure noise, periods log-uniform in [0.05, 500] d; noise sigma U[0.02,
+    0.1] per curve; magnitudes around 15.  Returns CSR (times float32,
+    mags float32, offsets int64), curve c = [off[c], off[c+1])."""
+    rng = np.random.default_rng(seed)
+    lens = np.clip(np.round(rng.lognormal(np.log(300.0), 0.8, n_curves)), 20, 2000).astype(np.int64)
+    cid = np.repeat(np.arange(n_curves), lens)
+    n_years = int(np.ceil(baseline / 365.25))
+    t = rng.integers(0, n_years, cid.size) * 365.25 + rng.uniform(0.0, 125.25, cid.size)
+    t = np.minimum(t, baseline)
+    order = np.lexsort((t, cid))
+    t = t[order].astype(np.float32)
+    period = np.exp(rng.uniform(np.log(0.05), np.log(500.0), n_curves))[cid]
+    phase = rng.uniform(0, 1, n_curves)[cid]
+    kind = (np.arange(n_curves) % 3)[cid]
+    sigma = rng.uniform(0.02, 0.1, n_curves)[cid]
+    ph = np.mod(t / period + phase, 1.0)
+    y = np.where(kind == 0, 0.3 * np.sin(2 * np.pi * ph),
+                 np.where(kind == 1, np.where(ph < 0.05, -0.5, 0.0), 0.0))
+    m = (15.0 + y + rng.normal(0.0, 1.0, cid.size) * sigma).astype(np.float32)
+    off = np.zeros(n_curves + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    return t, m, off
+
+
+def seasonal_ls_batch(lengths, seed, baseline=3000.0):
+    """LS study curves as CSR: seasonal cadence over `baseline` days
+    (240-day annual gap), 15 + A sin(2 pi f t) + N(0, sigma^2) with A ~
+    U[0.01, 0.5], sigma ~ U[0.01, 0.1], f ~ U[0.01, 20] / day; magnitudes
+    centred.  Returns (times float32, mags float32, offsets int64)."""
+    rng = np.random.default_rng(seed)
+    lengths = np.asarray(lengths, np.int64)
+    n_curves = len(lengths)
+    cid = np.repeat(np.arange(n_curves), lengths)
+    n_years = int(np.ceil(baseline / 365.25))
+    t = rng.integers(0, n_years, cid.size) * 365.25 + rng.uniform(0.0, 125.25, cid.size)
+    t = np.minimum(t, baseline)
+    t = t[np.lexsort((t, cid))].astype(np.float32)
+    amp = rng.uniform(0.01, 0.5, n_curves)[cid]
+    sig = rng.uniform(0.01, 0.1, n_curves)[cid]
+    f = rng.uniform(0.01, 20.0, n_curves)[cid]
+    ph = rng.uniform(0, 2 * np.pi, n_curves)[cid]
+    m = 15.0 + amp * np.sin(2 * np.pi * f * t.astype(np.float64) + ph)
+    m = m + rng.normal(0.0, 1.0, cid.size) * sig
+    off = np.zeros(n_curves + 1, np.int64)
+    np.cumsum(lengths, out=off[1:])
+    mean = np.add.reduceat(m, off[:-1]) / lengths
+    return t, (m - mean[cid]).astype(np.float32), off
+
+
+def split_csr(flat, off):
+    """The curves of a CSR array as a list of views (no copies)."""
+    return np.split(flat, off[1:-1])

@@ -90,11 +90,13 @@ SIGNATURES = {
     "pf_ls_refine_dev": ([_vp, _vp, _vp, _vp, _u64, _vp, _vp, _u64, _u32, _vp, _vp, _vp], _int),
     "pf_tuning_report": ([_vp, ctypes.c_char_p, _u64], _int),
     "pf_normalize_mags": ([_vp, _vp, _u64, _vp], _int),
+    "pf_center_mags": ([_vp, _vp, _u64, _vp], _int),
     "pf_plan_create": ([_int, _int, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32,
                         _u32, _int, _vp, _u32, _u32, _vp, _vp, ctypes.POINTER(_vp)], _int),
     "pf_plan_launch": ([_vp, _vp], _int),
     "pf_plan_error": ([_vp], ctypes.c_char_p),
     "pf_plan_destroy": ([_vp], None),
+    "pf_plan_kernel_count": ([_vp], _u64),
     "pf_launch_count": ([_vp], _u64),
     "pf_last_kernel_ms": ([_vp], ctypes.c_double),
 }

@@ -43,26 +43,31 @@ def prepare_magnitudes(mags, center, normalize):
             stacklevel=3,
         )
     if center:
-        return [mag - np.mean(mag) for mag in mags]
+        return _prepare_batch(mags, "pf_center_mags", _center_one)
     if normalize:
-        return _normalize_batch(mags)
+        return _prepare_batch(mags, "pf_normalize_mags", _normalize_one)
     return mags
 
 
-def _normalize_batch(mags):
-    """The per-curve normalisation of a whole batch in the native library:
-    the same float32 expression with exact per-curve min / max, so every
-    value equals numpy's one-curve-at-a-time result.  Batches with an empty
-    curve, or not all float32 1-D, take the per-curve numpy path (and its
-    errors)."""
+def _center_one(mag):
+    return mag - np.mean(mag)
+
+
+def _normalize_one(mag):
+    lo = np.min(mag)
+    hi = np.max(mag)
+    return ((mag - lo) / (hi - lo)) * 0.999 + 5e-4
+
+
+def _prepare_batch(mags, native_fn, one):
+    """Centre or normalise a whole batch in the native library
+    (pf_center_mags / pf_normalize_mags): numpy's float32 arithmetic per
+    curve, so every value equals numpy's one-curve-at-a-time result.
+    Batches with an empty curve, or not all float32 1-D, take the per-curve
+    numpy path `one` (and its warnings and errors)."""
     arrs = [np.asarray(m) for m in mags]
     if not arrs or any(a.ndim != 1 or a.size == 0 or a.dtype != np.float32 for a in arrs):
-        out = []
-        for mag in mags:
-            lo = np.min(mag)
-            hi = np.max(mag)
-            out.append(((mag - lo) / (hi - lo)) * 0.999 + 5e-4)
-        return out
+        return [one(mag) for mag in mags]
     # In the native library (multithreaded, same float32 arithmetic).
     from . import _native as nat
 
@@ -73,10 +78,10 @@ def _normalize_batch(mags):
     src, keep = nat.host_pointers(arrs, lens)
     flat = np.empty(int(lens.sum()), dtype=np.float32)
     dst = (np.uint64(flat.ctypes.data) + np.uint64(4) * starts).astype(np.uintp)
-    rc = nat.load().pf_normalize_mags(src.ctypes.data, lens.ctypes.data, n, dst.ctypes.data)
+    rc = getattr(nat.load(), native_fn)(src.ctypes.data, lens.ctypes.data, n, dst.ctypes.data)
     del keep
     if rc != nat.PF_OK:
-        raise RuntimeError(f"magnitude normalisation failed ({rc})")
+        raise RuntimeError(f"magnitude preparation failed ({rc})")
     bounds = starts.tolist() + [flat.shape[0]]
     return nat.FlatList([flat[a:b] for a, b in zip(bounds[:-1], bounds[1:])], flat, dst)
 

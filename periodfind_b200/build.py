@@ -3,9 +3,8 @@
     python -m periodfind_b200.build            # incremental
     python -m periodfind_b200.build --force    # rebuild everything
 
-Outputs (next to this file):
-    libpfb200.so   the C ABI of include/pf.h and its kernels
-    libpfpeaks.so  the pipe-throughput probes used for roofline denominators
+Output (next to this file): libpfb200.so, the C ABI of include/pf.h and its
+kernels.
 
 Per-translation-unit flags carry the two arithmetic semantics:
     kern_cudasem.cu  -use_fast_math   (the reference's CUDA build flags)
@@ -40,7 +39,6 @@ UNITS = {
 }
 
 LIB = os.path.join(HERE, "libpfb200.so")
-PEAKS_LIB = os.path.join(HERE, "libpfpeaks.so")
 
 
 def nvcc() -> str:
@@ -80,10 +78,6 @@ def build(force: bool = False, verbose: bool = True) -> str:
         objs = [f.result() for f in futs]
     if force or _mtime(LIB) < max(_mtime(o) for o in objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + sorted(objs) + ["-lpthread"]
-        subprocess.run(cmd, check=True)
-    src = os.path.join(CSRC, "pipe_peaks.cu")
-    if force or _mtime(PEAKS_LIB) < _mtime(src):
-        cmd = [nvcc()] + COMMON + ARCH + ["-shared", "-o", PEAKS_LIB, src]
         subprocess.run(cmd, check=True)
     if verbose:
         print(f"built {LIB}")

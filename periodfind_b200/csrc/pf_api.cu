@@ -1191,6 +1191,53 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
     return PF_OK;
 }
 
+// numpy's pairwise float32 summation (the add.reduce behind np.mean of a
+// contiguous float32 array; numpy/_core/src/umath/loops_utils.h.src,
+// pairwise_sum): fewer than 8 elements are added in order starting from
+// -0.0; up to 128 elements go to eight interleaved accumulators, combined as
+// ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7)), then the remainder in
+// order; a longer range splits at n / 2 rounded down to a multiple of 8 and
+// the two halves' sums are added.  This unit is built without contraction,
+// so every addition is one IEEE float32 rounding, as in numpy.
+float numpy_pairwise_sum(const float* a, uint64_t n) {
+    if (n < 8) {
+        float res = -0.0f;
+        for (uint64_t i = 0; i < n; i++) res += a[i];
+        return res;
+    }
+    if (n <= 128) {
+        float r[8];
+        for (int k = 0; k < 8; k++) r[k] = a[k];
+        uint64_t i = 8;
+        for (; i < n - (n % 8); i += 8)
+            for (int k = 0; k < 8; k++) r[k] += a[i + k];
+        float res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+        for (; i < n; i++) res += a[i];
+        return res;
+    }
+    uint64_t n2 = n / 2;
+    n2 -= n2 % 8;
+    return numpy_pairwise_sum(a, n2) + numpy_pairwise_sum(a + n2, n - n2);
+}
+
+// Run fn(c) for every curve, on several host threads when the batch holds
+// more than 2^20 points (curves interleaved across the threads).
+template <class F>
+void for_each_curve(uint64_t n_curves, uint64_t total_points, F& fn) {
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const unsigned nthr = total_points > (1u << 20) ? hw : 1u;
+    if (nthr == 1) {
+        for (uint64_t c = 0; c < n_curves; c++) fn(c);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned w = 0; w < nthr; w++)
+        th.emplace_back([&, w] {
+            for (uint64_t c = w; c < n_curves; c += nthr) fn(c);
+        });
+    for (auto& t : th) t.join();
+}
+
 }  // namespace
 
 size_t pfk::fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag) {
@@ -1338,18 +1385,29 @@ int pf_normalize_mags(const float* const* mags, const uint64_t* lengths, uint64_
         float* o = out[c];
         for (uint64_t i = 0; i < n; i++) o[i] = ((m[i] - lo) / range) * 0.999f + 5e-4f;
     };
-    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    const unsigned nthr = total > (1u << 20) ? hw : 1u;
-    if (nthr == 1) {
-        for (uint64_t c = 0; c < n_curves; c++) one(c);
-        return PF_OK;
+    for_each_curve(n_curves, total, one);
+    return PF_OK;
+}
+
+int pf_center_mags(const float* const* mags, const uint64_t* lengths, uint64_t n_curves,
+                   float* const* out) {
+    if (n_curves == 0) return PF_OK;
+    if (!mags || !lengths || !out) return PF_EINVAL;
+    uint64_t total = 0;
+    for (uint64_t c = 0; c < n_curves; c++) {
+        if (lengths[c] == 0 || !mags[c] || !out[c]) return PF_EINVAL;
+        total += lengths[c];
     }
-    std::vector<std::thread> th;
-    for (unsigned w = 0; w < nthr; w++)
-        th.emplace_back([&, w] {
-            for (uint64_t c = w; c < n_curves; c += nthr) one(c);
-        });
-    for (auto& t : th) t.join();
+    // np.mean of a float32 array: the pairwise float32 sum divided by the
+    // length in float32; then m - mean, one rounding per point.
+    auto one = [&](uint64_t c) {
+        const float* m = mags[c];
+        const uint64_t n = lengths[c];
+        const float mean = numpy_pairwise_sum(m, n) / (float)n;
+        float* o = out[c];
+        for (uint64_t i = 0; i < n; i++) o[i] = m[i] - mean;
+    };
+    for_each_curve(n_curves, total, one);
     return PF_OK;
 }
 
@@ -1948,6 +2006,20 @@ void pf_plan_destroy(pf_plan* plan) {
     if (plan->graph) cudaGraphDestroy(plan->graph);
     if (plan->ctx) pf_ctx_destroy(plan->ctx);
     delete plan;
+}
+
+uint64_t pf_plan_kernel_count(const pf_plan* plan) {
+    if (!plan || !plan->graph) return 0;
+    size_t n = 0;
+    if (cudaGraphGetNodes(plan->graph, nullptr, &n) != cudaSuccess) return 0;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n && cudaGraphGetNodes(plan->graph, nodes.data(), &n) != cudaSuccess) return 0;
+    uint64_t k = 0;
+    for (size_t i = 0; i < n; i++) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
 }
 
 int pf_ce_stats(pf_ctx* ctx, const float* const* times, const float* const* mags,

@@ -41,7 +41,7 @@ def _worker(rank, world, port, q):
 
     from oracle import oracle as O
     from periodfind_b200.distributed import calc_sharded, max_over_ranks
-    from tests import lightcurves as lc
+    import lightcurves as lc
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from periodfind_b200 import Periodogram, Statistics
-from tests import lightcurves as lc
+import lightcurves as lc
 
 pytestmark = pytest.mark.gpu
 

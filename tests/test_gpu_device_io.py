@@ -7,7 +7,7 @@ import warnings
 import numpy as np
 import pytest
 
-from tests import lightcurves as lc
+import lightcurves as lc
 
 pytestmark = pytest.mark.gpu
 

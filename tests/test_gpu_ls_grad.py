@@ -16,7 +16,7 @@ Tolerances (FP32 sums, FP64 phase reduction):
 import numpy as np
 import pytest
 
-from tests import lightcurves as lc
+import lightcurves as lc
 from tests.ls_reference import ls_power_tau
 
 pytestmark = pytest.mark.gpu

@@ -21,7 +21,7 @@ Tolerances, written per comparison:
 import numpy as np
 import pytest
 
-from tests import lightcurves as lc
+import lightcurves as lc
 
 pytestmark = pytest.mark.gpu
 
@@ -153,7 +153,7 @@ def test_bin_kernel_occupancy_exact_at_scale(gpu, pdts):
     reference's sequence near edges) against the plain kernel's reference
     fold: identical CE values over ~1.2e9 evaluations, i.e. identical
     histograms, including long baselines (MJD-like times, short periods)."""
-    from tests import lightcurves as lc2
+    import lightcurves as lc2
 
     ts, ms = lc2.mixed_signal_batch(48, 4096, 1234)
     rng = np.random.default_rng(5)

@@ -21,7 +21,7 @@ import os
 import numpy as np
 import pytest
 
-from tests import lightcurves as lc
+import lightcurves as lc
 
 pytestmark = pytest.mark.gpu
 

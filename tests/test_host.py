@@ -202,6 +202,37 @@ def test_native_normalisation_matches_numpy_bit_for_bit():
         prepare_magnitudes([np.zeros(0, np.float32)], False, True)
 
 
+def test_native_centring_matches_numpy_bit_for_bit():
+    """prepare_magnitudes(center=True) runs in the native library
+    (pf_center_mags, numpy's pairwise float32 sum) for float32 batches;
+    every value equals m - np.mean(m), across the pairwise sum's block
+    boundaries (7/8/9, 127/128/129 points and longer splits) and with
+    NaN, inf, constant and single-point curves."""
+    import warnings
+
+    from periodfind_b200._utils import prepare_magnitudes
+
+    rng = np.random.default_rng(13)
+    lens = [1, 2, 7, 8, 9, 15, 16, 17, 127, 128, 129, 255, 256, 257, 1023, 1024, 1025, 4097,
+            20000, 65537] + [int(n) for n in rng.integers(1, 3000, 200)]
+    ms = [(15 + rng.normal(0, 1, n) * rng.uniform(0.01, 3)).astype(np.float32) for n in lens]
+    ms[30][5] = np.nan
+    ms[31][:] = 7.25
+    ms[32][2] = np.inf
+    ms[33] = (rng.normal(size=777) * 1e-30).astype(np.float32)
+    got = prepare_magnitudes(ms, True, False)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        want = [m - np.mean(m) for m in ms]
+    for g, w in zip(got, want):
+        assert g.dtype == w.dtype == np.float32
+        np.testing.assert_array_equal(g, w)
+    # an empty curve keeps numpy's behaviour (NaN mean, a warning)
+    with pytest.warns(RuntimeWarning):
+        out = prepare_magnitudes([np.zeros(0, np.float32), np.ones(3, np.float32)], True, False)
+    assert out[0].size == 0 and np.array_equal(out[1], np.zeros(3, np.float32))
+
+
 def test_result_building_restores_collector_state():
     """Result objects are built with the cyclic collector paused; its state
     afterwards is the caller's, enabled or disabled, and the results are

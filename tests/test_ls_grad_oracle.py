@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 import torch
 
-from tests import lightcurves as lc
+import lightcurves as lc
 from tests.ls_reference import ls_power_tau
 
 

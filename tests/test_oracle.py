@@ -9,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-from tests import lightcurves as lc
+import lightcurves as lc
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "peaks_golden.json")
 

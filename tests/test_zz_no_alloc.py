@@ -18,7 +18,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from tests import lightcurves as lc
+import lightcurves as lc
 
 pytestmark = pytest.mark.gpu
 
