@@ -136,6 +136,24 @@ int pf_ls(pf_ctx* ctx, const float* const* times, const float* const* mags,
           uint64_t n_per, const float* period_dts, uint64_t n_pdt, int mode,
           float* out);
 
+/* The bins behind a CE or AOV periodogram, for occupancy checks: the
+ * counterpart of ConditionalEntropy::FoldAndBin (periodfind/cuda/ce.h:194,
+ * ce.cu:262-290, which returns count / (N * po * mo) per bin) and
+ * AOV::FoldAndBin (periodfind/cuda/aov.h:132, whose AOVData holds the
+ * count per bin).  algo is PF_ALGO_CE or PF_ALGO_AOV (n_mag and
+ * mag_overlap are ignored for AOV).  Computes the periodogram into `out`
+ * as pf_ce / pf_aov do and writes the raw u32 count of every bin of every
+ * cell into out_counts, [curve][period][pdt][bin] with bin = phase_bin *
+ * n_mag + mag_bin (CE) or phase_bin (AOV): n_curves * n_per * n_pdt *
+ * (n_phase * n_mag or n_phase) entries.  With PF_MODE_CHOSEN the counts come
+ * from the chosen kernels with PF_REF_STATS implied.  PF_ASYNC and
+ * PF_TIMING are rejected. */
+int pf_bin_counts(pf_ctx* ctx, int algo, const float* const* times,
+                  const float* const* mags, const uint64_t* lengths, uint64_t n_curves,
+                  const float* periods, uint64_t n_per, const float* period_dts,
+                  uint64_t n_pdt, uint32_t n_phase, uint32_t n_mag, uint32_t phase_overlap,
+                  uint32_t mag_overlap, int mode, float* out, uint32_t* out_counts);
+
 /* ----------------------------------------------------------------- peaks */
 
 /* Periodogram + top-N peak search without returning the periodogram.

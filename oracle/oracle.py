@@ -393,3 +393,42 @@ def ref_cuda(algo, times, mags, periods, pdts, **kw):
     else:
         raise ValueError(algo)
     return out
+
+
+def ref_fold_and_bin(algo, t, m, periods, pdts, n_phase=10, n_mag=10, po=1, mo=1):
+    """The reference CUDA build's own bins for one curve, from its
+    FoldAndBin step on the GPU (ConditionalEntropy::DeviceFoldAndBin,
+    periodfind/cuda/ce.cu:262-290; AOV::DeviceFoldAndBin, aov.cu:265-299).
+
+    CE: raw counts [n_per, n_pdt, n_phase * n_mag] uint32, recovered from
+    the reference's count / (N * po * mo) floats (exact: the quotient is
+    within 2 ulp of the true ratio and the counts are below 2^21).
+    AOV: (counts [n_per, n_pdt, n_phase] uint32, sums, squared sums float32)
+    exactly as the reference's AOVData holds them."""
+    import torch
+
+    lib = _load_ref()
+    i64, u32, vp = ctypes.c_uint64, ctypes.c_uint32, ctypes.c_void_p
+    lib.pfref_ce_hists.argtypes = [vp, vp, i64, vp, vp, i64, i64, u32, u32, u32, u32, vp]
+    lib.pfref_aov_bins.argtypes = [vp, vp, i64, vp, vp, i64, i64, u32, u32, vp]
+    dev = torch.device("cuda")
+    cuda = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    d_t, d_m, d_p, d_d = cuda(t), cuda(m), cuda(periods), cuda(pdts)
+    n, n_per, n_pdt = len(t), len(periods), len(pdts)
+    if algo == "ce":
+        h = np.zeros((n_per, n_pdt, n_phase * n_mag), np.float32)
+        rc = lib.pfref_ce_hists(d_t.data_ptr(), d_m.data_ptr(), n, d_p.data_ptr(),
+                                d_d.data_ptr(), n_per, n_pdt, n_phase, n_mag, po, mo,
+                                h.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("reference FoldAndBin failed")
+        div = float(n * po * mo)
+        counts = np.rint(h.astype(np.float64) * div).astype(np.uint32)
+        return counts
+    raw = np.zeros((n_per, n_pdt, n_phase, 3), np.uint32)
+    rc = lib.pfref_aov_bins(d_t.data_ptr(), d_m.data_ptr(), n, d_p.data_ptr(), d_d.data_ptr(),
+                            n_per, n_pdt, n_phase, po, raw.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("reference FoldAndBin failed")
+    return (raw[..., 0].copy(), raw[..., 1].copy().view(np.float32),
+            raw[..., 2].copy().view(np.float32))

@@ -51,6 +51,8 @@ SIGNATURES = {
                _vp], _int),
     "pf_aov": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int, _vp], _int),
     "pf_ls": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _int, _vp], _int),
+    "pf_bin_counts": ([_vp, _int, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32,
+                       _u32, _int, _vp, _vp], _int),
     "pf_ce_peaks": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32,
                      _u32, _u32, _int, _vp, _vp], _int),
     "pf_aov_peaks": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32,

@@ -61,6 +61,7 @@ struct pf_ctx {
     bool staged_pending = false, done_recorded = false, timed_pending = false;
     std::string err;
     DevBuf d_in, d_aux32, d_aux64, d_out, d_pidx, d_pval, d_pack, d_misc, d_stamps, d_stat;
+    DevBuf d_bins;  // pf_bin_counts: raw bin counts per cell
     // pf_prepare_mags_dev: the curve offsets on the device, and the event
     // after the last kernel that read them (the buffer is rewritten only
     // once that kernel is done).
@@ -182,7 +183,14 @@ struct Job {
     bool stats = false;
     uint32_t n_top = 0;
     float* out_stats = nullptr;
+    // pf_bin_counts: raw bin counts per cell ([curve][period][pdt][bins]).
+    uint32_t* out_bins = nullptr;
 };
+
+// Bins per cell of a bin-count call: n_phase x n_mag (CE), n_phase (AOV).
+size_t bins_per_cell(const Job& j) {
+    return j.algo == ALGO_CE ? (size_t)j.n_phase * j.n_mag : (size_t)j.n_phase;
+}
 
 // Layout of the packed input block (host staging and its device copy).
 struct Layout {
@@ -870,9 +878,18 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
     p.pdts = (const float*)(db + L.o_pdts);
     const size_t out_bytes = (size_t)j.n_curves * n_cells * 4;
     if ((rc = ensure_dev(ctx, ctx->d_out, out_bytes)) != PF_OK) return rc;
+    const size_t bins_bytes = j.out_bins ? out_bytes * bins_per_cell(j) : 0;
+    if (j.out_bins) {
+        if ((rc = ensure_dev(ctx, ctx->d_bins, bins_bytes)) != PF_OK) return rc;
+        PF_CUDA(cudaMemsetAsync(ctx->d_bins.p, 0, bins_bytes, s), "memset");
+        p.bins = (uint32_t*)ctx->d_bins.p;
+    }
     rc = device_pipeline(ctx, j, L, cfg, p, (CurveDesc*)(db + L.o_curves), (float*)ctx->d_out.p,
                          s);
     if (rc != PF_OK) return rc;
+    if (j.out_bins)
+        PF_CUDA(cudaMemcpyAsync(j.out_bins, ctx->d_bins.p, bins_bytes, cudaMemcpyDeviceToHost, s),
+                "D2H bin counts");
     if (j.stats) {
         PF_CUDA(cudaMemcpyAsync(j.out_stats, ctx->d_stat.p, (size_t)j.n_curves * 16,
                                 cudaMemcpyDeviceToHost, s),
@@ -1305,7 +1322,7 @@ void pf_ctx_destroy(pf_ctx* ctx) {
     if (ctx->done_recorded) cudaEventSynchronize(ctx->ev_done);
     if (ctx->prep_pending) cudaEventSynchronize(ctx->ev_prep);
     for (DevBuf* b : {&ctx->d_in, &ctx->d_aux32, &ctx->d_aux64, &ctx->d_out, &ctx->d_pidx,
-                      &ctx->d_pval, &ctx->d_pack, &ctx->d_misc, &ctx->d_stamps, &ctx->d_stat,
+                      &ctx->d_pval, &ctx->d_pack, &ctx->d_misc, &ctx->d_stamps, &ctx->d_stat, &ctx->d_bins,
                       &ctx->d_prep})
         if (b->p) cudaFree(b->p);
     if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
@@ -1620,6 +1637,36 @@ int pf_aov(pf_ctx* ctx, const float* const* times, const float* const* mags,
     j.n_phase = n_phase;
     j.po = phase_overlap;
     j.out = out;
+    return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_bin_counts(pf_ctx* ctx, int algo, const float* const* times, const float* const* mags,
+                  const uint64_t* lengths, uint64_t n_curves, const float* periods,
+                  uint64_t n_per, const float* period_dts, uint64_t n_pdt, uint32_t n_phase,
+                  uint32_t n_mag, uint32_t phase_overlap, uint32_t mag_overlap, int mode,
+                  float* out, uint32_t* out_counts) {
+    if (!ctx) return PF_EINVAL;
+    if (algo != PF_ALGO_CE && algo != PF_ALGO_AOV)
+        return fail(ctx, PF_EINVAL, "bin counts exist for PF_ALGO_CE and PF_ALGO_AOV only");
+    if (mode & (PF_ASYNC | PF_TIMING))
+        return fail(ctx, PF_EINVAL, "PF_ASYNC / PF_TIMING do not apply to pf_bin_counts");
+    if (n_curves > 0 && n_per > 0 && n_pdt > 0 && !out_counts)
+        return fail(ctx, PF_EINVAL, "out_counts is NULL");
+    Job j;
+    j.algo = algo == PF_ALGO_CE ? ALGO_CE : ALGO_AOV;
+    // The chosen form writes its counts from the reference-statistic epilogue.
+    j.mode = (mode & PF_MODE_CHOSEN) ? (mode | PF_REF_STATS) : mode;
+    j.n_curves = n_curves;
+    j.periods = periods;
+    j.n_per = n_per;
+    j.pdts = period_dts;
+    j.n_pdt = n_pdt;
+    j.n_phase = n_phase;
+    j.n_mag = algo == PF_ALGO_CE ? n_mag : 1;
+    j.po = phase_overlap;
+    j.mo = algo == PF_ALGO_CE ? mag_overlap : 1;
+    j.out = out;
+    j.out_bins = out_counts;
     return run_host(ctx, j, times, mags, lengths);
 }
 

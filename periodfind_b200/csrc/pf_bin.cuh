@@ -363,6 +363,11 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
                 return cnt32[(j * W + i) * BLOCK + tid];
             }
         };
+        if (p.bins) {
+            uint32_t* o = p.bins + out_idx * ((size_t)nP * nM);
+            for (uint32_t j = 0; j < nP; j++)
+                for (uint32_t i = 0; i < nM; i++) o[j * nM + i] = count(j, i);
+        }
         const float divf = (float)((unsigned long long)n * p.p_overlap * p.m_overlap);
         float ce = 0.0f;
         for (uint32_t j = 0; j < nP; j++) {
@@ -385,6 +390,10 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
         p.out[out_idx] = ce;
     } else {
         const uint32_t* sums = cnt32 + nP * BLOCK;
+        if (p.bins) {
+            uint32_t* o = p.bins + out_idx * (size_t)nP;
+            for (uint32_t b = 0; b < nP; b++) o[b] = cnt32[b * BLOCK + tid];
+        }
         const double xbar = cd.fix_sumx / (double)n;
         double s1 = 0.0, sbx = 0.0;
         for (uint32_t b = 0; b < nP; b++) {

@@ -479,6 +479,10 @@ __device__ __forceinline__ void fold_item(const FoldParams& p, const WorkItem w,
             for (uint32_t mb = 0; mb < nM; mb++)
                 hist[mb * BLOCK + tid] += hist[(nP * nM + mb) * BLOCK + tid];
         }
+        if (p.bins) {
+            uint32_t* o = p.bins + out_idx * ((size_t)nP * nM);
+            for (uint32_t k = 0; k < nP * nM; k++) o[k] = hist[k * BLOCK + tid];
+        }
         const float divf = (float)((unsigned long long)n * po * mo);
         float ce = 0.0f;
         for (uint32_t j = 0; j < nP; j++) {
@@ -506,6 +510,11 @@ __device__ __forceinline__ void fold_item(const FoldParams& p, const WorkItem w,
         if constexpr (ACC == AOVACC_FIX) {
             unsigned long long* hist64 = v.hist64;
             if constexpr (!OVL) hist64[tid] += hist64[nP * BLOCK + tid];
+            if (p.bins) {
+                uint32_t* o = p.bins + out_idx * (size_t)nP;
+                for (uint32_t b = 0; b < nP; b++)
+                    o[b] = (uint32_t)(hist64[b * BLOCK + tid] >> kFixCountShift);
+            }
             const unsigned long long mask = (1ull << kFixCountShift) - 1ull;
             const double xbar = cd.fix_sumx / (double)n;
             double s1 = 0.0, sbx = 0.0;
@@ -532,6 +541,10 @@ __device__ __forceinline__ void fold_item(const FoldParams& p, const WorkItem w,
             p.out[out_idx] = res;
         } else {
             // periodfind/cuda/aov.cu:225-244 / rust/src/aov.rs:184-201.
+            if (p.bins) {
+                uint32_t* o = p.bins + out_idx * (size_t)nP;
+                for (uint32_t b = 0; b < nP; b++) o[b] = v.a_cnt[b * BLOCK + tid];
+            }
             const float avg = cd.avg;
             float s1 = 0;
             float s2 = 0;

@@ -76,6 +76,10 @@ struct FoldParams {
     uint32_t edge_d;            // bin-edge guard (units of 2^-20 of a bin)
     unsigned long long* stamps; // optional: [work item][start, end] globaltimer ns
     WorkQueue q;                // persistent kernels (instead of `work`)
+    // Optional (occupancy tests): raw bin counts per cell, [curve][n_per]
+    // [n_pdt][bins] with bins = n_phase * n_mag (CE) or n_phase (AOV).
+    // Written by the plain kernels and the chosen reference-statistic form.
+    uint32_t* bins;
 };
 
 // Shared-memory bytes of the chosen bin kernel (pf_bin.cuh).

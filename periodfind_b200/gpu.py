@@ -108,6 +108,31 @@ class _Periodogram:
             ctx.check(self._native_pgram(ctx, b, periods, period_dts, out))
         return out
 
+    def bin_counts(self, times, mags, periods, period_dts):
+        """(periodogram float32 [n_curves, n_periods, n_pdts], raw bin counts
+        uint32 [n_curves, n_periods, n_pdts, bins]) for prepared magnitudes,
+        from this object's kernels (pf_bin_counts); bins = n_phase * n_mag
+        (CE, phase-major) or n_phase (AOV).  The counterpart of the
+        reference's ConditionalEntropy::FoldAndBin / AOV::FoldAndBin
+        (periodfind/cuda/ce.h:194, aov.h:132), for occupancy checks.  CE and
+        AOV only."""
+        if not hasattr(self, "_bin_args"):
+            raise NotImplementedError("bin counts exist for ConditionalEntropy and AOV only")
+        algo, n_phase, n_mag, po, mo = self._bin_args()
+        periods = _grid(periods, "periods")
+        period_dts = _grid(period_dts, "period_dts")
+        ctx = nat.default_context(self.device)
+        b = nat.CurveBatch(times, mags)
+        nb = n_phase * n_mag if algo == nat.PF_ALGO_CE else n_phase
+        out = np.empty((b.n, len(periods), len(period_dts)), dtype=np.float32)
+        counts = np.zeros((b.n, len(periods), len(period_dts), nb), dtype=np.uint32)
+        with ctx.lock:
+            ctx.check(ctx.lib.pf_bin_counts(ctx.handle, algo, *b.args(), nat.ptr(periods),
+                                            len(periods), nat.ptr(period_dts), len(period_dts),
+                                            n_phase, n_mag, po, mo, self._flags, nat.ptr(out),
+                                            nat.ptr(counts)))
+        return out, counts
+
     def periodograms_device(self, t, m, offsets, periods, period_dts, normalize=None,
                             center=None):
         """Periodograms of curves already on the GPU, left on the GPU.
@@ -347,6 +372,10 @@ class ConditionalEntropy(_Periodogram):
         self.phase_bin_extent = int(phase_bin_extent)
         self.mag_bin_extent = int(mag_bin_extent)
 
+    def _bin_args(self):
+        return (nat.PF_ALGO_CE, self.n_phase, self.n_mag, self.phase_bin_extent,
+                self.mag_bin_extent)
+
     def _native_pgram(self, ctx, b, periods, pdts, out):
         return ctx.lib.pf_ce(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                              nat.ptr(pdts), len(pdts), self.n_phase, self.n_mag,
@@ -384,6 +413,9 @@ class AOV(_Periodogram):
         super().__init__(mode=mode, semantics=semantics, device=device)
         self.n_phase = int(n_phase)
         self.phase_bin_extent = int(phase_bin_extent)
+
+    def _bin_args(self):
+        return (nat.PF_ALGO_AOV, self.n_phase, 1, self.phase_bin_extent, 1)
 
     def _native_pgram(self, ctx, b, periods, pdts, out):
         return ctx.lib.pf_aov(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
