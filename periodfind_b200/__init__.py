@@ -12,7 +12,7 @@ load the native library; constructing a GPU class does, and raises if it is
 absent or no B200 is visible.
 """
 
-from .stats import Periodogram, Statistics
+from .results import Periodogram, Statistics
 
 __all__ = ["Statistics", "Periodogram", "ConditionalEntropy", "AOV", "LombScargle", "FPW",
            "BoxLeastSquares", "gpu"]

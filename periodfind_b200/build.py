@@ -3,8 +3,12 @@
     python -m periodfind_b200.build            # incremental
     python -m periodfind_b200.build --force    # rebuild everything
 
-Output (next to this file): libpfb200.so, the C ABI of include/pf.h and its
-kernels.
+Outputs:
+    libpfb200.so            (next to this file) the C ABI of include/pf.h and
+                            its kernels
+    dropin/periodfind/*.so  the Cython modules ce, aov, ls, fpw, bls that take
+                            the place of periodfind's own .pyx modules inside
+                            the periodfind package, calling libpfb200.so
 
 Per-translation-unit flags carry the two arithmetic semantics:
     kern_cudasem.cu  -use_fast_math   (the reference's CUDA build flags)
@@ -39,6 +43,9 @@ UNITS = {
 }
 
 LIB = os.path.join(HERE, "libpfb200.so")
+DROPIN = os.path.join(HERE, "dropin")
+DROPIN_OUT = os.path.join(DROPIN, "periodfind")
+DROPIN_MODULES = ("ce", "aov", "ls", "fpw", "bls")
 
 
 def nvcc() -> str:
@@ -79,9 +86,44 @@ def build(force: bool = False, verbose: bool = True) -> str:
     if force or _mtime(LIB) < max(_mtime(o) for o in objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + sorted(objs) + ["-lpthread"]
         subprocess.run(cmd, check=True)
+    build_dropin(force)
     if verbose:
         print(f"built {LIB}")
     return LIB
+
+
+def _dropin_one(name: str, force: bool) -> str:
+    """Cython -> C -> one extension module, linked to libpfb200.so (found at
+    run time two directories up, through the rpath)."""
+    import sysconfig
+
+    import numpy as np
+
+    pyx = os.path.join(DROPIN, name + ".pyx")
+    so = os.path.join(DROPIN_OUT, name + sysconfig.get_config_var("EXT_SUFFIX"))
+    deps = [pyx, os.path.join(DROPIN, "_common.pxi"), os.path.join(DROPIN, "pf_abi.pxd"),
+            os.path.join(INCLUDE, "pf.h"), LIB]
+    if not force and _mtime(so) > max(_mtime(d) for d in deps):
+        return so
+    c_src = os.path.join(OBJ, f"dropin_{name}.c")
+    r = subprocess.run([sys.executable, "-m", "cython", "-3", "--module-name", f"periodfind.{name}",
+                        "-I", DROPIN, "-o", c_src, pyx],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"cython failed for {name}.pyx:\n{r.stdout}\n{r.stderr}")
+    cmd = ["gcc", "-O2", "-shared", "-fPIC", "-DNPY_NO_DEPRECATED_API=NPY_1_7_API_VERSION",
+           f"-I{sysconfig.get_paths()['include']}", f"-I{np.get_include()}", f"-I{INCLUDE}",
+           c_src, "-o", so, f"-L{HERE}", "-lpfb200", "-Wl,-rpath,$ORIGIN/../.."]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"gcc failed for {name}:\n{r.stdout}\n{r.stderr}")
+    return so
+
+
+def build_dropin(force: bool = False) -> list[str]:
+    os.makedirs(DROPIN_OUT, exist_ok=True)
+    with cf.ThreadPoolExecutor(max_workers=len(DROPIN_MODULES)) as ex:
+        return list(ex.map(lambda n: _dropin_one(n, force), DROPIN_MODULES))
 
 
 if __name__ == "__main__":

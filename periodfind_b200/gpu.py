@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _native as nat
 from ._utils import ensure_float32, gc_paused, prepare_magnitudes, validate_inputs
-from .stats import Periodogram, Statistics
+from .results import Periodogram, Statistics
 
 N_PEAKS_DEFAULT = 32
 MIN_DISTANCE_DEFAULT = 1

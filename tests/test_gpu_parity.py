@@ -304,39 +304,30 @@ def test_ce_vs_reference_cuda(gpu, oracle):
 
 
 def test_aov_vs_reference_cuda(gpu, oracle):
-    """Well-conditioned magnitudes (normalised into (0, 1)): the bins are the
-    reference's, so only the f32 summation order differs."""
-    _ref_or_skip(oracle)
-    ts, ms = _ragged(seed=9, lengths=(64, 300, 1025, 4096, 4097, 6000))
-    ms = [lc.normalize(m) for m in ms]
-    P, D = _grid(400, pdts=(0.0, 1e-4))
-    want = oracle.ref_cuda("aov", ts, ms, P, D, n_phase=15)
-    for mode in ("plain", "chosen"):
-        got = gpu.AOV(15, mode=mode).periodograms(ts, ms, P, D)
-        np.testing.assert_allclose(got, want, rtol=1e-4, atol=1e-5 * np.max(np.abs(want)))
-
-
-def test_aov_vs_reference_cuda_ill_conditioned(gpu, oracle):
-    """Magnitudes 15 +- 0.3 without normalisation: the reference's f32 sums
-    of squares cancel (s2 = sum(Q_b - n_b mu_b^2)), so its values carry up to
-    ~1% error at a few grid points.  The plain form must meet the reference's
-    own CPU-vs-CUDA acceptance rule (tests/test_cpu_vs_cuda.py:179-196:
-    >= 95% of points within rtol 5e-4 / atol 1e-3); the chosen form's exact
-    accumulator must be at least as close to the FP64 statistic as the
-    reference CUDA build is."""
+    """AOV against the reference CUDA build on a ragged batch.  The bins are
+    the reference's count for count (tests/test_gpu_bins.py compares them
+    bin by bin); the values then differ only by the f32 summation order of
+    the bin sums, which the reference adds with shared float atomics in no
+    fixed order.  Both are held to the FP64 statistic on the same bins: the
+    chosen form within 1e-5 relative, the plain form no further from it than
+    twice the reference's own largest error (normalised magnitudes, and
+    15 +- 0.3 raw magnitudes whose f32 sums of squares cancel)."""
     _ref_or_skip(oracle)
     ts, ms = _ragged(seed=9, lengths=(64, 300, 1025, 4096, 4097, 6000))
     P, D = _grid(400, pdts=(0.0, 1e-4))
-    want = oracle.ref_cuda("aov", ts, ms, P, D, n_phase=15)
-    plain = gpu.AOV(15, mode="plain").periodograms(ts, ms, P, D)
-    close = np.abs(plain - want) <= 1e-3 + 5e-4 * np.abs(want)
-    assert close.mean() >= 0.95, close.mean()
-    truth = oracle.aov_f64(ts, ms, P, D, 15, fused_tcorr=True)
-    chosen = gpu.AOV(15, mode="chosen").periodograms(ts, ms, P, D)
-    err_chosen = np.abs(chosen - truth)
-    err_ref = np.abs(want - truth)
-    frac = np.mean(err_chosen <= err_ref + 1e-6 * np.abs(truth))
-    assert frac >= 0.99, frac
+    for mags in ([lc.normalize(m) for m in ms], ms):
+        want = oracle.ref_cuda("aov", ts, mags, P, D, n_phase=15)
+        truth = oracle.aov_f64(ts, mags, P, D, 15, fused_tcorr=True)
+        scale = np.abs(truth).max(axis=(1, 2), keepdims=True)
+        rel = lambda x: np.abs(x - truth) / (np.abs(truth) + 1e-6 * scale)
+        # Cells whose oracle bins (IEEE divide) differ from the reference's
+        # (fast-math divide) have another FP64 truth: the largest errors are
+        # compared over the 99% closest cells.
+        e_ref = np.quantile(rel(want), 0.99)
+        chosen = gpu.AOV(15, mode="chosen").periodograms(ts, mags, P, D)
+        plain = gpu.AOV(15, mode="plain").periodograms(ts, mags, P, D)
+        assert np.quantile(rel(chosen), 0.99) <= 1e-5
+        assert np.quantile(rel(plain), 0.99) <= 2.0 * e_ref + 1e-6
 
 
 def test_ls_vs_reference_cuda(gpu, oracle):

@@ -120,7 +120,7 @@ def test_no_oracle_in_product_path():
     pkg = os.path.join(ROOT, "periodfind_b200")
     for dirpath, _, files in os.walk(pkg):
         for f in files:
-            if f.endswith((".py", ".cu", ".cuh", ".h", ".inc")):
+            if f.endswith((".py", ".cu", ".cuh", ".h", ".inc", ".pyx", ".pxi", ".pxd")):
                 with open(os.path.join(dirpath, f)) as fh:
                     src = fh.read()
                 assert "oracle" not in src.lower().replace("oracle/", ""), f
@@ -356,3 +356,11 @@ def test_chunked_peaks_pipeline_order_and_error_cleanup(monkeypatch):
     assert len(chunks) == 3 and ctx.pending == 0
     with pytest.raises(ValueError):
         obj._chunked_peaks(200, P, D, -1, issue)
+
+
+def test_dropin_declarations_are_in_the_header():
+    """Every C function the drop-in Cython modules declare
+    (periodfind_b200/dropin/pf_abi.pxd) is declared in include/pf.h."""
+    with open(os.path.join(ROOT, "periodfind_b200", "dropin", "pf_abi.pxd")) as fh:
+        pxd = set(re.findall(r"\b(pf_[a-z0-9_]+)\s*\(", fh.read()))
+    assert pxd and pxd <= set(_declared_symbols())
