@@ -64,6 +64,11 @@
  *                  pending on a context; a third is PF_EINVAL.  A caller
  *                  packs the next batch while the GPU runs this one.  Not
  *                  with PF_TIMING.
+ *  PF_TRIG_SINCOS / PF_TRIG_RECURRENCE  (pf_ls_fgrid*, chosen) keep one trig
+ *                  form instead of letting the autotuner pick per length
+ *                  class: MUFU sine / cosine at every (point, frequency), or
+ *                  one sine / cosine per point and thread followed by
+ *                  angle-addition rotations along the uniform grid.
  */
 #ifndef PERIODFIND_B200_PF_H
 #define PERIODFIND_B200_PF_H
@@ -91,6 +96,8 @@ extern "C" {
 #define PF_REF_STATS 0x2000
 #define PF_NO_TUNE 0x4000
 #define PF_ASYNC 0x8000
+#define PF_TRIG_SINCOS 0x10000
+#define PF_TRIG_RECURRENCE 0x20000
 
 typedef struct pf_ctx pf_ctx;
 
@@ -135,6 +142,23 @@ int pf_ls(pf_ctx* ctx, const float* const* times, const float* const* mags,
           const uint64_t* lengths, uint64_t n_curves, const float* periods,
           uint64_t n_per, const float* period_dts, uint64_t n_pdt, int mode,
           float* out);
+
+/* Lomb-Scargle on a uniform frequency grid (no counterpart in the
+ * reference, whose grid is an array of trial periods): trial frequency k is
+ * f_min + k * df exactly, k < n_freq (cycles per time unit), one period
+ * derivative (0); out is [curve][k].  On such a grid the phases of one point
+ * advance by the same angle from one frequency to the next, so besides the
+ * MUFU sine / cosine per evaluation the autotuner can pick, per length
+ * class, an angle-addition recurrence along the grid (PF_TRIG_* forces one).
+ * Chosen form only (PF_MODE_CHOSEN; PF_FOLD_EXACT for an FP64 phase);
+ * CUDA arithmetic only (PF_SEM_CPU is PF_EUNSUPPORTED).  Magnitudes as
+ * pf_ls.  The device-pointer variant takes CSR curves as pf_ls_dev. */
+int pf_ls_fgrid(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                const uint64_t* lengths, uint64_t n_curves, double f_min, double df,
+                uint64_t n_freq, int mode, float* out);
+int pf_ls_fgrid_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
+                    const int64_t* offsets, uint64_t n_curves, double f_min, double df,
+                    uint64_t n_freq, int mode, float* d_out, void* stream);
 
 /* The bins behind a CE or AOV periodogram, for occupancy checks: the
  * counterpart of ConditionalEntropy::FoldAndBin (periodfind/cuda/ce.h:194,

@@ -32,6 +32,8 @@ PF_TIMING = 0x1000
 PF_REF_STATS = 0x2000
 PF_NO_TUNE = 0x4000
 PF_ASYNC = 0x8000
+PF_TRIG_SINCOS = 0x10000
+PF_TRIG_RECURRENCE = 0x20000
 PF_PREP_CENTER, PF_PREP_NORMALIZE = 1, 2
 PF_ALGO_CE, PF_ALGO_AOV, PF_ALGO_LS = 0, 1, 2
 
@@ -51,6 +53,10 @@ SIGNATURES = {
                _vp], _int),
     "pf_aov": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _int, _vp], _int),
     "pf_ls": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _int, _vp], _int),
+    "pf_ls_fgrid": ([_vp, _vp, _vp, _vp, _u64, ctypes.c_double, ctypes.c_double, _u64, _int,
+                     _vp], _int),
+    "pf_ls_fgrid_dev": ([_vp, _vp, _vp, _vp, _u64, ctypes.c_double, ctypes.c_double, _u64,
+                         _int, _vp, _vp], _int),
     "pf_bin_counts": ([_vp, _int, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32,
                        _u32, _int, _vp, _vp], _int),
     "pf_ce_peaks": ([_vp, _vp, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _u32,

@@ -8,4 +8,5 @@
 #include "pf_fold.cuh"
 #include "pf_bin.cuh"
 #include "pf_fpw.cuh"
+#include "pf_lsrec.cuh"
 #include "pf_kern_dispatch.inc"

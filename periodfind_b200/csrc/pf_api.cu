@@ -81,6 +81,7 @@ struct pf_ctx {
     // Autotuner: launch shape per (computation, length class), measured on
     // the device the first time the key is met (see tuned_config).
     struct Tuned {
+        int kind;  // KIND_* of the winner (LS on a frequency grid: the trig form)
         int block;
         bool persist;
         int rounds;
@@ -185,6 +186,10 @@ struct Job {
     float* out_stats = nullptr;
     // pf_bin_counts: raw bin counts per cell ([curve][period][pdt][bins]).
     uint32_t* out_bins = nullptr;
+    // pf_ls_fgrid: trial frequencies f0 + k * df (k < n_per), no periods
+    // array, one period derivative (0).
+    bool fgrid = false;
+    double f0 = 0.0, df = 0.0;
 };
 
 // Bins per cell of a bin-count call: n_phase x n_mag (CE), n_phase (AOV).
@@ -216,8 +221,19 @@ float bin_size(uint32_t n, bool cpu_sem) {
 
 int validate_common(pf_ctx* ctx, const Job& j) {
     if (!ctx) return PF_EINVAL;
+    if (j.fgrid) {
+        if (j.algo != ALGO_LS || !(j.mode & PF_MODE_CHOSEN))
+            return fail(ctx, PF_EUNSUPPORTED, "a frequency grid is for the chosen LS form only");
+        if (j.mode & (PF_FOLD_F32 | PF_SEM_CPU))
+            return fail(ctx, PF_EUNSUPPORTED,
+                        "a frequency grid takes the split-precision or exact fold, CUDA arithmetic");
+        const double last = j.f0 + (double)(j.n_per ? j.n_per - 1 : 0) * j.df;
+        if (!std::isfinite(j.f0) || !std::isfinite(j.df) || !std::isfinite(last))
+            return fail(ctx, PF_EINVAL, "frequency grid f0 = %g, df = %g is not finite", j.f0,
+                        j.df);
+    }
     if (j.n_curves > 0 && (j.n_per == 0 || j.n_pdt == 0)) return PF_OK;  // nothing to compute
-    if (j.n_per > 0 && !j.periods) return fail(ctx, PF_EINVAL, "periods is NULL");
+    if (j.n_per > 0 && !j.periods && !j.fgrid) return fail(ctx, PF_EINVAL, "periods is NULL");
     if (j.n_pdt > 0 && !j.pdts) return fail(ctx, PF_EINVAL, "period_dts is NULL");
     if (j.n_per > 0xFFFFFFFFull || j.n_pdt > 0xFFFFull)
         return fail(ctx, PF_EINVAL, "grid too large (n_per %llu, n_pdt %llu)",
@@ -251,7 +267,7 @@ int validate_common(pf_ctx* ctx, const Job& j) {
 }
 
 int check_grid_host(pf_ctx* ctx, const Job& j) {
-    for (uint64_t i = 0; i < j.n_per; i++) {
+    for (uint64_t i = 0; i < (j.fgrid ? 0 : j.n_per); i++) {
         const float P = j.periods[i];
         if (!std::isfinite(P) || P == 0.0f)
             return fail(ctx, PF_EINVAL, "periods[%llu] = %g must be finite and non-zero",
@@ -490,7 +506,9 @@ const char* class_name(int c) {
     return names[c];
 }
 // Queue counters in the context's misc block: one per class, one for tuning.
+// (Offset 0 holds max |t|; kFgridZeroOffset a zero period derivative.)
 constexpr size_t kCounterOffset = 64;
+constexpr size_t kFgridZeroOffset = 48;
 constexpr int kTuneCounter = kClasses;
 
 // Items of a queue launch over n_curves curves, `per_item` periods each.
@@ -500,11 +518,14 @@ uint64_t queue_items(const Job& j, uint64_t n_curves, int per_item) {
 
 std::string tune_key(const Job& j, const FoldConfig& c, int cls) {
     char b[160];
-    snprintf(b, sizeof(b), "%s %s%s%s ph=%u mag=%u pdt=%s sem=%s class=%s",
+    snprintf(b, sizeof(b), "%s %s%s%s%s ph=%u mag=%u pdt=%s sem=%s class=%s",
              c.algo == ALGO_CE ? "ce" : c.algo == ALGO_AOV ? "aov" : "ls",
              c.kind == KIND_BIN ? "bin" : (c.fold == FOLD_DF ? "fold-split" : "fold-exact"),
-             c.cnt16 ? "-cnt16" : "", c.ref_stats ? "-refstats" : "", j.n_phase,
-             c.algo == ALGO_CE ? j.n_mag : 0u, j.n_pdt > 1 ? "many" : "one",
+             c.cnt16 ? "-cnt16" : "", c.ref_stats ? "-refstats" : "",
+             j.fgrid ? ((j.mode & PF_TRIG_SINCOS) ? "-fgrid-sincos"
+                        : (j.mode & PF_TRIG_RECURRENCE) ? "-fgrid-recurrence" : "-fgrid")
+                     : "",
+             j.n_phase, c.algo == ALGO_CE ? j.n_mag : 0u, j.n_pdt > 1 ? "many" : "one",
              use_cpu_semantics(j.mode) ? "cpu" : "cuda", class_name(cls));
     return b;
 }
@@ -527,9 +548,22 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
                  uint64_t nc, uint64_t cls_points, const FoldParams& p, cudaStream_t s,
                  FoldConfig& out) {
     out = base;
+    // LS on a uniform frequency grid: the trig form is a candidate axis too
+    // (MUFU sin / cos per evaluation, or the recurrence along the grid with
+    // 4 or 8 frequencies per thread); PF_TRIG_* keeps one form.
+    const bool rec_ok = j.fgrid && base.algo == ALGO_LS && base.fold == FOLD_DF;
+    const bool only_rec = rec_ok && (j.mode & PF_TRIG_RECURRENCE);
+    const bool no_rec = !rec_ok || (j.mode & PF_TRIG_SINCOS);
+    if (only_rec) {
+        out.kind = KIND_LSREC;
+        out.block = 256;
+        out.rounds = 8;
+        out.persist = false;
+    }
     const std::string key = tune_key(j, base, cls);
     auto it = ctx->tuned.find(key);
     if (it != ctx->tuned.end()) {
+        out.kind = it->second.kind;
         out.block = it->second.block;
         out.persist = it->second.persist;
         out.rounds = it->second.rounds;
@@ -546,49 +580,71 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
     const uint64_t s0 = c0 + (nc - k) / 2;
     FoldParams ps = p;
     ps.stamps = nullptr;
+    ps.bins = nullptr;
     ps.q.order = p.q.order + s0;
     ps.q.next = reinterpret_cast<unsigned*>((char*)ctx->d_misc.p + kCounterOffset) + kTuneCounter;
-    pf_ctx::Tuned best{base.block, base.persist, base.rounds, 1e30f, 0.0f, 0};
-    // The reference statistic is built in one shape; the bin kernel's
-    // chosen statistic also in 4 rounds per item.
+    pf_ctx::Tuned best{out.kind, out.block, out.persist, out.rounds, 1e30f, 0.0f, 0};
+    // Candidates: block x persistent-or-not, and for the bin kernel 1 or 4
+    // rounds of periods per item; for the recurrence 4 or 8 frequencies per
+    // thread.  The reference statistic is built in one shape only.
+    std::vector<FoldConfig> cands;
     const bool shapes = !(base.kind == KIND_BIN && base.ref_stats);
-    for (int block : {64, 128, 256}) {
-        FoldConfig t = base;
-        t.block = block;
-        if (fold_smem(t, j.n_phase, j.n_mag) > ctx->smem_optin) continue;
-        for (int shape = 0; shape < (shapes ? 4 : 1); shape++) {
-            t.persist = (shape & 1) != 0;
-            t.rounds = (base.kind == KIND_BIN && (shape & 2)) ? 4 : 1;
-            if (base.kind != KIND_BIN && (shape & 2)) continue;
-            const uint64_t nw = queue_items(j, k, item_periods(t));
-            if (nw == 0 || nw > 0x7FFFFFFFull) continue;
-            ps.q.n_work = (uint32_t)nw;
-            // The first launch warms up; the faster of the next two counts
-            // (shapes within a few percent of each other otherwise swap
-            // places by launch-to-launch noise on a ~1 ms sample).
-            float ms = 1e30f;
-            for (int rep = 0; rep < 3; rep++) {
-                float m = 0.0f;
-                PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
-                PF_CUDA(launch_fold_sem(j, t, ps, (uint32_t)nw, s), "tuning launch");
-                PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
-                PF_CUDA(cudaEventSynchronize(ctx->ev1), "tuning sync");
-                PF_CUDA(cudaEventElapsedTime(&m, ctx->ev0, ctx->ev1), "event time");
-                if (rep > 0) ms = std::min(ms, m);
+    if (!only_rec) {
+        for (int block : {64, 128, 256}) {
+            FoldConfig t = base;
+            t.block = block;
+            if (fold_smem(t, j.n_phase, j.n_mag) > ctx->smem_optin) continue;
+            for (int shape = 0; shape < (shapes ? 4 : 1); shape++) {
+                t.persist = (shape & 1) != 0;
+                t.rounds = (base.kind == KIND_BIN && (shape & 2)) ? 4 : 1;
+                if (base.kind != KIND_BIN && (shape & 2)) continue;
+                cands.push_back(t);
             }
-            ctx->launches += 3;
-            best.candidates++;
-            best.ms_worst = std::max(best.ms_worst, ms);
-            if (ms < best.ms) {
-                best.ms = ms;
-                best.block = block;
-                best.persist = t.persist;
-                best.rounds = t.rounds;
-            }
+        }
+    }
+    if (!no_rec) {
+        for (int block : {128, 256})
+            for (int r : {4, 8})
+                for (int persist = 0; persist < 2; persist++) {
+                    FoldConfig t = base;
+                    t.kind = KIND_LSREC;
+                    t.block = block;
+                    t.rounds = r;
+                    t.persist = persist != 0;
+                    cands.push_back(t);
+                }
+    }
+    for (const FoldConfig& t : cands) {
+        const uint64_t nw = queue_items(j, k, item_periods(t));
+        if (nw == 0 || nw > 0x7FFFFFFFull) continue;
+        ps.q.n_work = (uint32_t)nw;
+        // The first launch warms up; the faster of the next two counts
+        // (shapes within a few percent of each other otherwise swap places
+        // by launch-to-launch noise on a ~1 ms sample).
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3; rep++) {
+            float m = 0.0f;
+            PF_CUDA(cudaEventRecord(ctx->ev0, s), "event");
+            PF_CUDA(launch_fold_sem(j, t, ps, (uint32_t)nw, s), "tuning launch");
+            PF_CUDA(cudaEventRecord(ctx->ev1, s), "event");
+            PF_CUDA(cudaEventSynchronize(ctx->ev1), "tuning sync");
+            PF_CUDA(cudaEventElapsedTime(&m, ctx->ev0, ctx->ev1), "event time");
+            if (rep > 0) ms = std::min(ms, m);
+        }
+        ctx->launches += 3;
+        best.candidates++;
+        best.ms_worst = std::max(best.ms_worst, ms);
+        if (ms < best.ms) {
+            best.ms = ms;
+            best.kind = t.kind;
+            best.block = t.block;
+            best.persist = t.persist;
+            best.rounds = t.rounds;
         }
     }
     if (best.candidates == 0) return PF_OK;
     ctx->tuned[key] = best;
+    out.kind = best.kind;
     out.block = best.block;
     out.persist = best.persist;
     out.rounds = best.rounds;
@@ -671,6 +727,9 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
     p.mag_bin_size = bin_size(j.n_mag, cpu);
     p.out = d_out;
     p.edge_d = edge_guard(j.n_phase);
+    p.fgrid = j.fgrid ? 1 : 0;
+    p.f0 = j.f0;
+    p.df = j.df;
     const uint32_t ncur = (uint32_t)j.n_curves;
     int rc;
     if ((rc = ensure_dev(ctx, ctx->d_misc, 256)) != PF_OK) return rc;
@@ -860,7 +919,7 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
             if (b) return fail(ctx, PF_EINVAL, "times must be finite");
     }
     fill_meta(ctx, j, L, cfg, hb);
-    memcpy(hb + L.o_periods, j.periods, j.n_per * 4);
+    if (!j.fgrid) memcpy(hb + L.o_periods, j.periods, j.n_per * 4);
     memcpy(hb + L.o_pdts, j.pdts, j.n_pdt * 4);
 
     cudaStream_t s = ctx->stream;
@@ -970,6 +1029,13 @@ int run_dev(pf_ctx* ctx, const Job& j, const float* d_times, const float* d_mags
     p.work = (const WorkItem*)(db + L.o_work);
     p.periods = j.periods;
     p.pdts = j.pdts;
+    if (j.fgrid) {
+        // The one period derivative (0) of a frequency grid, on the device.
+        if ((rc = ensure_dev(ctx, ctx->d_misc, 256)) != PF_OK) return rc;
+        float* zero = (float*)((char*)ctx->d_misc.p + kFgridZeroOffset);
+        PF_CUDA(cudaMemsetAsync(zero, 0, sizeof(float), s), "memset");
+        p.pdts = zero;
+    }
     rc = device_pipeline(ctx, j, L, cfg, p, dcurves, j.out, s);
     if (rc != PF_OK) return rc;
     PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
@@ -1258,6 +1324,7 @@ void for_each_curve(uint64_t n_curves, uint64_t total_points, F& fn) {
 }  // namespace
 
 size_t pfk::fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag) {
+    if (c.kind == KIND_LSREC) return kRecTileBytes;
     if (c.kind == KIND_BIN) return bin_smem_bytes(c.algo, c.cnt16, c.block, n_phase, n_mag);
     return fold_smem_bytes(c.algo, c.fold, c.acc, c.block, c.ovl, n_phase, n_mag);
 }
@@ -1434,8 +1501,13 @@ int pf_tuning_report(const pf_ctx* ctx, char* buf, uint64_t len) {
     for (const auto& kv : ctx->tuned) {
         char line[320];
         snprintf(line, sizeof(line),
-                 "%s: block=%d rounds=%d %s sample_ms=%.3f slowest_ms=%.3f candidates=%u\n",
-                 kv.first.c_str(), kv.second.block, kv.second.rounds,
+                 "%s: %sblock=%d rounds=%d %s sample_ms=%.3f slowest_ms=%.3f candidates=%u\n",
+                 kv.first.c_str(),
+                 kv.second.kind == KIND_LSREC ? "trig=recurrence "
+                 : (kv.second.kind == KIND_FOLD && kv.first.find("fgrid") != std::string::npos)
+                     ? "trig=sincos "
+                     : "",
+                 kv.second.block, kv.second.rounds,
                  kv.second.persist ? "persistent" : "one-cta-per-item", kv.second.ms,
                  kv.second.ms_worst, kv.second.candidates);
         out += line;
@@ -1638,6 +1710,40 @@ int pf_aov(pf_ctx* ctx, const float* const* times, const float* const* mags,
     j.po = phase_overlap;
     j.out = out;
     return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_ls_fgrid(pf_ctx* ctx, const float* const* times, const float* const* mags,
+                const uint64_t* lengths, uint64_t n_curves, double f_min, double df,
+                uint64_t n_freq, int mode, float* out) {
+    static const float kZeroPdt = 0.0f;
+    Job j;
+    j.algo = ALGO_LS;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.n_per = n_freq;
+    j.pdts = &kZeroPdt;
+    j.n_pdt = 1;
+    j.fgrid = true;
+    j.f0 = f_min;
+    j.df = df;
+    j.out = out;
+    return run_host(ctx, j, times, mags, lengths);
+}
+
+int pf_ls_fgrid_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
+                    const int64_t* offsets, uint64_t n_curves, double f_min, double df,
+                    uint64_t n_freq, int mode, float* d_out, void* stream) {
+    Job j;
+    j.algo = ALGO_LS;
+    j.mode = mode;
+    j.n_curves = n_curves;
+    j.n_per = n_freq;
+    j.n_pdt = 1;
+    j.fgrid = true;
+    j.f0 = f_min;
+    j.df = df;
+    j.out = d_out;
+    return run_dev(ctx, j, d_times, d_mags, offsets, stream);
 }
 
 int pf_bin_counts(pf_ctx* ctx, int algo, const float* const* times, const float* const* mags,

@@ -78,6 +78,21 @@ __device__ __forceinline__ void cell_setup(Cell& s, float period, float period_d
     }
 }
 
+// A trial frequency f (FP64, exact) instead of a period: 1/P is f itself, so
+// the exact fold's double-double reciprocal is (f, 0) and the split-precision
+// fold's float pair is f rounded plus its remainder.  No period derivative.
+__device__ __forceinline__ void cell_setup_freq(Cell& s, double f) {
+    s.period = (float)(1.0 / f);
+    s.pdt_corr = 0.0f;
+    s.Pd = 1.0 / f;
+    s.yhi = f;
+    s.ylo = 0.0;
+    s.c = 0.0;
+    s.fhi = __double2float_rn(f);
+    s.flo = __double2float_rn(__dadd_rn(f, -(double)s.fhi));
+    s.ghi = s.glo = 0.0f;
+}
+
 // The reference fold, operation for operation (periodfind/cuda/ce.cu:140-143,
 // aov.cu:106-109, ls.cu:95-97; rust/src/fold.rs:22-26).
 __device__ __forceinline__ float fold_ref(float t, const Cell& s) {
@@ -166,7 +181,10 @@ __device__ double cta_qbound_of(const FoldParams& p, double my_min_abs_p, float 
 
 template <int BLOCK>
 __device__ double cta_qbound(const FoldParams& p, uint32_t pi, float period_dt) {
-    return cta_qbound_of<BLOCK>(p, fabs((double)p.periods[pi]), period_dt);
+    // On a frequency grid 1 / |f| stands for |P| (f = 0 gives an infinite
+    // bound, so the exact fold, whose phase is then 0).
+    const double absp = p.fgrid ? 1.0 / fabs(p.f0 + (double)pi * p.df) : fabs((double)p.periods[pi]);
+    return cta_qbound_of<BLOCK>(p, absp, period_dt);
 }
 
 // Optional per-work-item timing (%globaltimer, ns): the CTA's first thread
@@ -250,6 +268,31 @@ struct Views {
 struct LSAcc {
     float mag_cos, mag_sin, cos_cos, cos_sin;
 };
+
+// The LS power from a cell's sums (periodfind/cuda/ls.cu:144-165 /
+// rust/src/ls.rs:253-280), n points.
+__device__ __forceinline__ float ls_power(const LSAcc& ls, uint32_t n) {
+    const float mag_cos = ls.mag_cos, mag_sin = ls.mag_sin;
+    const float cos_cos = ls.cos_cos, cos_sin = ls.cos_sin;
+    float sin_sin = static_cast<float>(n) - cos_cos;
+    float cos_tau, sin_tau;
+    sincosf(0.5f * atan2f(2.0f * cos_sin, cos_cos - sin_sin), &sin_tau, &cos_tau);
+    float numerator_l = cos_tau * mag_cos + sin_tau * mag_sin;
+    numerator_l *= numerator_l;
+    float numerator_r = cos_tau * mag_sin - sin_tau * mag_cos;
+    numerator_r *= numerator_r;
+    float denominator_l = cos_tau * cos_tau * cos_cos + 2 * cos_tau * sin_tau * cos_sin +
+                          sin_tau * sin_tau * sin_sin;
+    float denominator_r = cos_tau * cos_tau * sin_sin - 2 * cos_tau * sin_tau * cos_sin +
+                          sin_tau * sin_tau * cos_cos;
+#if PF_SEM_CPU_TU
+    return (denominator_l == 0.0f || denominator_r == 0.0f)
+               ? 0.0f
+               : 0.5f * (numerator_l / denominator_l + numerator_r / denominator_r);
+#else
+    return 0.5f * ((numerator_l / denominator_l) + (numerator_r / denominator_r));
+#endif
+}
 
 // Stream the curve through shared memory and accumulate this thread's cell.
 template <int ALGO, int FOLD, int ACC, int BLOCK, bool OVL, bool HAS_PDT, bool ALT>
@@ -434,7 +477,8 @@ __device__ __forceinline__ void fold_item(const FoldParams& p, const WorkItem w,
     const float period_dt = p.pdts[w.pdt];
 
     Cell s;
-    cell_setup<FOLD>(s, p.periods[pi], period_dt);
+    if (ALGO == ALGO_LS && p.fgrid) cell_setup_freq(s, p.f0 + (double)pi * p.df);
+    else cell_setup<FOLD>(s, p.periods[pi], period_dt);
 
     // Zero this thread's column of the private histogram.
     if constexpr (ALGO == ALGO_CE) {
@@ -570,27 +614,7 @@ __device__ __forceinline__ void fold_item(const FoldParams& p, const WorkItem w,
 #endif
         }
     } else {
-        // periodfind/cuda/ls.cu:144-165 / rust/src/ls.rs:253-280.
-        const float mag_cos = ls.mag_cos, mag_sin = ls.mag_sin;
-        const float cos_cos = ls.cos_cos, cos_sin = ls.cos_sin;
-        float sin_sin = static_cast<float>(n) - cos_cos;
-        float cos_tau, sin_tau;
-        sincosf(0.5f * atan2f(2.0f * cos_sin, cos_cos - sin_sin), &sin_tau, &cos_tau);
-        float numerator_l = cos_tau * mag_cos + sin_tau * mag_sin;
-        numerator_l *= numerator_l;
-        float numerator_r = cos_tau * mag_sin - sin_tau * mag_cos;
-        numerator_r *= numerator_r;
-        float denominator_l = cos_tau * cos_tau * cos_cos + 2 * cos_tau * sin_tau * cos_sin +
-                              sin_tau * sin_tau * sin_sin;
-        float denominator_r = cos_tau * cos_tau * sin_sin - 2 * cos_tau * sin_tau * cos_sin +
-                              sin_tau * sin_tau * cos_cos;
-#if PF_SEM_CPU_TU
-        p.out[out_idx] = (denominator_l == 0.0f || denominator_r == 0.0f)
-                             ? 0.0f
-                             : 0.5f * (numerator_l / denominator_l + numerator_r / denominator_r);
-#else
-        p.out[out_idx] = 0.5f * ((numerator_l / denominator_l) + (numerator_r / denominator_r));
-#endif
+        p.out[out_idx] = ls_power(ls, n);
     }
     stamp_end(p, item);
 }

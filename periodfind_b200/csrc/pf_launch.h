@@ -8,7 +8,11 @@
 
 namespace pfk {
 
-enum : int { KIND_FOLD = 0, KIND_BIN = 1 };
+// KIND_LSREC: Lomb-Scargle on a uniform frequency grid with the
+// angle-addition recurrence along the grid (pf_lsrec.cuh); `rounds` holds
+// its frequencies per thread.
+enum : int { KIND_FOLD = 0, KIND_BIN = 1, KIND_LSREC = 2 };
+constexpr uint32_t kRecTileBytes = 512 * 16;  // lsrec_kernel's staged points
 
 // Kernels that take their items from the device work queue (a curve order;
 // the device derives the items): the chosen bin kernel and the chosen folds.
@@ -16,7 +20,7 @@ enum : int { KIND_FOLD = 0, KIND_BIN = 1 };
 // counter) or statically (one CTA per item).  The reference fold and the
 // all-FP32 study fold take one CTA per item of a host-built list.
 __host__ __device__ constexpr bool uses_queue(int kind, int fold) {
-    return kind == KIND_BIN || fold == FOLD_EXACT || fold == FOLD_DF;
+    return kind == KIND_BIN || kind == KIND_LSREC || fold == FOLD_EXACT || fold == FOLD_DF;
 }
 
 struct FoldConfig {
@@ -29,7 +33,8 @@ struct FoldConfig {
     bool ovl;   // general bin-overlap path
     bool ref_stats; // bin_kernel: the reference's statistic operation sequence
     bool persist;   // queue kernels: persistent grid instead of one CTA per item
-    int rounds;     // bin kernel: an item is rounds x block periods (1 or 4)
+    int rounds;     // bin kernel: an item is rounds x block periods (1 or 4);
+                    // KIND_LSREC: frequencies per thread (4 or 8)
     int n_sm;       // persistent kernels: grid = n_sm x resident CTAs per SM
 };
 
@@ -37,7 +42,7 @@ size_t fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag);
 
 // Periods in one work item of a queue kernel.
 inline int item_periods(const FoldConfig& c) {
-    return c.block * (c.kind == KIND_BIN && c.rounds > 1 ? c.rounds : 1);
+    return c.block * ((c.kind == KIND_BIN || c.kind == KIND_LSREC) && c.rounds > 1 ? c.rounds : 1);
 }
 
 // Semantics of the reference's CUDA build (-use_fast_math).

@@ -80,6 +80,11 @@ struct FoldParams {
     // [n_pdt][bins] with bins = n_phase * n_mag (CE) or n_phase (AOV).
     // Written by the plain kernels and the chosen reference-statistic form.
     uint32_t* bins;
+    // LS on a uniform frequency grid (fgrid != 0): trial frequency k is
+    // f0 + k * df exactly (FP64), in place of 1 / periods[k]; one period
+    // derivative, 0.
+    int fgrid;
+    double f0, df;
 };
 
 // Shared-memory bytes of the chosen bin kernel (pf_bin.cuh).

@@ -474,6 +474,39 @@ class LombScargle(_Periodogram):
                                    nat.ptr(pdts), len(pdts), n_peaks, min_distance,
                                    self._flags | extra, nat.ptr(idx), nat.ptr(val))
 
+    def periodograms_frequency_grid(self, times, mags, f_min, df, n_freq, trig=None,
+                                    center=None):
+        """LS power at the trial frequencies f_min + k * df (cycles per time
+        unit), k < n_freq, as float32 [n_curves, n_freq]; magnitudes centred
+        as calc() centres them.  No counterpart in the reference, whose grid
+        is an array of trial periods (pf_ls_fgrid).
+
+        On a uniform frequency grid the phase of a point advances by the same
+        angle from one frequency to the next, so the sine and cosine can
+        follow the grid by angle-addition rotations instead of one MUFU pair
+        per evaluation.  trig: None lets the autotuner pick per curve-length
+        class; 'sincos' or 'recurrence' keeps one form.  Chosen form and
+        CUDA arithmetic only (fold='exact' for an FP64 phase)."""
+        if self.mode != "chosen" or self.semantics != "cuda":
+            raise ValueError("a frequency grid needs mode='chosen', semantics='cuda'")
+        if trig not in (None, "sincos", "recurrence"):
+            raise ValueError(f"trig must be None, 'sincos' or 'recurrence', got {trig!r}")
+        if center is None:
+            center = self._center_default
+        validate_inputs(times, mags)
+        ensure_float32(times, "times")
+        ensure_float32(mags, "mags")
+        mags_use = prepare_magnitudes(mags, center, False)
+        flags = self._flags | {None: 0, "sincos": nat.PF_TRIG_SINCOS,
+                               "recurrence": nat.PF_TRIG_RECURRENCE}[trig]
+        ctx = nat.default_context(self.device)
+        b = nat.CurveBatch(times, mags_use)
+        out = np.empty((b.n, int(n_freq)), dtype=np.float32)
+        with ctx.lock:
+            ctx.check(ctx.lib.pf_ls_fgrid(ctx.handle, *b.args(), float(f_min), float(df),
+                                          int(n_freq), flags, nat.ptr(out)))
+        return out
+
     def refine_peaks(self, times, mags, periods, peak_indices, n_steps=5, center=None):
         """Refine grid peaks off the trial grid by Newton steps on dP/domega
         (no counterpart in the reference, whose peaks are grid points).
