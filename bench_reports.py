@@ -407,6 +407,24 @@ def precision_arm(args):
         with clocks.region(name):
             ms_ = _event_ms(torch, run, max(1, args.steps), flush)
         out["folds"][name] = {"ms": ms_, "evals_per_s": ev / (ms_ * 1e-3)}
+    # The same grid given as a uniform frequency grid (pf_ls_fgrid_dev):
+    # trial frequency k is exactly 0.01 + k * df.  Sincos per evaluation,
+    # the angle-addition recurrence along the grid, and the autotuner's pick
+    # per length class.
+    f_min, df = 0.01, (20.0 - 0.01) / (n_freq - 1)
+    for name, flags in (("frequency grid, sincos", nat.PF_MODE_CHOSEN | nat.PF_TRIG_SINCOS),
+                        ("frequency grid, recurrence",
+                         nat.PF_MODE_CHOSEN | nat.PF_TRIG_RECURRENCE),
+                        ("frequency grid, tuned trig", nat.PF_MODE_CHOSEN)):
+        def run(flags=flags):
+            ctx.check(ctx.lib.pf_ls_fgrid_dev(ctx.handle, d_t.data_ptr(), d_m.data_ptr(),
+                                              off.ctypes.data, n_curves, f_min, df, n_freq,
+                                              flags, pg.data_ptr(), s))
+        run()
+        with clocks.region(name):
+            ms_ = _event_ms(torch, run, max(1, args.steps), flush)
+        out["folds"][name] = {"ms": ms_, "evals_per_s": ev / (ms_ * 1e-3)}
+    out["tuning"] = [ln for ln in ctx.tuning_report().splitlines() if "fgrid" in ln]
     _emit(out, clocks)
 
 

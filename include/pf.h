@@ -69,6 +69,12 @@
  *                  class: MUFU sine / cosine at every (point, frequency), or
  *                  one sine / cosine per point and thread followed by
  *                  angle-addition rotations along the uniform grid.
+ *  PF_BINS_SHARED  (CE / AOV, chosen) keep the shared-histogram binning
+ *                  (one histogram per warp and trial period, filled with
+ *                  shared atomics) for the length classes it serves (curves
+ *                  shorter than 1024 points) instead of letting the
+ *                  autotuner weigh it against per-thread privatised
+ *                  histograms.  Values are identical either way.
  */
 #ifndef PERIODFIND_B200_PF_H
 #define PERIODFIND_B200_PF_H
@@ -98,6 +104,7 @@ extern "C" {
 #define PF_ASYNC 0x8000
 #define PF_TRIG_SINCOS 0x10000
 #define PF_TRIG_RECURRENCE 0x20000
+#define PF_BINS_SHARED 0x40000
 
 typedef struct pf_ctx pf_ctx;
 

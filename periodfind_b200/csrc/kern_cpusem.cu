@@ -9,4 +9,5 @@
 #include "pf_bin.cuh"
 #include "pf_fpw.cuh"
 #include "pf_lsrec.cuh"
+#include "pf_binwarp.cuh"
 #include "pf_kern_dispatch.inc"

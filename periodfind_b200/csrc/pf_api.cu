@@ -509,6 +509,9 @@ const char* class_name(int c) {
 // (Offset 0 holds max |t|; kFgridZeroOffset a zero period derivative.)
 constexpr size_t kCounterOffset = 64;
 constexpr size_t kFgridZeroOffset = 48;
+// Length classes whose curves fit the shared-histogram kernel's staging
+// (kWarpMaxPoints = 1024 points): [0,64), [64,256), [256,1024).
+constexpr int kWarpClassMax = 2;
 constexpr int kTuneCounter = kClasses;
 
 // Items of a queue launch over n_curves curves, `per_item` periods each.
@@ -524,7 +527,7 @@ std::string tune_key(const Job& j, const FoldConfig& c, int cls) {
              c.cnt16 ? "-cnt16" : "", c.ref_stats ? "-refstats" : "",
              j.fgrid ? ((j.mode & PF_TRIG_SINCOS) ? "-fgrid-sincos"
                         : (j.mode & PF_TRIG_RECURRENCE) ? "-fgrid-recurrence" : "-fgrid")
-                     : "",
+                     : (j.mode & PF_BINS_SHARED) ? "-shared-bins" : "",
              j.n_phase, c.algo == ALGO_CE ? j.n_mag : 0u, j.n_pdt > 1 ? "many" : "one",
              use_cpu_semantics(j.mode) ? "cpu" : "cuda", class_name(cls));
     return b;
@@ -554,10 +557,21 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
     const bool rec_ok = j.fgrid && base.algo == ALGO_LS && base.fold == FOLD_DF;
     const bool only_rec = rec_ok && (j.mode & PF_TRIG_RECURRENCE);
     const bool no_rec = !rec_ok || (j.mode & PF_TRIG_SINCOS);
+    // Likewise the binning strategy of the chosen CE / AOV kernels:
+    // per-thread privatised histograms, or shared histograms with atomics
+    // (PF_BINS_SHARED keeps the latter where the curves fit it).
+    const bool warp_ok = base.kind == KIND_BIN && !base.ref_stats && cls <= kWarpClassMax;
+    const bool only_warp = warp_ok && (j.mode & PF_BINS_SHARED);
     if (only_rec) {
         out.kind = KIND_LSREC;
         out.block = 256;
         out.rounds = 8;
+        out.persist = false;
+    }
+    if (only_warp) {
+        out.kind = KIND_BINWARP;
+        out.block = 256;
+        out.rounds = 1;
         out.persist = false;
     }
     const std::string key = tune_key(j, base, cls);
@@ -589,7 +603,7 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
     // thread.  The reference statistic is built in one shape only.
     std::vector<FoldConfig> cands;
     const bool shapes = !(base.kind == KIND_BIN && base.ref_stats);
-    if (!only_rec) {
+    if (!only_rec && !only_warp) {
         for (int block : {64, 128, 256}) {
             FoldConfig t = base;
             t.block = block;
@@ -601,6 +615,19 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
                 cands.push_back(t);
             }
         }
+    }
+    // The shared-histogram binning (one histogram per warp and period,
+    // shared atomics) for classes of curves shorter than its staging limit.
+    if (warp_ok) {
+        for (int block : {128, 256})
+            for (int persist = 0; persist < 2; persist++) {
+                FoldConfig t = base;
+                t.kind = KIND_BINWARP;
+                t.block = block;
+                t.rounds = 1;
+                t.persist = persist != 0;
+                if (fold_smem(t, j.n_phase, j.n_mag) <= ctx->smem_optin) cands.push_back(t);
+            }
     }
     if (!no_rec) {
         for (int block : {128, 256})
@@ -1325,6 +1352,9 @@ void for_each_curve(uint64_t n_curves, uint64_t total_points, F& fn) {
 
 size_t pfk::fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag) {
     if (c.kind == KIND_LSREC) return kRecTileBytes;
+    if (c.kind == KIND_BINWARP)
+        return (size_t)kWarpMaxPoints * 16 +
+               (size_t)(c.block / 32) * (c.algo == ALGO_CE ? n_phase * n_mag : 2 * n_phase) * 4;
     if (c.kind == KIND_BIN) return bin_smem_bytes(c.algo, c.cnt16, c.block, n_phase, n_mag);
     return fold_smem_bytes(c.algo, c.fold, c.acc, c.block, c.ovl, n_phase, n_mag);
 }
@@ -1504,6 +1534,8 @@ int pf_tuning_report(const pf_ctx* ctx, char* buf, uint64_t len) {
                  "%s: %sblock=%d rounds=%d %s sample_ms=%.3f slowest_ms=%.3f candidates=%u\n",
                  kv.first.c_str(),
                  kv.second.kind == KIND_LSREC ? "trig=recurrence "
+                 : kv.second.kind == KIND_BINWARP ? "bins=shared-atomic "
+                 : kv.second.kind == KIND_BIN ? "bins=privatised "
                  : (kv.second.kind == KIND_FOLD && kv.first.find("fgrid") != std::string::npos)
                      ? "trig=sincos "
                      : "",

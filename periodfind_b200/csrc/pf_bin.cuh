@@ -63,23 +63,44 @@ struct BinPoint {
     uint32_t a, b;
 };
 
+// c log2 c of a count (zero for c = 0 and 1): one log per bin, no divide,
+// ln 2 applied once at the end.  A count (< 2^16 here: the bin kernels run
+// curves of fewer than 65536 points) becomes a float exactly by placing it
+// in the mantissa of 2^23, which costs a bitwise OR and an add instead of an
+// integer-to-float conversion.  Explicit roundings, so that every kernel
+// that sums these terms in the same order gets the same bits.
+__device__ __forceinline__ float ce_xlx(uint32_t c) {
+    const float f = __fsub_rn(__uint_as_float(c | 0x4B000000u), 8388608.0f);
+    return __fmul_rn(f, log2f(fmaxf(f, 1.0f)));
+}
+
+// CE of one cell from its running sum of row terms, over n points.
+__device__ __forceinline__ float ce_finish(float acc, uint32_t n) {
+    return __fmul_rn(acc, 0.69314718055994531f / (float)n);
+}
+
+// AOV of one cell from sum_b X_b^2 / c_b (fixed-point bin sums X_b).
+__device__ __forceinline__ float aov_finish(double sbx, const CurveDesc& cd, uint32_t n,
+                                            uint32_t nP) {
+    const double s1 = fmax(sbx - cd.fix_sumx * cd.fix_sumx / (double)n, 0.0);
+    const double s2 = __dadd_rn(cd.fix_sumx2, -sbx);
+    const double scale = ((double)n - (double)nP) / ((double)nP - 1.0);
+#if PF_SEM_CPU_TU
+    return (s2 <= 0.0) ? 0.0f : (float)(scale * (s1 / s2));
+#else
+    return (float)(scale * (s1 / (s2 <= 0.0 ? 0.0 : s2)));
+#endif
+}
+
 // The chosen form's CE statistic.  Counters are read through 32-bit shared
 // addresses (tbase = this thread's column).  Each row term
 // C_j ln C_j - sum_i c_ij ln c_ij is non-negative, so FP32 accumulation keeps
 // the relative error near 1e-7 (FP64 here costs registers in the binning
-// loop, measured slower).
+// loop, measured slower).  Per row, the magnitude bins are taken in pairs
+// (the two 16-bit halves of a word).
 template <bool CNT16>
 __device__ __forceinline__ float ce_stat_fast(uint32_t tbase, uint32_t nP, uint32_t W,
                                               uint32_t block, uint32_t n) {
-    // c log2 c, zero for c = 0 and 1: one log per bin, no divide, and ln 2
-    // applied once at the end.  A count (< 2^16 here: the bin kernel runs
-    // curves of fewer than 65536 points) becomes a float exactly by placing
-    // it in the mantissa of 2^23, which costs a bitwise OR and an add
-    // instead of an integer-to-float conversion.
-    auto xlx = [](uint32_t c) -> float {
-        const float f = __uint_as_float(c | 0x4B000000u) - 8388608.0f;
-        return f * log2f(fmaxf(f, 1.0f));
-    };
     float acc = 0.0f;
     for (uint32_t j = 0; j < nP; j++) {
         uint32_t col = 0;
@@ -90,16 +111,16 @@ __device__ __forceinline__ float ce_stat_fast(uint32_t tbase, uint32_t nP, uint3
                 // Both 16-bit halves summed at once: each half's column
                 // total is at most n < 2^16, so no carry crosses halves.
                 col += wv;
-                row += xlx(wv & 0xFFFFu) + xlx(wv >> 16);
+                row = __fadd_rn(row, __fadd_rn(ce_xlx(wv & 0xFFFFu), ce_xlx(wv >> 16)));
             } else {
                 col += wv;
-                row += xlx(wv);
+                row = __fadd_rn(row, ce_xlx(wv));
             }
         }
         if constexpr (CNT16) col = (col & 0xFFFFu) + (col >> 16);
-        acc += xlx(col) - row;
+        acc = __fadd_rn(acc, __fsub_rn(ce_xlx(col), row));
     }
-    return acc * (0.69314718055994531f / (float)n);
+    return ce_finish(acc, n);
 }
 
 // The chosen form's AOV sum_b X_b^2 / c_b over the fixed-point bin sums X_b
@@ -110,7 +131,7 @@ __device__ __forceinline__ double aov_sbx_fast(uint32_t tbase, uint32_t nP, uint
     for (uint32_t b = 0; b < nP; b++) {
         const uint32_t c = lds_u32(tbase + b * block * 4u);
         const double Xd = (double)lds_u32(tbase + sum_off + b * block * 4u);
-        sbx = __fma_rn(Xd * Xd, __drcp_rn((double)max(c, 1u)), sbx);
+        sbx = __fma_rn(__dmul_rn(Xd, Xd), __drcp_rn((double)max(c, 1u)), sbx);
     }
     return sbx;
 }
@@ -345,15 +366,7 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
     if constexpr (ALGO == ALGO_CE && !REF_STATS) {
         p.out[out_idx] = ce_stat_fast<CNT16>(tbase, nP, W, BLOCK, n);
     } else if constexpr (ALGO == ALGO_AOV && !REF_STATS) {
-        const double sbx = aov_sbx_fast(tbase, nP, BLOCK);
-        const double s1 = fmax(sbx - cd.fix_sumx * cd.fix_sumx / (double)n, 0.0);
-        const double s2 = __dadd_rn(cd.fix_sumx2, -sbx);
-        const double scale = ((double)n - (double)nP) / ((double)nP - 1.0);
-#if PF_SEM_CPU_TU
-        p.out[out_idx] = (s2 <= 0.0) ? 0.0f : (float)(scale * (s1 / s2));
-#else
-        p.out[out_idx] = (float)(scale * (s1 / (s2 <= 0.0 ? 0.0 : s2)));
-#endif
+        p.out[out_idx] = aov_finish(aov_sbx_fast(tbase, nP, BLOCK), cd, n, nP);
     } else if constexpr (ALGO == ALGO_CE) {
         auto count = [&](uint32_t j, uint32_t i) -> uint32_t {
             if constexpr (CNT16) {

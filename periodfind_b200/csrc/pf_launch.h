@@ -11,7 +11,11 @@ namespace pfk {
 // KIND_LSREC: Lomb-Scargle on a uniform frequency grid with the
 // angle-addition recurrence along the grid (pf_lsrec.cuh); `rounds` holds
 // its frequencies per thread.
-enum : int { KIND_FOLD = 0, KIND_BIN = 1, KIND_LSREC = 2 };
+// KIND_BINWARP: the chosen CE / AOV binning with one shared histogram per
+// warp and trial period, filled with shared atomics (pf_binwarp.cuh), the
+// alternative to KIND_BIN's per-thread privatised histograms.
+enum : int { KIND_FOLD = 0, KIND_BIN = 1, KIND_LSREC = 2, KIND_BINWARP = 3 };
+constexpr uint32_t kWarpMaxPoints = 1024;  // KIND_BINWARP: longest curve it stages
 constexpr uint32_t kRecTileBytes = 512 * 16;  // lsrec_kernel's staged points
 
 // Kernels that take their items from the device work queue (a curve order;
@@ -20,7 +24,8 @@ constexpr uint32_t kRecTileBytes = 512 * 16;  // lsrec_kernel's staged points
 // counter) or statically (one CTA per item).  The reference fold and the
 // all-FP32 study fold take one CTA per item of a host-built list.
 __host__ __device__ constexpr bool uses_queue(int kind, int fold) {
-    return kind == KIND_BIN || kind == KIND_LSREC || fold == FOLD_EXACT || fold == FOLD_DF;
+    return kind == KIND_BIN || kind == KIND_LSREC || kind == KIND_BINWARP || fold == FOLD_EXACT ||
+           fold == FOLD_DF;
 }
 
 struct FoldConfig {

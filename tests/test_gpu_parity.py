@@ -488,6 +488,30 @@ def test_autotuned_launch_shapes_change_no_value(gpu):
     assert "ce bin" in report and "aov bin" in report and "ls fold-split" in report
 
 
+def test_shared_histogram_binning_changes_no_value(gpu):
+    """The chosen CE / AOV binning with shared histograms and atomics
+    (PF_BINS_SHARED; one histogram per warp and period) gives the
+    privatised form's values bit for bit, untuned and tuned, on every
+    length class it serves and beside the longer classes it leaves to the
+    privatised form; both overlaps of one, with and without a period
+    derivative; the tuner lists the strategy it kept per class."""
+    from periodfind_b200 import _native as nat
+
+    lengths = [1, 2, 5, 10, 31, 32, 33, 63, 64, 100, 255, 256, 257, 700, 1023, 1024, 3000]
+    ts, ms = _ragged(seed=43, lengths=lengths)
+    msn = [lc.normalize(m) if len(m) > 1 else np.full(1, 0.5, np.float32) for m in ms]
+    P, D = _grid(700, pdts=(0.0, 2e-5))
+    for make, mags in ((lambda **k: gpu.ConditionalEntropy(**k), msn),
+                       (lambda **k: gpu.AOV(15, **k), ms)):
+        want = make(mode="chosen").periodograms(ts, mags, P, D)
+        for extra in (nat.PF_BINS_SHARED | nat.PF_NO_TUNE, nat.PF_BINS_SHARED):
+            obj = make(mode="chosen")
+            obj._flags |= extra
+            np.testing.assert_array_equal(obj.periodograms(ts, mags, P, D), want)
+    report = nat.default_context(0).tuning_report()
+    assert "bins=shared-atomic" in report and "bins=privatised" in report, report
+
+
 @pytest.mark.parametrize("use_max", [True, False])
 def test_peaks_adversarial_rows_match_oracle(gpu, oracle, use_max):
     """The device peak search drops extrema that are not better than the
