@@ -590,6 +590,12 @@ int tuned_config(pf_ctx* ctx, const Job& j, const FoldConfig& base, int cls, uin
 
     const double per_curve = (double)cls_points / (double)nc * (double)j.n_per * (double)j.n_pdt;
     uint64_t k = (uint64_t)std::max(1.0, std::ceil(2e9 / std::max(per_curve, 1.0)));
+    // Enough curves that the candidate with the largest items (2048 periods)
+    // still has four items per SM: a sample that leaves SMs idle would
+    // favour small items over what the whole class runs best with.
+    const uint64_t big_items = j.n_pdt * ((j.n_per + 2047) / 2048);
+    k = std::max<uint64_t>(k, (4ull * (uint64_t)std::max(ctx->n_sm, 1) + big_items - 1) /
+                                  std::max<uint64_t>(big_items, 1));
     k = std::min(k, nc);
     const uint64_t s0 = c0 + (nc - k) / 2;
     FoldParams ps = p;

@@ -68,7 +68,8 @@ def test_tuner_reports_trig_choice(gpu):
     ts, ms, _, _ = lc.ls_study_curves(len(lengths), seed=32, lengths=lengths)
     f_min, df, n = _grid(3000)
     gpu.LombScargle().periodograms_frequency_grid(ts, ms, f_min, df, n)
-    rep = [ln for ln in nat.default_context(0).tuning_report().splitlines() if "fgrid" in ln]
+    rep = [ln for ln in nat.default_context(0).tuning_report().splitlines()
+           if "fold-split-fgrid " in ln]
     print("\n" + "\n".join(rep))
     assert len(rep) == 5 and all("trig=" in ln for ln in rep)
 
