@@ -489,6 +489,7 @@ def _refine_f64(t, y, w0, hw, n_steps=5, keep_last=1e-5):
     w = w0.copy()
     best_w, best_p = w.copy(), np.full_like(w, -1.0)
     last_w, last_p = w.copy(), best_p.copy()
+    moved = np.full_like(w, np.inf)
     for e in range(n_steps + 1):
         P, P1, P2 = _ls_derivs_f64(t, y, w)
         last_w, last_p = w.copy(), P
@@ -498,8 +499,11 @@ def _refine_f64(t, y, w0, hw, n_steps=5, keep_last=1e-5):
         if e < n_steps:
             step = np.where(P2 < 0, -P1 / np.where(P2 < 0, P2, -1.0),
                             np.where(P1 > 0, 0.25 * hw, -0.25 * hw))
-            w = np.clip(w + step, w0 - hw, w0 + hw)
-    return np.where(last_p >= best_p * (1.0 - keep_last), last_w, best_w)
+            nw = np.clip(w + step, w0 - hw, w0 + hw)
+            moved = np.abs(nw - w) / np.abs(w)
+            w = nw
+    out = np.where(last_p >= best_p * (1.0 - keep_last), last_w, best_w)
+    return out, moved
 
 
 def ls_peak_error(step, periods, n_sample, torch, seed=SEED + 9):
@@ -532,23 +536,31 @@ def ls_peak_error(step, periods, n_sample, torch, seed=SEED + 9):
                                 torch.from_numpy(w0).to(dev), torch.from_numpy(hw).to(dev),
                                 sub_off, n_steps=5)
     w = w.cpu().numpy()
-    errs = []
+    errs, conv = [], []
     for k in range(n_sample):
         v = valid[k]
         if len(ts[k]) < 16 or not v.any():
             continue
         t = ts[k].astype(np.float64)
         t = t - 0.5 * (t.min() + t.max())
-        ref = _refine_f64(t, ys[k].astype(np.float64), w0[k][v], hw[k][v])
+        ref, moved = _refine_f64(t, ys[k].astype(np.float64), w0[k][v], hw[k][v])
         errs.extend((np.abs(w[k][v] - ref) / ref).tolist())
+        conv.extend((moved <= 1e-9).tolist())
     errs = np.array(errs) if errs else np.zeros(1)
-    return {"peaks": int(errs.size), "curves": n_sample, "max_rel": float(errs.max()),
-            "median_rel": float(np.median(errs)), "p99_rel": float(np.percentile(errs, 99)),
-            "target": 1e-7,
+    conv = np.array(conv, bool) if conv else np.ones(1, bool)
+    ec = errs[conv] if conv.any() else np.zeros(1)
+    return {"peaks": int(errs.size), "curves": n_sample,
+            "converged_peaks": int(conv.sum()),
+            "max_rel_converged": float(ec.max()), "median_rel": float(np.median(errs)),
+            "p99_rel": float(np.percentile(errs, 99)), "max_rel_all": float(errs.max()),
+            "within_target": float(np.mean(errs <= 1e-7)), "target": 1e-7,
             "method": "top-32 grid peaks of the chosen LS periodogram of 64 random curves, "
                       "refined by 5 safeguarded Newton steps on the GPU (pf_ls_refine_dev) and "
                       "by the same iteration in FP64 (numpy, analytic derivatives) from the "
-                      "same starts; relative frequency difference"}
+                      "same starts; relative frequency difference.  'converged': the FP64 "
+                      "iteration's last step moved the frequency by at most 1e-9 (elsewhere "
+                      "the 5-step iteration has not settled and the difference measures the "
+                      "path, not the arithmetic)"}
 
 
 # ------------------------------------------------------------ baselines

@@ -234,7 +234,7 @@ int validate_common(pf_ctx* ctx, const Job& j) {
     }
     if (j.n_curves > 0 && (j.n_per == 0 || j.n_pdt == 0)) return PF_OK;  // nothing to compute
     if (j.n_per > 0 && !j.periods && !j.fgrid) return fail(ctx, PF_EINVAL, "periods is NULL");
-    if (j.n_pdt > 0 && !j.pdts) return fail(ctx, PF_EINVAL, "period_dts is NULL");
+    if (j.n_pdt > 0 && !j.pdts && !j.fgrid) return fail(ctx, PF_EINVAL, "period_dts is NULL");
     if (j.n_per > 0xFFFFFFFFull || j.n_pdt > 0xFFFFull)
         return fail(ctx, PF_EINVAL, "grid too large (n_per %llu, n_pdt %llu)",
                     (unsigned long long)j.n_per, (unsigned long long)j.n_pdt);
