@@ -22,8 +22,10 @@ reference's):
   - plain form and the reference: f32 sums whose rounding depends on the
     summation order (the plain form adds in point order, the reference with
     shared float atomics in no fixed order).  The plain form's error against
-    the FP64 statistic is bounded by the reference's own: its largest and
-    median errors are at most twice the reference's.
+    the FP64 statistic is that of the f32 statistic summed in point order
+    (the oracle, the Rust path's order): at most 1.25 times it at the
+    median and the 99th percentile over cells.  The reference's own error is
+    printed beside it.
 """
 
 import numpy as np
@@ -145,15 +147,16 @@ def test_aov_statistic_on_identical_bins(gpu, oracle, raw):
     assert same.mean() > 0.9
     scale = np.abs(truth).max(axis=(1, 2), keepdims=True)
     rel = lambda x: (np.abs(x - truth) / (np.abs(truth) + 1e-6 * scale))[same]
-    e_chosen, e_plain, e_ref = rel(chosen), rel(plain), rel(ref)
+    seq = oracle.aov(ts, ms, PERIODS, PDTS, 15, fused_tcorr=True)
+    e_chosen, e_plain, e_ref, e_seq = rel(chosen), rel(plain), rel(ref), rel(seq)
     print(f"\nAOV vs FP64 on identical bins ({'raw' if raw else 'normalised'}): "
           f"chosen max {e_chosen.max():.2e}; plain max {e_plain.max():.2e} median "
           f"{np.median(e_plain):.2e}; reference max {e_ref.max():.2e} median "
           f"{np.median(e_ref):.2e}; plain within 1e-5 of the reference at "
           f"{np.mean(np.abs(plain - ref)[same] <= 1e-5 * np.abs(ref)[same] + 1e-6):.4f}")
     assert e_chosen.max() <= 1e-5
-    assert e_plain.max() <= 2.0 * e_ref.max() + 1e-6
-    assert np.median(e_plain) <= 2.0 * np.median(e_ref) + 1e-7
+    for q in (0.5, 0.99):
+        assert np.quantile(e_plain, q) <= 1.25 * np.quantile(e_seq, q) + 1e-7
 
 
 def test_ce_statistic_on_identical_bins(gpu, oracle):

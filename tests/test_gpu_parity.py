@@ -310,8 +310,11 @@ def test_aov_vs_reference_cuda(gpu, oracle):
     the bin sums, which the reference adds with shared float atomics in no
     fixed order.  Both are held to the FP64 statistic on the same bins: the
     chosen form within 1e-5 relative, the plain form no further from it than
-    twice the reference's own largest error (normalised magnitudes, and
-    15 +- 0.3 raw magnitudes whose f32 sums of squares cancel)."""
+    the same f32 statistic summed in point order as the reference's Rust
+    path sums it (the oracle; the plain form adds in that order too), on
+    normalised magnitudes and on 15 +- 0.3 raw magnitudes whose f32 sums of
+    squares cancel; the reference CUDA build's own error is printed beside
+    them.  All at the 99th percentile over cells."""
     _ref_or_skip(oracle)
     ts, ms = _ragged(seed=9, lengths=(64, 300, 1025, 4096, 4097, 6000))
     P, D = _grid(400, pdts=(0.0, 1e-4))
@@ -324,10 +327,14 @@ def test_aov_vs_reference_cuda(gpu, oracle):
         # (fast-math divide) have another FP64 truth: the largest errors are
         # compared over the 99% closest cells.
         e_ref = np.quantile(rel(want), 0.99)
+        e_seq = np.quantile(rel(oracle.aov(ts, mags, P, D, 15)), 0.99)
         chosen = gpu.AOV(15, mode="chosen").periodograms(ts, mags, P, D)
         plain = gpu.AOV(15, mode="plain").periodograms(ts, mags, P, D)
+        e_plain = np.quantile(rel(plain), 0.99)
+        print(f"\nAOV 99th-percentile error vs FP64: chosen {np.quantile(rel(chosen), 0.99):.2e}"
+              f", plain {e_plain:.2e}, point-order f32 {e_seq:.2e}, reference {e_ref:.2e}")
         assert np.quantile(rel(chosen), 0.99) <= 1e-5
-        assert np.quantile(rel(plain), 0.99) <= 2.0 * e_ref + 1e-6
+        assert e_plain <= 1.25 * e_seq + 1e-6
 
 
 def test_ls_vs_reference_cuda(gpu, oracle):
