@@ -352,7 +352,8 @@ int pf_find_peaks_dev(pf_ctx* ctx, const float* d_data, uint64_t n_curves,
  * more is rejected with PF_EINVAL and a message in `err` (a caller buffer of
  * err_len bytes, may be NULL).  The first call on a device looks up the
  * array's address with that device current: make it before any stream
- * capture.  Calls share the array, so calls whose GPU work overlaps race on
+ * capture (the lookup is repeated once for a new CUDA context, e.g. after
+ * cudaDeviceReset).  Calls share the array, so calls whose GPU work overlaps race on
  * it; order them on one stream.  Work is enqueued on `stream` (NULL = the
  * CUDA default stream) and the call returns without synchronising. */
 int pf_ls_peaks_dev_noalloc(const float* d_times, const float* d_mags,

@@ -21,12 +21,15 @@
 // Rules for callers:
 //  - The first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//    before any stream capture.  The address is kept per device and CUDA
+//    context: after cudaDeviceReset, or under another context, the next call
+//    looks it up again (and should likewise come before any capture).
 //  - Every call shares the one array and leaves its contents behind: calls
 //    whose GPU work overlaps (different streams, or host threads with
 //    different streams) race on it.  Order them on one stream.
 //  - The call enqueues work on `stream` and returns; outputs are ready when
 //    the stream reaches that point.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdint.h>
@@ -52,8 +55,26 @@ constexpr int kBlock = 256;  // LS launch shape (no histogram)
 
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-std::mutex g_mu;                       // guards g_meta and g_ptr
+std::mutex g_mu;                       // guards g_meta, g_ptr and g_ctx
 unsigned char* g_ptr[kMaxDevices];     // g_scratch's device address per device
+CUcontext g_ctx[kMaxDevices];          // the context that address belongs to
+
+// The calling thread's current CUDA context (the driver's cuCtxGetCurrent,
+// reached through the runtime; NULL if it cannot be had).
+CUcontext current_context() {
+    using Fn = CUresult (*)(CUcontext*);
+    static Fn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<Fn>(f);
+    }();
+    CUcontext c = nullptr;
+    if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+    return c;
+}
 alignas(256) unsigned char g_meta[kMetaBytes];
 
 // Write the message into the caller's buffer (if any) and return `code`.
@@ -153,14 +174,16 @@ extern "C" int pf_ls_peaks_dev_noalloc(const float* d_times, const float* d_mags
     if (dev < 0 || dev >= kMaxDevices) return fail(err, err_len, PF_EUNSUPPORTED, "device index %d", dev);
 
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_ptr[dev]) {
-        // One-time set-up on this device (with it current): the host-side
-        // name g_scratch is only a stand-in; the kernels need its address.
+    if (!g_ptr[dev] || g_ctx[dev] != current_context()) {
+        // Set-up on this device (with it current), once per context: the
+        // host-side name g_scratch is only a stand-in; the kernels need its
+        // address, which a new context (after cudaDeviceReset) moves.
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_scratch);
         if (e != cudaSuccess)
             return fail(err, err_len, PF_ECUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
         g_ptr[dev] = static_cast<unsigned char*>(p);
+        g_ctx[dev] = current_context();
     }
     unsigned char* base = g_ptr[dev];
     cudaStream_t s = (cudaStream_t)stream;

@@ -89,6 +89,43 @@ def test_noalloc_matches_allocating_path_two_calls():
         assert (ni[:, 0] >= 0).all()
 
 
+def test_noalloc_allocates_nothing():
+    """After a first call, further calls with other batch layouts leave the
+    device's free memory exactly as it was: the entry point allocates
+    nothing (the inputs and outputs are made before the measurement)."""
+    torch = pytest.importorskip("torch")
+    from periodfind_b200 import _native as nat
+
+    lib = nat.load()
+    batches = []
+    for seed, lengths, n_per in ((3, (300, 50, 1200), 800), (4, (2000, 10, 700, 90), 1500)):
+        ts, ms, periods, pd = _batch(seed, lengths, n_per, (0.0,))
+        off = np.zeros(len(ts) + 1, np.int64)
+        np.cumsum([len(t) for t in ts], out=off[1:])
+        batches.append((torch.from_numpy(np.concatenate(ts)).cuda(),
+                        torch.from_numpy(np.concatenate(ms)).cuda(), off,
+                        torch.from_numpy(periods).cuda(), torch.from_numpy(pd).cuda(),
+                        torch.empty((len(ts), 8), dtype=torch.int64, device="cuda"),
+                        torch.empty((len(ts), 8), dtype=torch.float32, device="cuda")))
+    err = ctypes.create_string_buffer(512)
+
+    def call(b):
+        d_t, d_m, off, d_p, d_d, idx, val = b
+        rc = lib.pf_ls_peaks_dev_noalloc(d_t.data_ptr(), d_m.data_ptr(), off.ctypes.data,
+                                         len(off) - 1, d_p.data_ptr(), d_p.numel(),
+                                         d_d.data_ptr(), d_d.numel(), 8, 1, nat.PF_MODE_CHOSEN,
+                                         idx.data_ptr(), val.data_ptr(), None, err, len(err))
+        assert rc == 0, err.value.decode()
+        torch.cuda.synchronize()
+
+    call(batches[0])  # first call on the device: its one-time set-up
+    free0, _ = torch.cuda.mem_get_info()
+    call(batches[1])
+    call(batches[0])
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_rejects_batch_beyond_its_scratch():
     torch = pytest.importorskip("torch")
     from periodfind_b200 import _native as nat
