@@ -830,7 +830,7 @@ def ragged_main(args):
     # Per algorithm: the plan's replay (CUDA events), the fold / bin kernels
     # alone (the library's events around the class launches of a direct
     # chosen call, tuned by its first call), per-curve latency.
-    algo_ms, kernel_ms, latency = {}, {}, {}
+    algo_ms, kernel_ms, latency, one_launch_ms = {}, {}, {}, {}
     for algo in ALGOS:
         plan = step.plans[algo]
         algo_ms[algo], _ = time_steps(lambda: plan.launch(stream), 3, 1, torch, flush, stream)
@@ -841,6 +841,10 @@ def ragged_main(args):
             torch.cuda.synchronize()
             ks.append(step.ctx.last_kernel_ms)
         kernel_ms[algo] = float(np.mean(ks))
+        # The same kernels with every length class in one launch (one shape).
+        step.direct(algo, nat.PF_MODE_CHOSEN | nat.PF_ONE_LAUNCH, peaks=False)
+        torch.cuda.synchronize()
+        one_launch_ms[algo] = step.ctx.last_kernel_ms
         latency[algo] = {"chosen": curve_latency(step, algo, nat.PF_MODE_CHOSEN),
                          "plain": curve_latency(step, algo, nat.PF_MODE_PLAIN)}
     step.chosen()  # the chosen peaks back in pk_i / pk_v for the precision check
@@ -888,6 +892,8 @@ def ragged_main(args):
                 "path": "gpu.ConditionalEntropy / AOV / LombScargle .calc(list of numpy, "
                         "output='peaks'), 3.2e6 Statistics objects per algorithm"},
             "algo_ms": algo_ms, "kernels_ms": kernel_ms,
+            "kernels_ms_one_launch": one_launch_ms,
+            "tuning": step.ctx.tuning_report().strip().splitlines(),
             "latency_per_curve": latency,
             "ls_peak_frequency_error": prec,
             "roofline": _roofline(kernel_ms, evals_algo, pipes, off, periods, pdts),

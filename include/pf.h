@@ -75,6 +75,10 @@
  *                  shorter than 1024 points) instead of letting the
  *                  autotuner weigh it against per-thread privatised
  *                  histograms.  Values are identical either way.
+ *  PF_ONE_LAUNCH   (chosen) run every curve in one launch with the shape
+ *                  tuned for the length class holding the most points,
+ *                  instead of one launch per class with its own tuned shape
+ *                  (for comparison; values are identical).
  */
 #ifndef PERIODFIND_B200_PF_H
 #define PERIODFIND_B200_PF_H
@@ -105,6 +109,7 @@ extern "C" {
 #define PF_TRIG_SINCOS 0x10000
 #define PF_TRIG_RECURRENCE 0x20000
 #define PF_BINS_SHARED 0x40000
+#define PF_ONE_LAUNCH 0x80000
 
 typedef struct pf_ctx pf_ctx;
 

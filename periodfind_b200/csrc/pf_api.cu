@@ -712,6 +712,24 @@ int launch_classes(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig&
             return rc;
         total_items += queue_items(j, r[c].n, item_periods(cc[c]));
     }
+    if (j.mode & PF_ONE_LAUNCH) {
+        // Every curve in one launch with the shape tuned for the class that
+        // holds the most points (or, where that shape is the shared-histogram
+        // binning and longer curves are present, the longest class's).
+        int d = -1, longest = -1;
+        for (int c = 0; c < kClasses; c++) {
+            if (!r[c].n) continue;
+            if (d < 0 || r[c].points > r[d].points) d = c;
+            longest = c;
+        }
+        if (cc[d].kind == KIND_BINWARP && longest > kWarpClassMax) d = longest;
+        const FoldConfig one = cc[d];
+        const uint64_t pts = L.total_pts;
+        for (int c = 0; c < kClasses; c++) r[c] = Range{0, 0, 0};
+        r[0] = Range{0, j.n_curves, pts};
+        cc[0] = one;
+        total_items = queue_items(j, j.n_curves, item_periods(one));
+    }
     if (total_items > 0x7FFFFFFFull) return fail(ctx, PF_EINVAL, "too much work for one launch");
     if (j.mode & PF_TIMING) {
         if ((rc = ensure_dev(ctx, ctx->d_stamps, (size_t)total_items * 16)) != PF_OK) return rc;

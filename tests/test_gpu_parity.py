@@ -489,6 +489,10 @@ def test_autotuned_launch_shapes_change_no_value(gpu):
         untuned_obj = make(mode="chosen")
         untuned_obj._flags |= nat.PF_NO_TUNE
         np.testing.assert_array_equal(tuned, untuned_obj.periodograms(ts, mags, P, D))
+        # Every class in one launch with one shape: the same values.
+        one_obj = make(mode="chosen")
+        one_obj._flags |= nat.PF_ONE_LAUNCH
+        np.testing.assert_array_equal(tuned, one_obj.periodograms(ts, mags, P, D))
     report = ctx.tuning_report()
     for name in ("[0,64)", "[64,256)", "[256,1024)", "[1024,4096)", "[4096,inf)"):
         assert f"class={name}" in report, report
