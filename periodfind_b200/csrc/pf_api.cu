@@ -30,6 +30,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/pf.h"
 #include "pf_launch.h"
 #include "pf_types.h"
@@ -49,6 +51,16 @@ struct PinnedBuf {
 };
 
 thread_local std::string g_create_error;
+
+// An NVTX range around one stage of a call (pack, copies, preparation,
+// fold / bin kernels, statistics, peak search), seen by a profiler's
+// timeline; without a profiler attached it costs a function-pointer check.
+struct Stage {
+    explicit Stage(const char* name) { nvtxRangePushA(name); }
+    ~Stage() { nvtxRangePop(); }
+    Stage(const Stage&) = delete;
+    Stage& operator=(const Stage&) = delete;
+};
 
 }  // namespace
 
@@ -786,6 +798,7 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
     if ((rc = ensure_dev(ctx, ctx->d_misc, 256)) != PF_OK) return rc;
     static_assert(kCounterOffset + 4 * (kClasses + 1) <= 256, "counters fit the misc block");
     p.tmax_bits = (const unsigned*)ctx->d_misc.p;
+    Stage stage_prep("pf prepare");
     PF_CUDA(launch_tmax(p.t, L.total_pts, (unsigned*)ctx->d_misc.p, s), "max|t| kernel");
     ctx->launches++;
     if (cfg.kind == KIND_BIN && j.algo == ALGO_CE) {
@@ -826,6 +839,8 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
         ctx->launches++;
     }
     p.stamps = nullptr;
+    Stage stage_fold(j.algo == ALGO_LS ? "pf LS fold" : j.algo == ALGO_CE ? "pf CE bins"
+                                                                          : "pf AOV bins");
     if (uses_queue(cfg.kind, cfg.fold)) {
         // The staged work section holds the curve order (fill_meta).
         p.q.order = reinterpret_cast<const uint32_t*>(p.work);
@@ -845,6 +860,7 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
         ctx->timed_pending = true;
     }
     if (j.stats) {
+        Stage stage_stats("pf statistics");
         const size_t pk = (size_t)j.n_curves * std::max<uint32_t>(j.n_top, 1u);
         if ((rc = ensure_dev(ctx, ctx->d_pidx, pk * 8)) != PF_OK) return rc;
         if ((rc = ensure_dev(ctx, ctx->d_pval, pk * 4)) != PF_OK) return rc;
@@ -856,6 +872,7 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
         ctx->launches++;
     }
     if (j.peaks && j.n_peaks > 0) {
+        Stage stage_peaks("pf peak search");
         const size_t pk = (size_t)j.n_curves * j.n_peaks;
         if ((rc = ensure_dev(ctx, ctx->d_pidx, pk * 8)) != PF_OK) return rc;
         if ((rc = ensure_dev(ctx, ctx->d_pval, pk * 4)) != PF_OK) return rc;
@@ -948,6 +965,7 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
 
     // Pack the curves (several host threads for large batches).
     {
+        Stage stage_pack("pf pack");
         const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
         const unsigned nthr = (L.total_pts > (1u << 20)) ? hw : 1u;
         std::vector<int> bad(nthr, 0);
@@ -975,7 +993,10 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
 
     cudaStream_t s = ctx->stream;
     char* db = (char*)ctx->d_in.p;
-    PF_CUDA(cudaMemcpyAsync(db, hb, L.bytes, cudaMemcpyHostToDevice, s), "H2D inputs");
+    {
+        Stage stage_h2d("pf H2D");
+        PF_CUDA(cudaMemcpyAsync(db, hb, L.bytes, cudaMemcpyHostToDevice, s), "H2D inputs");
+    }
     PF_CUDA(cudaEventRecord(ctx->ev_staged, s), "event");
     ctx->staged_pending = true;
 
