@@ -341,13 +341,19 @@ def _stats_from_device(st, idx, val, periods, period_dts, n_stats, significance_
     """Statistics objects from the device statistics, typed as the reference
     builds them from numpy (float32 scalars), best first."""
     n_pdt = len(period_dts)
+    # numpy float32 scalars throughout, as the reference's numpy statistics
+    # hold them; list() makes a row's scalars in one call.
+    k = idx.shape[1]
+    per = list(np.asarray(periods)[idx // n_pdt].ravel())
+    pdt = list(np.asarray(period_dts)[idx % n_pdt].ravel())
+    vals = list(np.asarray(val).ravel())
+    summ = list(np.asarray(st).ravel())
     out = []
     with gc_paused():
         for c in range(st.shape[0]):
-            mean, std, median, mad = st[c]
-            best = [Statistics([periods[k // n_pdt], period_dts[k % n_pdt]], val[c, j], mean,
-                               std, median, mad, significance_type)
-                    for j, k in enumerate(idx[c].tolist())]
+            mean, std, median, mad = summ[4 * c:4 * c + 4]
+            best = [Statistics([per[c * k + j], pdt[c * k + j]], vals[c * k + j], mean, std,
+                               median, mad, significance_type) for j in range(k)]
             out.append(best[0] if n_stats == 1 else best)
     return out
 
