@@ -244,6 +244,30 @@ def small_arm(args):
         kms, ws = float(np.median(k)), float(np.median(w))
         out[mode] = {"kernel_ms": kms, "evals_per_s": evals / (kms * 1e-3),
                      "e2e_ms": ws * 1e3, "e2e_evals_per_s": evals / ws}
+    # End to end through the C ABI from the host arrays (no Python result
+    # objects): pf_ce_stats with the normalisation fused into the packing,
+    # statistics and best cells back in host arrays.
+    bt = nat.CurveBatch(ts, ms)
+    st = np.empty((n_curves, 4), np.float32)
+    bi = np.empty((n_curves, 1), np.int64)
+    bv = np.empty((n_curves, 1), np.float32)
+
+    def cabi():
+        ctx.check(ctx.lib.pf_ce_stats(ctx.handle, *bt.args(), periods.ctypes.data, len(periods),
+                                      pdts.ctypes.data, 1, 10, 10, 1, 1, 1,
+                                      nat.PF_MODE_CHOSEN | nat.PF_HOST_NORMALIZE,
+                                      st.ctypes.data, bi.ctypes.data, bv.ctypes.data))
+    for _ in range(3):
+        cabi()
+    w = []
+    with clocks.region("chosen_e2e_cabi"):
+        t_end = time.perf_counter() + 1.0
+        while len(w) < max(3, args.steps) or time.perf_counter() < t_end:
+            t0 = time.perf_counter()
+            cabi()
+            w.append(time.perf_counter() - t0)
+    out["chosen"]["e2e_cabi_ms"] = float(np.median(w)) * 1e3
+    out["chosen"]["e2e_cabi_evals_per_s"] = evals / float(np.median(w))
     a = gpu.ConditionalEntropy(mode="plain").periodograms(ts, msn, periods, pdts)
     b = gpu.ConditionalEntropy(mode="chosen", reference_stats=True).periodograms(
         ts, msn, periods, pdts)

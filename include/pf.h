@@ -79,6 +79,11 @@
  *                  tuned for the length class holding the most points,
  *                  instead of one launch per class with its own tuned shape
  *                  (for comparison; values are identical).
+ *  PF_HOST_NORMALIZE / PF_HOST_CENTER  (host-pointer periodogram, peak and
+ *                  stats calls) prepare the magnitudes while packing them,
+ *                  as pf_normalize_mags / pf_center_mags would (numpy's
+ *                  values): the caller passes raw magnitudes and saves a
+ *                  pass and a copy.  Empty curves are left as they are.
  */
 #ifndef PERIODFIND_B200_PF_H
 #define PERIODFIND_B200_PF_H
@@ -110,6 +115,8 @@ extern "C" {
 #define PF_TRIG_RECURRENCE 0x20000
 #define PF_BINS_SHARED 0x40000
 #define PF_ONE_LAUNCH 0x80000
+#define PF_HOST_NORMALIZE 0x100000
+#define PF_HOST_CENTER 0x200000
 
 typedef struct pf_ctx pf_ctx;
 

@@ -36,6 +36,8 @@ PF_TRIG_SINCOS = 0x10000
 PF_TRIG_RECURRENCE = 0x20000
 PF_BINS_SHARED = 0x40000
 PF_ONE_LAUNCH = 0x80000
+PF_HOST_NORMALIZE = 0x100000
+PF_HOST_CENTER = 0x200000
 PF_PREP_CENTER, PF_PREP_NORMALIZE = 1, 2
 PF_ALGO_CE, PF_ALGO_AOV, PF_ALGO_LS = 0, 1, 2
 

@@ -175,6 +175,110 @@ int ensure_pinned(pf_ctx* ctx, PinnedBuf& b, size_t bytes) {
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// numpy's pairwise float32 summation (the add.reduce behind np.mean of a
+// contiguous float32 array; numpy/_core/src/umath/loops_utils.h.src,
+// pairwise_sum): fewer than 8 elements are added in order starting from
+// -0.0; up to 128 elements go to eight interleaved accumulators, combined as
+// ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7)), then the remainder in
+// order; a longer range splits at n / 2 rounded down to a multiple of 8 and
+// the two halves' sums are added.  This unit is built without contraction,
+// so every addition is one IEEE float32 rounding, as in numpy.
+float numpy_pairwise_sum(const float* a, uint64_t n) {
+    if (n < 8) {
+        float res = -0.0f;
+        for (uint64_t i = 0; i < n; i++) res += a[i];
+        return res;
+    }
+    if (n <= 128) {
+        float r[8];
+        for (int k = 0; k < 8; k++) r[k] = a[k];
+        uint64_t i = 8;
+        for (; i < n - (n % 8); i += 8)
+            for (int k = 0; k < 8; k++) r[k] += a[i + k];
+        float res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+        for (; i < n; i++) res += a[i];
+        return res;
+    }
+    uint64_t n2 = n / 2;
+    n2 -= n2 % 8;
+    return numpy_pairwise_sum(a, n2) + numpy_pairwise_sum(a + n2, n - n2);
+}
+
+// Run fn(c) for every curve, on several host threads when the batch holds
+// more than 2^20 points (curves interleaved across the threads).
+template <class F>
+void for_each_curve(uint64_t n_curves, uint64_t total_points, F& fn) {
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const unsigned nthr = total_points > (1u << 20) ? hw : 1u;
+    if (nthr == 1) {
+        for (uint64_t c = 0; c < n_curves; c++) fn(c);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned w = 0; w < nthr; w++)
+        th.emplace_back([&, w] {
+            for (uint64_t c = w; c < n_curves; c += nthr) fn(c);
+        });
+    for (auto& t : th) t.join();
+}
+
+// The reference's normalize=True preparation of one curve
+// (periodfind/_utils.py:39-45) with numpy's float32 arithmetic:
+// ((m - min) / (max - min)) * 0.999 + 5e-4, out may equal m.
+void normalize_curve(const float* m, uint64_t n, float* o) {
+    // Per curve: numpy's float32 min / max (NaN propagates), then
+    // ((m - lo) / (hi - lo)) * 0.999f + 5e-4f in single precision, one
+    // rounding per operation, as numpy evaluates the same expression.
+    float lo = m[0], hi = m[0];
+    bool nan = std::isnan(m[0]);
+    uint64_t i = 1;
+    if (n >= 16) {
+        // Eight interleaved running minima / maxima, which the compiler
+        // turns into SIMD min / max.  Without NaN the result is the exact
+        // minimum and maximum whatever the order; only the sign of a
+        // zero extreme may differ, and lo, hi enter the output solely
+        // through m - lo and hi - lo, whose values it does not change.
+        float l[8], h[8];
+        int bad[8];
+        for (int k = 0; k < 8; k++) {
+            l[k] = h[k] = m[k];
+            bad[k] = 0;
+        }
+        for (i = 0; i + 8 <= n; i += 8)
+            for (int k = 0; k < 8; k++) {
+                const float v = m[i + k];
+                bad[k] |= (v != v);
+                l[k] = v < l[k] ? v : l[k];
+                h[k] = v > h[k] ? v : h[k];
+            }
+        for (int k = 0; k < 8; k++) {
+            nan |= bad[k] != 0;
+            lo = l[k] < lo ? l[k] : lo;
+            hi = h[k] > hi ? h[k] : hi;
+        }
+    }
+    for (; i < n; i++) {
+        const float v = m[i];
+        nan |= std::isnan(v);
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
+    }
+    if (nan) lo = hi = std::numeric_limits<float>::quiet_NaN();
+    // This unit is built with -ffp-contract=off: no fused multiply-add.
+    const float range = hi - lo;
+    for (uint64_t i = 0; i < n; i++) o[i] = ((m[i] - lo) / range) * 0.999f + 5e-4f;
+}
+
+// The reference's center=True preparation of one curve
+// (periodfind/_utils.py:35-37): np.mean of a float32 array is the pairwise
+// float32 sum divided by the length in float32; then m - mean, one
+// rounding per point.  out may equal m.
+void center_curve(const float* m, uint64_t n, float* o) {
+    const float mean = numpy_pairwise_sum(m, n) / (float)n;
+    for (uint64_t i = 0; i < n; i++) o[i] = m[i] - mean;
+}
+
+
 // What one call computes.
 struct Job {
     int algo = ALGO_CE;
@@ -943,6 +1047,8 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
             return fail(ctx, PF_EINVAL, "%d PF_ASYNC calls are pending; collect one with pf_wait",
                         pf_ctx::kMaxPending);
     }
+    if ((j.mode & PF_HOST_NORMALIZE) && (j.mode & PF_HOST_CENTER))
+        return fail(ctx, PF_EINVAL, "PF_HOST_NORMALIZE and PF_HOST_CENTER exclude each other");
     if (j.n_curves == 0) return async ? push_pending(ctx, j, 0, false, nullptr) : PF_OK;
     if (!times || !mags || !lengths) return fail(ctx, PF_EINVAL, "times/mags/lengths is NULL");
     const uint64_t n_cells = j.n_per * j.n_pdt;
@@ -975,6 +1081,12 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
                 const uint32_t pad = (uint32_t)align_up(n, 4);
                 if (!copy_curve(times[c], mags[c], n, ht + L.off[c], hm + L.off[c], pad))
                     bad[w] = 1;
+                // Magnitude preparation fused into the packing (numpy's
+                // values, as pf_normalize_mags / pf_center_mags).
+                if (n && (j.mode & PF_HOST_NORMALIZE))
+                    normalize_curve(hm + L.off[c], n, hm + L.off[c]);
+                else if (n && (j.mode & PF_HOST_CENTER))
+                    center_curve(hm + L.off[c], n, hm + L.off[c]);
             }
         };
         if (nthr == 1) {
@@ -1346,53 +1458,6 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
     return PF_OK;
 }
 
-// numpy's pairwise float32 summation (the add.reduce behind np.mean of a
-// contiguous float32 array; numpy/_core/src/umath/loops_utils.h.src,
-// pairwise_sum): fewer than 8 elements are added in order starting from
-// -0.0; up to 128 elements go to eight interleaved accumulators, combined as
-// ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7)), then the remainder in
-// order; a longer range splits at n / 2 rounded down to a multiple of 8 and
-// the two halves' sums are added.  This unit is built without contraction,
-// so every addition is one IEEE float32 rounding, as in numpy.
-float numpy_pairwise_sum(const float* a, uint64_t n) {
-    if (n < 8) {
-        float res = -0.0f;
-        for (uint64_t i = 0; i < n; i++) res += a[i];
-        return res;
-    }
-    if (n <= 128) {
-        float r[8];
-        for (int k = 0; k < 8; k++) r[k] = a[k];
-        uint64_t i = 8;
-        for (; i < n - (n % 8); i += 8)
-            for (int k = 0; k < 8; k++) r[k] += a[i + k];
-        float res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
-        for (; i < n; i++) res += a[i];
-        return res;
-    }
-    uint64_t n2 = n / 2;
-    n2 -= n2 % 8;
-    return numpy_pairwise_sum(a, n2) + numpy_pairwise_sum(a + n2, n - n2);
-}
-
-// Run fn(c) for every curve, on several host threads when the batch holds
-// more than 2^20 points (curves interleaved across the threads).
-template <class F>
-void for_each_curve(uint64_t n_curves, uint64_t total_points, F& fn) {
-    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    const unsigned nthr = total_points > (1u << 20) ? hw : 1u;
-    if (nthr == 1) {
-        for (uint64_t c = 0; c < n_curves; c++) fn(c);
-        return;
-    }
-    std::vector<std::thread> th;
-    for (unsigned w = 0; w < nthr; w++)
-        th.emplace_back([&, w] {
-            for (uint64_t c = w; c < n_curves; c += nthr) fn(c);
-        });
-    for (auto& t : th) t.join();
-}
-
 }  // namespace
 
 size_t pfk::fold_smem(const FoldConfig& c, uint32_t n_phase, uint32_t n_mag) {
@@ -1498,52 +1563,7 @@ int pf_normalize_mags(const float* const* mags, const uint64_t* lengths, uint64_
         if (!mags[c] || !out[c]) return PF_EINVAL;
         total += lengths[c];
     }
-    // Per curve: numpy's float32 min / max (NaN propagates), then
-    // ((m - lo) / (hi - lo)) * 0.999f + 5e-4f in single precision, one
-    // rounding per operation, as numpy evaluates the same expression.
-    auto one = [&](uint64_t c) {
-        const float* m = mags[c];
-        const uint64_t n = lengths[c];
-        float lo = m[0], hi = m[0];
-        bool nan = std::isnan(m[0]);
-        uint64_t i = 1;
-        if (n >= 16) {
-            // Eight interleaved running minima / maxima, which the compiler
-            // turns into SIMD min / max.  Without NaN the result is the exact
-            // minimum and maximum whatever the order; only the sign of a
-            // zero extreme may differ, and lo, hi enter the output solely
-            // through m - lo and hi - lo, whose values it does not change.
-            float l[8], h[8];
-            int bad[8];
-            for (int k = 0; k < 8; k++) {
-                l[k] = h[k] = m[k];
-                bad[k] = 0;
-            }
-            for (i = 0; i + 8 <= n; i += 8)
-                for (int k = 0; k < 8; k++) {
-                    const float v = m[i + k];
-                    bad[k] |= (v != v);
-                    l[k] = v < l[k] ? v : l[k];
-                    h[k] = v > h[k] ? v : h[k];
-                }
-            for (int k = 0; k < 8; k++) {
-                nan |= bad[k] != 0;
-                lo = l[k] < lo ? l[k] : lo;
-                hi = h[k] > hi ? h[k] : hi;
-            }
-        }
-        for (; i < n; i++) {
-            const float v = m[i];
-            nan |= std::isnan(v);
-            lo = v < lo ? v : lo;
-            hi = v > hi ? v : hi;
-        }
-        if (nan) lo = hi = std::numeric_limits<float>::quiet_NaN();
-        // This unit is built with -ffp-contract=off: no fused multiply-add.
-        const float range = hi - lo;
-        float* o = out[c];
-        for (uint64_t i = 0; i < n; i++) o[i] = ((m[i] - lo) / range) * 0.999f + 5e-4f;
-    };
+    auto one = [&](uint64_t c) { normalize_curve(mags[c], lengths[c], out[c]); };
     for_each_curve(n_curves, total, one);
     return PF_OK;
 }
@@ -1557,15 +1577,7 @@ int pf_center_mags(const float* const* mags, const uint64_t* lengths, uint64_t n
         if (lengths[c] == 0 || !mags[c] || !out[c]) return PF_EINVAL;
         total += lengths[c];
     }
-    // np.mean of a float32 array: the pairwise float32 sum divided by the
-    // length in float32; then m - mean, one rounding per point.
-    auto one = [&](uint64_t c) {
-        const float* m = mags[c];
-        const uint64_t n = lengths[c];
-        const float mean = numpy_pairwise_sum(m, n) / (float)n;
-        float* o = out[c];
-        for (uint64_t i = 0; i < n; i++) o[i] = m[i] - mean;
-    };
+    auto one = [&](uint64_t c) { center_curve(mags[c], lengths[c], out[c]); };
     for_each_curve(n_curves, total, one);
     return PF_OK;
 }

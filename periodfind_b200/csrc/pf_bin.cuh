@@ -100,7 +100,12 @@ __device__ __forceinline__ float aov_finish(double sbx, const CurveDesc& cd, uin
 // (the two 16-bit halves of a word).
 template <bool CNT16>
 __device__ __forceinline__ float ce_stat_fast(uint32_t tbase, uint32_t nP, uint32_t W,
-                                              uint32_t block, uint32_t n) {
+                                              uint32_t block, uint32_t n, uint32_t tab) {
+    // Curves shorter than the table read c log2 c from it (the same values).
+    const bool use_tab = n < kXlxTable;
+    auto xlx = [&](uint32_t c) -> float {
+        return use_tab ? __uint_as_float(lds_u32(tab + c * 4u)) : ce_xlx(c);
+    };
     float acc = 0.0f;
     for (uint32_t j = 0; j < nP; j++) {
         uint32_t col = 0;
@@ -111,26 +116,26 @@ __device__ __forceinline__ float ce_stat_fast(uint32_t tbase, uint32_t nP, uint3
                 // Both 16-bit halves summed at once: each half's column
                 // total is at most n < 2^16, so no carry crosses halves.
                 col += wv;
-                row = __fadd_rn(row, __fadd_rn(ce_xlx(wv & 0xFFFFu), ce_xlx(wv >> 16)));
+                row = __fadd_rn(row, __fadd_rn(xlx(wv & 0xFFFFu), xlx(wv >> 16)));
             } else {
                 col += wv;
-                row = __fadd_rn(row, ce_xlx(wv));
+                row = __fadd_rn(row, xlx(wv));
             }
         }
         if constexpr (CNT16) col = (col & 0xFFFFu) + (col >> 16);
-        acc = __fadd_rn(acc, __fsub_rn(ce_xlx(col), row));
+        acc = __fadd_rn(acc, __fsub_rn(xlx(col), row));
     }
     return ce_finish(acc, n);
 }
 
 // The chosen form's AOV sum_b X_b^2 / c_b over the fixed-point bin sums X_b
-// (empty bins have X_b = 0 and contribute nothing).
+// (empty bins have X_b = 0 and contribute nothing).  Counters [bin][count,
+// sum][thread].
 __device__ __forceinline__ double aov_sbx_fast(uint32_t tbase, uint32_t nP, uint32_t block) {
     double sbx = 0.0;
-    const uint32_t sum_off = nP * block * 4u;
     for (uint32_t b = 0; b < nP; b++) {
-        const uint32_t c = lds_u32(tbase + b * block * 4u);
-        const double Xd = (double)lds_u32(tbase + sum_off + b * block * 4u);
+        const uint32_t c = lds_u32(tbase + 2u * b * block * 4u);
+        const double Xd = (double)lds_u32(tbase + (2u * b + 1u) * block * 4u);
         sbx = __fma_rn(__dmul_rn(Xd, Xd), __drcp_rn((double)max(c, 1u)), sbx);
     }
     return sbx;
@@ -161,12 +166,13 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
     const uint32_t nP = p.n_phase, nM = p.n_mag;
 
     // Counter layout: CE  [nP rows][W words][BLOCK] u32, W = nM or ceil(nM/2)
-    //                 AOV [2][nP][BLOCK] u32 (count, fixed-point sum)
+    //                 AOV [nP][2][BLOCK] u32 (count, fixed-point sum): a bin's
+    //                 sum lies a constant BLOCK words after its count, so the
+    //                 second reduction takes an immediate address offset.
     const uint32_t W = (ALGO == ALGO_CE) ? (CNT16 ? (nM + 1) / 2 : nM) : 1;
     const uint32_t row_stride = W * BLOCK * 4;  // bytes per phase row
     const uint32_t slots = (ALGO == ALGO_CE) ? nP * W : 2 * nP;
     const uint32_t tbase = cnt_base + tid * 4;
-    const uint32_t sum_off = nP * BLOCK * 4;  // AOV: sums after counts
 
     // The item covers ROUNDS x BLOCK periods; thread tid takes period
     // p0 + r * BLOCK + tid in round r.  Range guard for y = q * n * 2^20 over
@@ -287,9 +293,9 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
             if constexpr (ALGO == ALGO_CE) {
                 red_shared_u32(row * row_stride + pt.a + tbase, pt.b * sign);
             } else {
-                const uint32_t a0 = row * (BLOCK * 4) + tbase;
+                const uint32_t a0 = row * (2 * BLOCK * 4) + tbase;
                 red_shared_u32(a0, sign);
-                red_shared_u32(a0 + sum_off, pt.a * sign);
+                red_shared_u32(a0 + BLOCK * 4, pt.a * sign);
             }
         };
 
@@ -364,7 +370,8 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
     uint32_t* cnt32 = reinterpret_cast<uint32_t*>(cnt_raw);
 
     if constexpr (ALGO == ALGO_CE && !REF_STATS) {
-        p.out[out_idx] = ce_stat_fast<CNT16>(tbase, nP, W, BLOCK, n);
+        const uint32_t tab = cnt_base + slots * BLOCK * 4u;
+        p.out[out_idx] = ce_stat_fast<CNT16>(tbase, nP, W, BLOCK, n, tab);
     } else if constexpr (ALGO == ALGO_AOV && !REF_STATS) {
         p.out[out_idx] = aov_finish(aov_sbx_fast(tbase, nP, BLOCK), cd, n, nP);
     } else if constexpr (ALGO == ALGO_CE) {
@@ -402,16 +409,16 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
         }
         p.out[out_idx] = ce;
     } else {
-        const uint32_t* sums = cnt32 + nP * BLOCK;
+        const uint32_t* sums = cnt32 + BLOCK;
         if (p.bins) {
             uint32_t* o = p.bins + out_idx * (size_t)nP;
-            for (uint32_t b = 0; b < nP; b++) o[b] = cnt32[b * BLOCK + tid];
+            for (uint32_t b = 0; b < nP; b++) o[b] = cnt32[2 * b * BLOCK + tid];
         }
         const double xbar = cd.fix_sumx / (double)n;
         double s1 = 0.0, sbx = 0.0;
         for (uint32_t b = 0; b < nP; b++) {
-            const uint32_t c = cnt32[b * BLOCK + tid];
-            const uint32_t X = sums[b * BLOCK + tid];
+            const uint32_t c = cnt32[2 * b * BLOCK + tid];
+            const uint32_t X = sums[2 * b * BLOCK + tid];
             if (c != 0u) {
                 const double nb = (double)c;
                 const double Xd = (double)X;
@@ -439,6 +446,15 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
 template <int ALGO, bool CNT16, int BLOCK, bool REF_STATS, bool PERSIST, int ROUNDS>
 __global__ void __launch_bounds__(BLOCK, queue_min_blocks<ALGO, BLOCK>())
     bin_kernel(const FoldParams p) {
+    if constexpr (ALGO == ALGO_CE && !REF_STATS) {
+        // The c log2 c table after the counters, once per CTA.
+        extern __shared__ __align__(16) unsigned char smem[];
+        const uint32_t W = CNT16 ? (p.n_mag + 1) / 2 : p.n_mag;
+        float* tab = reinterpret_cast<float*>(smem + kBinTile * sizeof(BinPoint) +
+                                              (size_t)p.n_phase * W * BLOCK * 4u);
+        for (uint32_t c = threadIdx.x; c < kXlxTable; c += BLOCK) tab[c] = ce_xlx(c);
+        __syncthreads();
+    }
     if constexpr (PERSIST) {
         for_each_queued_item<BLOCK * ROUNDS>(p, [&](const WorkItem& w, uint32_t k) {
             bin_item<ALGO, CNT16, BLOCK, REF_STATS, ROUNDS>(p, w, k);

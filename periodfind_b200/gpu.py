@@ -63,6 +63,20 @@ def _grid(a, name):
     return np.ascontiguousarray(a)
 
 
+def _fused_prep(mags, center, normalize):
+    """(magnitudes to pass, extra mode bits).  For float32 1-D curves that
+    are all non-empty the native packing prepares the magnitudes itself
+    (PF_HOST_CENTER / PF_HOST_NORMALIZE: numpy's values, no separate pass
+    or copy); anything else is prepared here as the reference does.  The
+    centre / normalise conflict is settled by the caller."""
+    if not (center or normalize):
+        return mags, 0
+    if all(isinstance(m, np.ndarray) and m.ndim == 1 and m.size and m.dtype == np.float32
+           for m in mags):
+        return mags, (nat.PF_HOST_CENTER if center else nat.PF_HOST_NORMALIZE)
+    return prepare_magnitudes(mags, center, normalize), 0
+
+
 def unravel_peaks(peak_indices, peak_values, periods, period_dts, n_peaks):
     """Flat peak indices -> list (per curve) of lists of Statistics, stopping
     at the first -1 (periodfind/cpu/__init__.py:46-70)."""
@@ -93,19 +107,19 @@ class _Periodogram:
                                   getattr(self, "_reference_stats", False))
 
     # -- native calls, implemented per algorithm
-    def _native_pgram(self, ctx, b, periods, pdts, out):
+    def _native_pgram(self, ctx, b, periods, pdts, out, extra=0):
         raise NotImplementedError
 
     def _native_peaks(self, ctx, b, periods, pdts, n_peaks, min_distance, idx, val, extra=0):
         raise NotImplementedError
 
-    def periodograms(self, times, mags, periods, period_dts):
+    def periodograms(self, times, mags, periods, period_dts, _extra=0):
         """Raw [n_curves, n_periods, n_pdts] float32 array for prepared mags."""
         ctx = nat.default_context(self.device)
         b = nat.CurveBatch(times, mags)
         out = np.empty((b.n, len(periods), len(period_dts)), dtype=np.float32)
         with ctx.lock:
-            ctx.check(self._native_pgram(ctx, b, periods, period_dts, out))
+            ctx.check(self._native_pgram(ctx, b, periods, period_dts, out, _extra))
         return out
 
     def bin_counts(self, times, mags, periods, period_dts):
@@ -268,13 +282,15 @@ class _Periodogram:
             return unravel_peaks(idx, val, periods, period_dts, n_peaks)
 
         def issue(ctx, a, e, idx, val):
-            b = nat.CurveBatch(times[a:e], prepare_magnitudes(mags[a:e], center, normalize))
+            m, extra = _fused_prep(mags[a:e], center, normalize)
+            b = nat.CurveBatch(times[a:e], m)
             return self._native_peaks(ctx, b, periods, period_dts, idx.shape[1],
-                                      int(min_distance), idx, val, nat.PF_ASYNC)
+                                      int(min_distance), idx, val, nat.PF_ASYNC | extra)
 
         return self._chunked_peaks(len(times), periods, period_dts, n_peaks, issue)
 
-    def _stats_on_device(self, times, mags, periods, period_dts, n_stats, significance_type):
+    def _stats_on_device(self, times, mags, periods, period_dts, n_stats, significance_type,
+                         extra=0):
         """The 'stats' output with the statistics computed on the device
         (identical to numpy's); None where the device path does not apply."""
         ctx = nat.default_context(self.device)
@@ -283,7 +299,7 @@ class _Periodogram:
         idx = np.empty((b.n, n_stats), dtype=np.int64)
         val = np.empty((b.n, n_stats), dtype=np.float32)
         with ctx.lock:
-            rc = self._native_stats(ctx, b, periods, period_dts, n_stats, st, idx, val)
+            rc = self._native_stats(ctx, b, periods, period_dts, n_stats, st, idx, val, extra)
             if rc == nat.PF_EUNSUPPORTED:
                 return None
             ctx.check(rc)
@@ -319,16 +335,19 @@ class _Periodogram:
                 normalize = False
             return self._peaks_overlapped(times, mags, periods, period_dts, int(n_peaks),
                                           min_distance, center, normalize)
-        mags_use = prepare_magnitudes(mags, center, normalize)
+        if center and normalize:  # the reference's conflict warning, then centre
+            prepare_magnitudes([], center, normalize)
+            normalize = False
+        mags_use, extra = _fused_prep(mags, center, normalize)
 
         if (output == "stats" and 1 <= int(n_stats) < len(periods) * len(period_dts)
                 and (not self._use_max or len(period_dts) == 1)):
             res = self._stats_on_device(times, mags_use, periods, period_dts, int(n_stats),
-                                        significance_type)
+                                        significance_type, extra)
             if res is not None:
                 return res
 
-        data = self.periodograms(times, mags_use, periods, period_dts)
+        data = self.periodograms(times, mags_use, periods, period_dts, extra)
         with gc_paused():
             if output == "stats":
                 return [Statistics.statistics_from_data(
@@ -382,17 +401,18 @@ class ConditionalEntropy(_Periodogram):
         return (nat.PF_ALGO_CE, self.n_phase, self.n_mag, self.phase_bin_extent,
                 self.mag_bin_extent)
 
-    def _native_pgram(self, ctx, b, periods, pdts, out):
+    def _native_pgram(self, ctx, b, periods, pdts, out, extra=0):
         return ctx.lib.pf_ce(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                              nat.ptr(pdts), len(pdts), self.n_phase, self.n_mag,
-                             self.phase_bin_extent, self.mag_bin_extent, self._flags,
+                             self.phase_bin_extent, self.mag_bin_extent, self._flags | extra,
                              nat.ptr(out))
 
-    def _native_stats(self, ctx, b, periods, pdts, n_top, st, idx, val):
+    def _native_stats(self, ctx, b, periods, pdts, n_top, st, idx, val, extra=0):
         return ctx.lib.pf_ce_stats(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                                    nat.ptr(pdts), len(pdts), self.n_phase, self.n_mag,
                                    self.phase_bin_extent, self.mag_bin_extent, n_top,
-                                   self._flags, nat.ptr(st), nat.ptr(idx), nat.ptr(val))
+                                   self._flags | extra, nat.ptr(st), nat.ptr(idx),
+                                   nat.ptr(val))
 
     def _native_dev(self, ctx, d_t, d_m, off, n, d_p, n_per, d_d, n_pdt, d_out, stream):
         return ctx.lib.pf_ce_dev(ctx.handle, d_t, d_m, off.ctypes.data, n, d_p, n_per, d_d,
@@ -423,16 +443,16 @@ class AOV(_Periodogram):
     def _bin_args(self):
         return (nat.PF_ALGO_AOV, self.n_phase, 1, self.phase_bin_extent, 1)
 
-    def _native_pgram(self, ctx, b, periods, pdts, out):
+    def _native_pgram(self, ctx, b, periods, pdts, out, extra=0):
         return ctx.lib.pf_aov(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                               nat.ptr(pdts), len(pdts), self.n_phase, self.phase_bin_extent,
-                              self._flags, nat.ptr(out))
+                              self._flags | extra, nat.ptr(out))
 
-    def _native_stats(self, ctx, b, periods, pdts, n_top, st, idx, val):
+    def _native_stats(self, ctx, b, periods, pdts, n_top, st, idx, val, extra=0):
         return ctx.lib.pf_aov_stats(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
                                     nat.ptr(pdts), len(pdts), self.n_phase,
-                                    self.phase_bin_extent, n_top, self._flags, nat.ptr(st),
-                                    nat.ptr(idx), nat.ptr(val))
+                                    self.phase_bin_extent, n_top, self._flags | extra,
+                                    nat.ptr(st), nat.ptr(idx), nat.ptr(val))
 
     def _native_dev(self, ctx, d_t, d_m, off, n, d_p, n_per, d_d, n_pdt, d_out, stream):
         return ctx.lib.pf_aov_dev(ctx.handle, d_t, d_m, off.ctypes.data, n, d_p, n_per, d_d,
@@ -462,14 +482,14 @@ class LombScargle(_Periodogram):
         self._fold = fold
         super().__init__(mode=mode, semantics=semantics, device=device)
 
-    def _native_pgram(self, ctx, b, periods, pdts, out):
+    def _native_pgram(self, ctx, b, periods, pdts, out, extra=0):
         return ctx.lib.pf_ls(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
-                             nat.ptr(pdts), len(pdts), self._flags, nat.ptr(out))
+                             nat.ptr(pdts), len(pdts), self._flags | extra, nat.ptr(out))
 
-    def _native_stats(self, ctx, b, periods, pdts, n_top, st, idx, val):
+    def _native_stats(self, ctx, b, periods, pdts, n_top, st, idx, val, extra=0):
         return ctx.lib.pf_ls_stats(ctx.handle, *b.args(), nat.ptr(periods), len(periods),
-                                   nat.ptr(pdts), len(pdts), n_top, self._flags, nat.ptr(st),
-                                   nat.ptr(idx), nat.ptr(val))
+                                   nat.ptr(pdts), len(pdts), n_top, self._flags | extra,
+                                   nat.ptr(st), nat.ptr(idx), nat.ptr(val))
 
     def _native_dev(self, ctx, d_t, d_m, off, n, d_p, n_per, d_d, n_pdt, d_out, stream):
         return ctx.lib.pf_ls_dev(ctx.handle, d_t, d_m, off.ctypes.data, n, d_p, n_per, d_d,

@@ -455,3 +455,31 @@ def test_ce_magnitudes_outside_unit_interval_run_memory_safely(gpu):
     cen = (0.3 * (m - np.mean(m))).astype(np.float32)
     got = gpu.ConditionalEntropy(semantics="cpu").periodograms([t], [cen], P, Z)
     np.testing.assert_allclose(got, O.ce([t], [cen], P, Z), rtol=2e-6)
+
+
+def test_preparation_fused_into_packing_is_bit_exact():
+    """PF_HOST_NORMALIZE / PF_HOST_CENTER prepare the magnitudes while the
+    library packs them: the periodograms equal those of magnitudes prepared
+    by numpy first, bit for bit (CE normalised, LS centred, AOV centred),
+    with a constant and a one-point curve among them."""
+    from periodfind_b200 import _native as nat
+    from periodfind_b200 import gpu
+
+    rng = np.random.default_rng(61)
+    ts, ms = [], []
+    for n in (1, 7, 8, 9, 129, 300, 1025, 4097):
+        t = lc.uniform_times(rng, n, 200.0)
+        ts.append(t)
+        ms.append(lc.noisy(rng, lc.sinusoid(t, float(rng.uniform(1, 4)), 0.3, 0.0, 15.0), 0.05))
+    ms[3][:] = 7.5
+    P = np.linspace(0.5, 6.0, 257).astype(np.float32)
+    D = np.array([0.0, 1e-5], np.float32)
+    for obj, center in ((gpu.ConditionalEntropy(10, 10), False), (gpu.LombScargle(), True),
+                        (gpu.AOV(15), True)):
+        with np.errstate(all="ignore"):
+            want = obj.periodograms(ts, [np.asarray(m) for m in
+                                         (lc.center(x) if center else lc.normalize(x)
+                                          for x in ms)], P, D)
+            got = obj.periodograms(ts, ms, P, D, _extra=nat.PF_HOST_CENTER if center
+                                   else nat.PF_HOST_NORMALIZE)
+        np.testing.assert_array_equal(got, want)
