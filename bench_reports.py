@@ -11,6 +11,7 @@ timed region carries its own nvidia-smi clock record ("clocks").
              50000 frequencies)
   fpw / bls  FPW(10) / BLS(50, 0.01, 0.5) on the 1000 x 4096 batch
   device     device-resident CE + AOV periodograms against the host path
+  profile    a short run whose kernels ncu captures (NVTX range pf_profile)
 """
 
 from __future__ import annotations
@@ -452,7 +453,59 @@ def precision_arm(args):
     _emit(out, clocks)
 
 
-ARMS = {"batch": batch_arm, "small": small_arm, "lsgrad": lsgrad_arm,
+def profile_arm(args):
+    """A short run for ncu captures: the mixed ragged batch (--curves,
+    default 10000), one tuned direct call per computation outside the
+    capture, then inside the NVTX range "pf_profile" one chosen call each
+    of CE, AOV and LS over the 20000 log periods, and LS on the uniform
+    frequency grid of 20000 frequencies in [0.002, 20] / d with the sincos
+    form and with the recurrence (4 or 5 class launches each).  Prints the
+    kernel times (the library's CUDA events)."""
+    import json
+
+    import torch
+
+    from bench import RaggedStep, ragged_grid
+    from periodfind_b200 import _native as nat
+
+    torch.cuda.set_device(0)
+    n_curves = args.curves or 10000
+    t, m, off = lc.ragged_batch(n_curves, SEED + 5)
+    periods, pdts = ragged_grid()
+    step = RaggedStep(t, m, off, periods, pdts, torch, 0)
+    c, lib = step.ctx, step.ctx.lib
+    f_min, n_freq = 0.002, 20000
+    df = (20.0 - f_min) / (n_freq - 1)
+    fg = torch.empty((step.n, n_freq), dtype=torch.float32, device="cuda")
+
+    def fgrid(flags):
+        c.check(lib.pf_ls_fgrid_dev(c.handle, step.d_t.data_ptr(), step.mags["ls"].data_ptr(),
+                                    step.off.ctypes.data, step.n, f_min, df, n_freq, flags,
+                                    fg.data_ptr(), step.s))
+
+    runs = [(a, lambda a=a: step.direct(a, nat.PF_MODE_CHOSEN, peaks=False))
+            for a in ("ce", "aov", "ls")]
+    runs += [("ls_fgrid_sincos", lambda: fgrid(nat.PF_MODE_CHOSEN | nat.PF_TRIG_SINCOS)),
+             ("ls_fgrid_recurrence",
+              lambda: fgrid(nat.PF_MODE_CHOSEN | nat.PF_TRIG_RECURRENCE))]
+    for _, fn in runs:  # tuning and warm-up, outside the captured range
+        fn()
+    torch.cuda.synchronize()
+    out = {"workload": f"ragged batch sample: {n_curves} curves ({int(off[-1])} points), "
+                       f"{len(periods)} log periods / {n_freq} uniform frequencies",
+           "kernel_ms": {}}
+    torch.cuda.nvtx.range_push("pf_profile")
+    for name, fn in runs:
+        fn()
+        torch.cuda.synchronize()
+        out["kernel_ms"][name] = c.last_kernel_ms
+    torch.cuda.nvtx.range_pop()
+    out["tuning"] = c.tuning_report().strip().splitlines()
+    step.close()
+    print(json.dumps(out), flush=True)
+
+
+ARMS = {"batch": batch_arm, "profile": profile_arm, "small": small_arm, "lsgrad": lsgrad_arm,
         "precision": precision_arm, "fpw": fpw_arm, "bls": lambda a: fpw_arm(a, bls=True),
         "device": device_arm}
 

@@ -100,12 +100,8 @@ __device__ __forceinline__ float aov_finish(double sbx, const CurveDesc& cd, uin
 // (the two 16-bit halves of a word).
 template <bool CNT16>
 __device__ __forceinline__ float ce_stat_fast(uint32_t tbase, uint32_t nP, uint32_t W,
-                                              uint32_t block, uint32_t n, uint32_t tab) {
-    // Curves shorter than the table read c log2 c from it (the same values).
-    const bool use_tab = n < kXlxTable;
-    auto xlx = [&](uint32_t c) -> float {
-        return use_tab ? __uint_as_float(lds_u32(tab + c * 4u)) : ce_xlx(c);
-    };
+                                              uint32_t block, uint32_t n) {
+    auto xlx = [](uint32_t c) -> float { return ce_xlx(c); };
     float acc = 0.0f;
     for (uint32_t j = 0; j < nP; j++) {
         uint32_t col = 0;
@@ -370,8 +366,7 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
     uint32_t* cnt32 = reinterpret_cast<uint32_t*>(cnt_raw);
 
     if constexpr (ALGO == ALGO_CE && !REF_STATS) {
-        const uint32_t tab = cnt_base + slots * BLOCK * 4u;
-        p.out[out_idx] = ce_stat_fast<CNT16>(tbase, nP, W, BLOCK, n, tab);
+        p.out[out_idx] = ce_stat_fast<CNT16>(tbase, nP, W, BLOCK, n);
     } else if constexpr (ALGO == ALGO_AOV && !REF_STATS) {
         p.out[out_idx] = aov_finish(aov_sbx_fast(tbase, nP, BLOCK), cd, n, nP);
     } else if constexpr (ALGO == ALGO_CE) {
@@ -446,15 +441,6 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
 template <int ALGO, bool CNT16, int BLOCK, bool REF_STATS, bool PERSIST, int ROUNDS>
 __global__ void __launch_bounds__(BLOCK, queue_min_blocks<ALGO, BLOCK>())
     bin_kernel(const FoldParams p) {
-    if constexpr (ALGO == ALGO_CE && !REF_STATS) {
-        // The c log2 c table after the counters, once per CTA.
-        extern __shared__ __align__(16) unsigned char smem[];
-        const uint32_t W = CNT16 ? (p.n_mag + 1) / 2 : p.n_mag;
-        float* tab = reinterpret_cast<float*>(smem + kBinTile * sizeof(BinPoint) +
-                                              (size_t)p.n_phase * W * BLOCK * 4u);
-        for (uint32_t c = threadIdx.x; c < kXlxTable; c += BLOCK) tab[c] = ce_xlx(c);
-        __syncthreads();
-    }
     if constexpr (PERSIST) {
         for_each_queued_item<BLOCK * ROUNDS>(p, [&](const WorkItem& w, uint32_t k) {
             bin_item<ALGO, CNT16, BLOCK, REF_STATS, ROUNDS>(p, w, k);

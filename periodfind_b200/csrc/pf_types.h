@@ -88,18 +88,12 @@ struct FoldParams {
 };
 
 // Shared-memory bytes of the chosen bin kernel (pf_bin.cuh).
-// CE: a table of c log2 c for counts c < kXlxTable after the counters,
-// which the statistic of curves shorter than that reads instead of a log per
-// bin (512 entries keep 4 CTAs of 256 threads per SM at 10 x 10 bins).
-constexpr uint32_t kXlxTable = 512;
-
 inline size_t bin_smem_bytes(int algo, bool cnt16, int block, uint32_t n_phase,
                              uint32_t n_mag) {
     size_t bytes = (size_t)kBinTile * 16;  // {double t; u32 a, b} per point
     if (algo == ALGO_CE) {
         const size_t w = cnt16 ? (n_mag + 1) / 2 : n_mag;
         bytes += (size_t)n_phase * w * block * 4;
-        bytes += (size_t)kXlxTable * 4;
     } else {
         bytes += (size_t)2 * n_phase * block * 4;
     }
