@@ -238,7 +238,7 @@ class RaggedStep:
     """The ragged batch resident on the device, its three batch plans
     (chosen) and the plain form's direct calls, on the current stream."""
 
-    def __init__(self, t, m, off, periods, pdts, torch, device):
+    def __init__(self, t, m, off, periods, pdts, torch, device, plans=True):
         from periodfind_b200 import _native as nat
         from periodfind_b200.plan import BatchPlan
 
@@ -265,7 +265,7 @@ class RaggedStep:
         self.s = self.stream.cuda_stream
         self.prepare()
         self.plans = {}
-        for k, algo in enumerate(ALGOS):
+        for k, algo in enumerate(ALGOS if plans else ()):
             self.plans[algo] = BatchPlan(
                 algo, self.d_t, self.mags[algo], self.off, self.d_p, self.d_d, self.pg,
                 n_phase=10 if algo == "ce" else 15, n_mag=10, flags=nat.PF_MODE_CHOSEN,

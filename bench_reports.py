@@ -472,7 +472,7 @@ def profile_arm(args):
     n_curves = args.curves or 10000
     t, m, off = lc.ragged_batch(n_curves, SEED + 5)
     periods, pdts = ragged_grid()
-    step = RaggedStep(t, m, off, periods, pdts, torch, 0)
+    step = RaggedStep(t, m, off, periods, pdts, torch, 0, plans=False)
     c, lib = step.ctx, step.ctx.lib
     f_min, n_freq = 0.002, 20000
     df = (20.0 - f_min) / (n_freq - 1)
