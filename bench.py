@@ -224,11 +224,11 @@ ROOFLINE = {
            "pipe": "mufu_sin+cos", "ops": 2.0, "views": {}},
 }
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the class
-# kernels of one algorithm over the whole ragged batch, from one ncu capture
-# of a curve sample of the batch scaled by its evaluations (the traffic is
-# the curve points and the periodogram, both proportional).  None where no
-# capture has been made.
-RAGGED_TRAFFIC = {"ce": None, "aov": None, "ls": None}
+# kernels of one call over the whole ragged batch: one ncu capture of a
+# 3000-curve sample of the batch (bench.py --workload profile --curves 3000),
+# scaled by its evaluations (x 32.64; the traffic is the curve points read
+# and the periodogram written, both proportional).
+RAGGED_TRAFFIC = {"ce": 3.82e9, "aov": 3.90e9, "ls": 3.62e9}
 
 
 # ------------------------------------------------------------ ragged step
