@@ -924,13 +924,13 @@ def main():
     ap.add_argument("--no-calc", action="store_true", help="skip the Python calc() path")
     ap.add_argument("--workload", default="ragged",
                     choices=["ragged", "batch", "small", "lsgrad", "precision", "fpw", "bls",
-                             "device", "profile"],
+                             "device", "profile", "profile_batch"],
                     help="'ragged' (default): the mixed ragged batch; separate reports on 1 "
                          "GPU: 'batch' CE + AOV on 1000 x 4096, 'small' CE stats on 100 x "
                          "1024, 'lsgrad' LS derivatives and Newton refinement, 'precision' LS "
                          "folds on the precision-study batch, 'fpw' / 'bls' on the 1000 x 4096 "
-                         "batch, 'device' device-resident periodograms, 'profile' a short run "
-                         "for ncu captures")
+                         "batch, 'device' device-resident periodograms, 'profile' / "
+                         "'profile_batch' short runs for ncu captures")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

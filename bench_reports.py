@@ -11,7 +11,10 @@ timed region carries its own nvidia-smi clock record ("clocks").
              50000 frequencies)
   fpw / bls  FPW(10) / BLS(50, 0.01, 0.5) on the 1000 x 4096 batch
   device     device-resident CE + AOV periodograms against the host path
-  profile    a short run whose kernels ncu captures (NVTX range pf_profile)
+  profile    a short run whose kernels ncu captures (NVTX range pf_profile):
+             chosen CE / AOV / LS on a sample of the ragged batch
+  profile_batch  the same for chosen CE and AOV on the 1000 x 4096 batch
+             shape (default 10 curves)
 """
 
 from __future__ import annotations
@@ -505,7 +508,49 @@ def profile_arm(args):
     print(json.dumps(out), flush=True)
 
 
-ARMS = {"batch": batch_arm, "profile": profile_arm, "small": small_arm, "lsgrad": lsgrad_arm,
+def profile_batch_arm(args):
+    """A short run for ncu captures on the 1000 x 4096 batch's shape
+    (--curves, default 10): one tuned chosen call of CE and of AOV outside
+    the capture, then inside the NVTX range "pf_profile" one chosen call of
+    each (one class launch each: every curve has 4096 points).  Prints the
+    kernel times (the library's CUDA events)."""
+    import json
+
+    import torch
+
+    from periodfind_b200 import _native as nat
+
+    torch.cuda.set_device(0)
+    ts, ms, periods, pdts = make_workload(args.curves or 10)
+    st = BatchStep(ts, ms, periods, pdts, nat.PF_MODE_CHOSEN, torch, 0)
+    c, lib, h = st.ctx, st.ctx.lib, st.ctx.handle
+
+    def common(m):
+        return (h, st.t.data_ptr(), m.data_ptr(), st.off.ctypes.data, st.n, st.P.data_ptr(),
+                st.np_, st.D.data_ptr(), st.nd)
+
+    runs = [("ce", lambda: c.check(lib.pf_ce_dev(*common(st.m_ce), 10, 10, 1, 1,
+                                                 nat.PF_MODE_CHOSEN, st.pg[0].data_ptr(),
+                                                 st.s))),
+            ("aov", lambda: c.check(lib.pf_aov_dev(*common(st.m_aov), 15, 1, nat.PF_MODE_CHOSEN,
+                                                   st.pg[1].data_ptr(), st.s)))]
+    for _, fn in runs:  # tuning and warm-up, outside the captured range
+        fn()
+    torch.cuda.synchronize()
+    out = {"workload": f"{st.n} curves x {N_POINTS} points x {N_PERIODS} log periods x "
+                       f"pdts {list(PDTS)}", "kernel_ms": {}}
+    torch.cuda.nvtx.range_push("pf_profile")
+    for name, fn in runs:
+        fn()
+        torch.cuda.synchronize()
+        out["kernel_ms"][name] = c.last_kernel_ms
+    torch.cuda.nvtx.range_pop()
+    out["tuning"] = c.tuning_report().strip().splitlines()
+    c.close()
+    print(json.dumps(out), flush=True)
+
+
+ARMS = {"batch": batch_arm, "profile": profile_arm, "profile_batch": profile_batch_arm, "small": small_arm, "lsgrad": lsgrad_arm,
         "precision": precision_arm, "fpw": fpw_arm, "bls": lambda a: fpw_arm(a, bls=True),
         "device": device_arm}
 

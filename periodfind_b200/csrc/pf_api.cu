@@ -70,7 +70,7 @@ struct pf_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // around the fold kernel
     cudaEvent_t ev_staged = nullptr;            // staging block copied out
-    cudaEvent_t ev_done = nullptr;              // last device-pointer call done
+    cudaEvent_t ev_done = nullptr;              // the last call's work done
     bool staged_pending = false, done_recorded = false, timed_pending = false;
     std::string err;
     DevBuf d_in, d_aux32, d_aux64, d_out, d_pidx, d_pval, d_pack, d_misc, d_stamps, d_stat;
@@ -140,8 +140,27 @@ int cuda_fail(pf_ctx* ctx, cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
     } while (0)
 
+// Calls on a context share its device buffers, and may run on different
+// streams (host-pointer calls on the context's stream, device-pointer calls
+// on the caller's).  Each call orders its first use of the buffers after
+// the previous call's last (order_after_previous) and marks its own end
+// (mark_done), so a call never overwrites inputs, descriptors or queue
+// counters that an earlier call's kernels still read.
+int order_after_previous(pf_ctx* ctx, cudaStream_t s) {
+    if (ctx->done_recorded) PF_CUDA(cudaStreamWaitEvent(s, ctx->ev_done, 0), "stream wait");
+    return PF_OK;
+}
+
+int mark_done(pf_ctx* ctx, cudaStream_t s) {
+    PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
+    ctx->done_recorded = true;
+    return PF_OK;
+}
+
 int ensure_dev(pf_ctx* ctx, DevBuf& b, size_t bytes) {
     if (bytes <= b.cap) return PF_OK;
+    // The old block may still be read by the previous call's kernels.
+    if (b.p && ctx->done_recorded) cudaEventSynchronize(ctx->ev_done);
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.cap = 0;
@@ -1132,6 +1151,7 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
 
     cudaStream_t s = ctx->stream;
     char* db = (char*)ctx->d_in.p;
+    if ((rc = order_after_previous(ctx, s)) != PF_OK) return rc;
     {
         Stage stage_h2d("pf H2D");
         PF_CUDA(cudaMemcpyAsync(db, hb, L.bytes, cudaMemcpyHostToDevice, s), "H2D inputs");
@@ -1178,8 +1198,9 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
         if ((rc = copy_peaks_back(ctx, j, async, s)) != PF_OK) return rc;
         // PF_ASYNC: the call returns with its work queued.  The staging
         // block stays marked in use until the H2D copy above has finished.
-        if (async) return PF_OK;
+        if (async) return mark_done(ctx, s);
     }
+    if ((rc = mark_done(ctx, s)) != PF_OK) return rc;
     PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
     ctx->staged_pending = false;
     read_kernel_time(ctx);
@@ -1220,7 +1241,7 @@ int run_dev(pf_ctx* ctx, const Job& j, const float* d_times, const float* d_mags
 
     // Order this call after the previous one on this context (its buffers
     // are reused), whichever stream that one ran on.
-    if (ctx->done_recorded) PF_CUDA(cudaStreamWaitEvent(s, ctx->ev_done, 0), "stream wait");
+    if ((rc = order_after_previous(ctx, s)) != PF_OK) return rc;
     char* db = (char*)ctx->d_in.p;
     PF_CUDA(cudaMemcpyAsync(db, hb, L.bytes, cudaMemcpyHostToDevice, s), "H2D metadata");
     PF_CUDA(cudaEventRecord(ctx->ev_staged, s), "event");
@@ -1421,6 +1442,7 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
     memcpy(hb + o_pdt, pdts, n_pdt * 4);
     cudaStream_t s = ctx->stream;
     char* db = (char*)ctx->d_in.p;
+    if ((rc = order_after_previous(ctx, s)) != PF_OK) return rc;
     PF_CUDA(cudaMemcpyAsync(db, hb, bytes, cudaMemcpyHostToDevice, s), "H2D inputs");
     PF_CUDA(cudaEventRecord(ctx->ev_staged, s), "event");
     ctx->staged_pending = true;
@@ -1474,11 +1496,12 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
             ctx->launches++;
         }
         if ((rc = copy_peaks_back(ctx, j, async, s)) != PF_OK) return rc;
-        if (async) return PF_OK;
+        if (async) return mark_done(ctx, s);
     } else {
         PF_CUDA(cudaMemcpyAsync(out, p.out, out_bytes, cudaMemcpyDeviceToHost, s),
                 "D2H periodogram");
     }
+    if ((rc = mark_done(ctx, s)) != PF_OK) return rc;
     PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
     ctx->staged_pending = false;
     read_kernel_time(ctx);
@@ -2374,6 +2397,7 @@ int pf_find_peaks(pf_ctx* ctx, const float* data, uint64_t n_curves, uint64_t fl
     if ((rc = ensure_dev(ctx, ctx->d_pidx, pk * 8)) != PF_OK) return rc;
     if ((rc = ensure_dev(ctx, ctx->d_pval, pk * 4)) != PF_OK) return rc;
     cudaStream_t s = ctx->stream;
+    if ((rc = order_after_previous(ctx, s)) != PF_OK) return rc;
     PF_CUDA(cudaMemcpyAsync(ctx->d_out.p, data, in_bytes, cudaMemcpyHostToDevice, s), "H2D");
     PF_CUDA(launch_peaks((const float*)ctx->d_out.p, n_curves, flat_len, n_peaks, min_distance,
                          use_max, (int64_t*)ctx->d_pidx.p, (float*)ctx->d_pval.p, s),
@@ -2381,6 +2405,7 @@ int pf_find_peaks(pf_ctx* ctx, const float* data, uint64_t n_curves, uint64_t fl
     ctx->launches++;
     PF_CUDA(cudaMemcpyAsync(out_idx, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s), "D2H");
     PF_CUDA(cudaMemcpyAsync(out_val, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    if ((rc = mark_done(ctx, s)) != PF_OK) return rc;
     PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
     return PF_OK;
 }

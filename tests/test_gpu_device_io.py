@@ -109,6 +109,38 @@ def test_periodograms_device_equal_host_path(gpu, mode):
         np.testing.assert_array_equal(got.cpu().numpy(), want, err_msg=type(obj).__name__)
 
 
+def test_host_call_waits_for_device_call_on_one_context(gpu):
+    """A device-pointer call whose kernels are still running on the caller's
+    stream when a host-pointer call starts on the same context: the two
+    share the context's buffers (inputs, curve descriptors, queue counters),
+    so the host call is ordered after the device call, and both results
+    equal separate calls' bit for bit."""
+    import torch
+
+    ts, ms = _curves(seed=12, lengths=(3000,) * 48 + (40, 700))
+    t_flat, off = _csr(ts)
+    m_flat, _ = _csr(ms)
+    d_t = torch.from_numpy(t_flat).cuda()
+    d_m = torch.from_numpy(m_flat).cuda()
+    P = np.exp(np.linspace(np.log(0.1), np.log(80.0), 20000)).astype(np.float32)
+    D = np.array([0.0], np.float32)
+    small_t, small_m = _curves(seed=13, lengths=(9, 300, 1500))
+    Ps = P[:500].copy()
+    for obj in (gpu.ConditionalEntropy(), gpu.AOV(15), gpu.LombScargle()):
+        obj.periodograms_device(d_t, d_m, off, P, D)  # tuned, buffers sized
+        obj.periodograms(small_t, small_m, Ps, D)
+        torch.cuda.synchronize()
+        got_dev = obj.periodograms_device(d_t, d_m, off, P, D)
+        got_host = obj.periodograms(small_t, small_m, Ps, D)  # while got_dev runs
+        torch.cuda.synchronize()
+        want_dev = obj.periodograms_device(d_t, d_m, off, P, D)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(got_dev.cpu().numpy(), want_dev.cpu().numpy(),
+                                      err_msg=type(obj).__name__)
+        np.testing.assert_array_equal(got_host, obj.periodograms(small_t, small_m, Ps, D),
+                                      err_msg=type(obj).__name__)
+
+
 def test_periodograms_device_argument_checks(gpu):
     import torch
 
