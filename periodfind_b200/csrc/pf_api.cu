@@ -22,9 +22,13 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <functional>
 #include <limits>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -63,6 +67,91 @@ struct Stage {
     Stage& operator=(const Stage&) = delete;
 };
 
+// Host threads kept by a context for the packing of host-pointer calls:
+// run() hands the tasks of one job to the workers and the calling thread,
+// which take them in turn; idle workers wait on a condition variable.
+// Threads are created on first use (a thread start costs tens of
+// microseconds, more than packing a small batch).  A task ticket carries
+// the job number, so a worker that wakes after its job has finished takes
+// nothing from the next one, and the caller waits for its tasks, not for
+// every worker to wake.  One job at a time (a context is used by one host
+// thread at a time).
+class WorkerPool {
+  public:
+    WorkerPool() = default;
+    WorkerPool(const WorkerPool&) = delete;
+    WorkerPool& operator=(const WorkerPool&) = delete;
+    ~WorkerPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (std::thread& t : threads_) t.join();
+    }
+
+    // fn(k) for every k < n_tasks, on at most `width` threads (the caller
+    // included); returns when all tasks have finished.
+    void run(unsigned n_tasks, unsigned width, const std::function<void(unsigned)>& fn) {
+        width = std::min(width, n_tasks);
+        if (width <= 1) {
+            for (unsigned k = 0; k < n_tasks; k++) fn(k);
+            return;
+        }
+        while (threads_.size() + 1 < width) {
+            const uint32_t g = gen_;  // the new worker waits for the next job
+            threads_.emplace_back([this, g] { work(g); });
+        }
+        uint32_t g;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            g = ++gen_;
+            fn_ = &fn;
+            n_tasks_ = n_tasks;
+            done_.store(0, std::memory_order_relaxed);
+            ticket_.store((uint64_t)g << 32, std::memory_order_release);
+        }
+        cv_.notify_all();
+        take(g, &fn, n_tasks);
+        while (done_.load(std::memory_order_acquire) < n_tasks) std::this_thread::yield();
+    }
+
+  private:
+    // Tasks of job g until none is left (or a newer job has started).
+    void take(uint32_t g, const std::function<void(unsigned)>* fn, unsigned n) {
+        for (;;) {
+            uint64_t v = ticket_.load(std::memory_order_acquire);
+            do {
+                if ((uint32_t)(v >> 32) != g || (uint32_t)v >= n) return;
+            } while (!ticket_.compare_exchange_weak(v, v + 1, std::memory_order_acq_rel));
+            (*fn)((unsigned)(uint32_t)v);
+            done_.fetch_add(1, std::memory_order_release);
+        }
+    }
+    void work(uint32_t seen) {
+        for (;;) {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+            if (stop_) return;
+            seen = gen_;
+            const std::function<void(unsigned)>* fn = fn_;
+            const unsigned n = n_tasks_;
+            lk.unlock();
+            take(seen, fn, n);
+        }
+    }
+
+    std::vector<std::thread> threads_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    const std::function<void(unsigned)>* fn_ = nullptr;
+    unsigned n_tasks_ = 0;
+    uint32_t gen_ = 0;                 // job number (guarded by mu_)
+    std::atomic<uint64_t> ticket_{0};  // (job number << 32) | next task
+    std::atomic<unsigned> done_{0};    // tasks of the current job finished
+    bool stop_ = false;
+};
+
 }  // namespace
 
 struct pf_ctx {
@@ -87,6 +176,17 @@ struct pf_ctx {
     uint64_t stamp_n_curves = 0;
     cudaStream_t stamp_stream = nullptr;
     PinnedBuf h_in;
+    // Small results (statistics, best cells, synchronous peaks) land here
+    // and are copied into the caller's arrays after the synchronisation: a
+    // device-to-host copy into pageable memory costs more than the memcpy.
+    PinnedBuf h_res;
+    struct HostCopy {
+        void* dst;
+        const void* src;
+        size_t n;
+    };
+    std::vector<HostCopy> res_copies;  // h_res -> caller, after the synchronisation
+    WorkerPool pool;
     uint64_t launches = 0;
     double last_ms = -1.0;
     int n_sm = 0;
@@ -240,6 +340,32 @@ void for_each_curve(uint64_t n_curves, uint64_t total_points, F& fn) {
             for (uint64_t c = w; c < n_curves; c += nthr) fn(c);
         });
     for (auto& t : th) t.join();
+}
+
+// The packing of a host-pointer call split into tasks for the context's
+// worker threads: consecutive curve ranges of about equal point counts
+// (first[k] .. first[k+1]), on one thread per 16k points up to 16.
+struct CurveTasks {
+    unsigned width = 1;
+    std::vector<uint64_t> first;
+    unsigned count() const { return (unsigned)first.size() - 1; }
+};
+
+CurveTasks curve_tasks(const std::vector<int64_t>& off, uint64_t total_pts) {
+    constexpr uint64_t kPointsPerThread = 16384;
+    CurveTasks T;
+    const uint64_t n_curves = off.size();
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    T.width = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(hw, total_pts / kPointsPerThread));
+    const uint64_t n_tasks = std::max<uint64_t>(1, std::min<uint64_t>(n_curves, 4ull * T.width));
+    T.first.resize(n_tasks + 1);
+    for (uint64_t k = 0; k < n_tasks; k++)
+        T.first[k] = (uint64_t)(std::lower_bound(off.begin(), off.end(),
+                                                 (int64_t)(k * total_pts / n_tasks)) -
+                                off.begin());
+    T.first[0] = 0;
+    T.first[n_tasks] = n_curves;
+    return T;
 }
 
 // The reference's normalize=True preparation of one curve
@@ -1056,6 +1182,30 @@ int push_pending(pf_ctx* ctx, const Job& j, size_t n, bool work, cudaStream_t s)
     return PF_OK;
 }
 
+// Queue the device-to-host copy of a small result into the pinned result
+// block at byte offset `at` (the block must already hold it), and its copy
+// on into the caller's array once the call has synchronised.
+int queue_result(pf_ctx* ctx, void* dst, const void* d_src, size_t n, size_t at,
+                 cudaStream_t s) {
+    char* h = (char*)ctx->h_res.p + at;
+    PF_CUDA(cudaMemcpyAsync(h, d_src, n, cudaMemcpyDeviceToHost, s), "D2H results");
+    ctx->res_copies.push_back(pf_ctx::HostCopy{dst, h, n});
+    return PF_OK;
+}
+
+// End of a synchronous host call: mark the call's end, wait for it, hand
+// the queued small results to the caller.
+int finish_sync(pf_ctx* ctx, cudaStream_t s) {
+    int rc;
+    if ((rc = mark_done(ctx, s)) != PF_OK) return rc;
+    PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
+    ctx->staged_pending = false;
+    for (const pf_ctx::HostCopy& c : ctx->res_copies) memcpy(c.dst, c.src, c.n);
+    ctx->res_copies.clear();
+    read_kernel_time(ctx);
+    return PF_OK;
+}
+
 // Copy a peak call's results (d_pidx / d_pval, n_curves x n_peaks) back:
 // into the caller's arrays, or with PF_ASYNC into the next pending slot's
 // pinned block (free: its last user was collected, so no copy into it is
@@ -1071,6 +1221,14 @@ int copy_peaks_back(pf_ctx* ctx, const Job& j, bool async, cudaStream_t s) {
         hi = q.res.p;
         hv = (char*)q.res.p + pk * 8;
     }
+    if (pk > 0 && !async) {
+        // Through the pinned result block; the caller's arrays are filled
+        // after the synchronisation.
+        int rc = ensure_pinned(ctx, ctx->h_res, pk * 12);
+        if (rc != PF_OK) return rc;
+        if ((rc = queue_result(ctx, hi, ctx->d_pidx.p, pk * 8, 0, s)) != PF_OK) return rc;
+        return queue_result(ctx, hv, ctx->d_pval.p, pk * 4, pk * 8, s);
+    }
     if (pk > 0) {
         PF_CUDA(cudaMemcpyAsync(hi, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
                 "D2H peak indices");
@@ -1083,6 +1241,7 @@ int copy_peaks_back(pf_ctx* ctx, const Job& j, bool async, cudaStream_t s) {
 // The whole pipeline for host-pointer inputs.
 int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* const* mags,
              const uint64_t* lengths) {
+    ctx->res_copies.clear();
     int rc = validate_common(ctx, j);
     if (rc != PF_OK) return rc;
     const bool async = (j.mode & PF_ASYNC) != 0;
@@ -1118,11 +1277,10 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
     // Pack the curves (several host threads for large batches).
     {
         Stage stage_pack("pf pack");
-        const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-        const unsigned nthr = (L.total_pts > (1u << 20)) ? hw : 1u;
-        std::vector<int> bad(nthr, 0);
+        const CurveTasks T = curve_tasks(L.off, L.total_pts);
+        std::vector<int> bad(T.count(), 0);
         auto worker = [&](unsigned w) {
-            for (uint64_t c = w; c < j.n_curves; c += nthr) {
+            for (uint64_t c = T.first[w]; c < T.first[w + 1]; c++) {
                 const uint32_t n = L.len[c];
                 const uint32_t pad = (uint32_t)align_up(n, 4);
                 if (!copy_curve(times[c], mags[c], n, ht + L.off[c], hm + L.off[c], pad))
@@ -1135,13 +1293,7 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
                     center_curve(hm + L.off[c], n, hm + L.off[c]);
             }
         };
-        if (nthr == 1) {
-            worker(0);
-        } else {
-            std::vector<std::thread> th;
-            for (unsigned w = 0; w < nthr; w++) th.emplace_back(worker, w);
-            for (auto& t : th) t.join();
-        }
+        ctx->pool.run(T.count(), T.width, worker);
         for (int b : bad)
             if (b) return fail(ctx, PF_EINVAL, "times must be finite");
     }
@@ -1181,15 +1333,18 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
         PF_CUDA(cudaMemcpyAsync(j.out_bins, ctx->d_bins.p, bins_bytes, cudaMemcpyDeviceToHost, s),
                 "D2H bin counts");
     if (j.stats) {
-        PF_CUDA(cudaMemcpyAsync(j.out_stats, ctx->d_stat.p, (size_t)j.n_curves * 16,
-                                cudaMemcpyDeviceToHost, s),
-                "D2H statistics");
-        if (j.n_top > 0) {
-            const size_t pk = (size_t)j.n_curves * j.n_top;
-            PF_CUDA(cudaMemcpyAsync(j.out_idx, ctx->d_pidx.p, pk * 8, cudaMemcpyDeviceToHost, s),
-                    "D2H best indices");
-            PF_CUDA(cudaMemcpyAsync(j.out_val, ctx->d_pval.p, pk * 4, cudaMemcpyDeviceToHost, s),
-                    "D2H best values");
+        // Through the pinned result block (filled into the caller's arrays
+        // after the synchronisation).
+        const size_t b_st = (size_t)j.n_curves * 16;
+        const size_t pk = (size_t)j.n_curves * j.n_top;
+        if ((rc = ensure_pinned(ctx, ctx->h_res, b_st + pk * 12)) != PF_OK) return rc;
+        if ((rc = queue_result(ctx, j.out_stats, ctx->d_stat.p, b_st, 0, s)) != PF_OK) return rc;
+        if (pk > 0) {
+            if ((rc = queue_result(ctx, j.out_idx, ctx->d_pidx.p, pk * 8, b_st, s)) != PF_OK)
+                return rc;
+            if ((rc = queue_result(ctx, j.out_val, ctx->d_pval.p, pk * 4, b_st + pk * 8, s)) !=
+                PF_OK)
+                return rc;
         }
     } else if (!j.peaks) {
         PF_CUDA(cudaMemcpyAsync(j.out, ctx->d_out.p, out_bytes, cudaMemcpyDeviceToHost, s),
@@ -1200,11 +1355,7 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
         // block stays marked in use until the H2D copy above has finished.
         if (async) return mark_done(ctx, s);
     }
-    if ((rc = mark_done(ctx, s)) != PF_OK) return rc;
-    PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
-    ctx->staged_pending = false;
-    read_kernel_time(ctx);
-    return PF_OK;
+    return finish_sync(ctx, s);
 }
 
 // Device-pointer inputs and output, enqueued on the caller's stream.
@@ -1333,6 +1484,7 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
             uint32_t min_distance, int64_t* out_idx, float* out_val, bool bls = false,
             float qmin = 0.0f, float qmax = 0.0f) {
     if (!ctx) return PF_EINVAL;
+    ctx->res_copies.clear();
     Job j;
     j.algo = ALGO_LS;  // no bin-count checks of CE / AOV apply
     j.mode = mode;
@@ -1391,12 +1543,11 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
     float* hivy = (float*)(hb + o_ivy);
     double tmax = 0.0;
     {
-        const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-        const unsigned nthr = total > (1u << 20) ? hw : 1u;
-        std::vector<int> bad(nthr, 0);
-        std::vector<float> tmx(nthr, 0.0f);
+        const CurveTasks T = curve_tasks(off, total);
+        std::vector<int> bad(T.count(), 0);
+        std::vector<float> tmx(T.count(), 0.0f);
         auto worker = [&](unsigned w) {
-            for (uint64_t c = w; c < n_curves; c += nthr) {
+            for (uint64_t c = T.first[w]; c < T.first[w + 1]; c++) {
                 const float* t = times[c];
                 const float* m = mags[c];
                 const float* e = errs ? errs[c] : nullptr;
@@ -1425,13 +1576,7 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
                 }
             }
         };
-        if (nthr == 1) {
-            worker(0);
-        } else {
-            std::vector<std::thread> th;
-            for (unsigned w = 0; w < nthr; w++) th.emplace_back(worker, w);
-            for (auto& t : th) t.join();
-        }
+        ctx->pool.run(T.count(), T.width, worker);
         for (int b : bad)
             if (b) return fail(ctx, PF_EINVAL, "times must be finite");
         for (float x : tmx) tmax = std::max(tmax, (double)x);
@@ -1501,11 +1646,7 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
         PF_CUDA(cudaMemcpyAsync(out, p.out, out_bytes, cudaMemcpyDeviceToHost, s),
                 "D2H periodogram");
     }
-    if ((rc = mark_done(ctx, s)) != PF_OK) return rc;
-    PF_CUDA(cudaStreamSynchronize(s), "stream synchronize");
-    ctx->staged_pending = false;
-    read_kernel_time(ctx);
-    return PF_OK;
+    return finish_sync(ctx, s);
 }
 
 }  // namespace
@@ -1583,6 +1724,7 @@ void pf_ctx_destroy(pf_ctx* ctx) {
                       &ctx->d_prep})
         if (b->p) cudaFree(b->p);
     if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
+    if (ctx->h_res.p) cudaFreeHost(ctx->h_res.p);
     for (pf_ctx::Pending& q : ctx->pend) {
         if (q.res.p) cudaFreeHost(q.res.p);
         if (q.done) cudaEventDestroy(q.done);

@@ -185,6 +185,65 @@ __device__ float median_row(const float* x, uint32_t n, int tr, float ref, bool 
     return __fdiv_rn(__fadd_rn(__fadd_rn(-0.0f, unkey(a)), unkey(b)), 2.0f);
 }
 
+// Rows of at most kSortMax cells are sorted once in shared memory instead of
+// radix-selected pass by pass: the median, the MAD and the best entries are
+// then read off the sorted row.
+constexpr uint32_t kSortMax = 8192;
+
+__host__ __device__ inline uint32_t sort_width(uint32_t n) {
+    uint32_t p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+// Dynamic shared memory of stats_kernel: the leaf table, then (sorted path)
+// the row and its sort records.
+__host__ __device__ inline size_t stats_rowcopy_offset(uint32_t leaf_cap) {
+    return ((size_t)leaf_cap * 12 + 15) & ~(size_t)15;
+}
+__host__ __device__ inline size_t stats_sortrec_offset(uint32_t leaf_cap, uint32_t n) {
+    return stats_rowcopy_offset(leaf_cap) + (((size_t)n * 4 + 15) & ~(size_t)15);
+}
+
+// Ascending bitonic sort of w (a power of two) 64-bit records, all threads.
+__device__ void bitonic_sort(unsigned long long* s, uint32_t w) {
+    for (uint32_t k = 2; k <= w; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < w; i += kStatThreads) {
+                const uint32_t p = i ^ j;
+                if (p > i) {
+                    const unsigned long long a = s[i], b = s[p];
+                    const bool up = (i & k) == 0;
+                    if ((a > b) == up) {
+                        s[i] = b;
+                        s[p] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// The k-th smallest (0-based) of the merge of two non-decreasing sequences
+// A (na values) and B (nb values), k < na + nb: binary search for how many
+// of the k + 1 smallest come from A.
+template <class FA, class FB>
+__device__ float kth_of_merge(FA A, uint32_t na, FB B, uint32_t nb, uint32_t k) {
+    uint32_t lo = (k + 1 > nb) ? k + 1 - nb : 0u;
+    uint32_t hi = min(na, k + 1);
+    while (lo < hi) {
+        const uint32_t i = (lo + hi) / 2;
+        const uint32_t j = k + 1 - i;
+        if (i < na && j > 0 && B(j - 1) > A(i)) lo = i + 1;
+        else hi = i;
+    }
+    const uint32_t i = lo, j = k + 1 - lo;
+    if (i == 0) return B(j - 1);
+    if (j == 0) return A(i - 1);
+    return fmaxf(A(i - 1), B(j - 1));
+}
+
 __global__ void __launch_bounds__(kStatThreads)
     stats_kernel(const float* __restrict__ pg, uint32_t n, int use_max, uint32_t n_top,
                  uint32_t leaf_cap, float* __restrict__ stats, int64_t* __restrict__ top_idx,
@@ -207,9 +266,34 @@ __global__ void __launch_bounds__(kStatThreads)
     }
     __syncthreads();
     const uint32_t n_leaves = s_leaves;  // == leaf_cap (the same recursion on the host)
+    const bool sorted = n <= kSortMax;
+    unsigned long long* rec = nullptr;
+    const uint32_t w = sort_width(n);
     int nan_local = 0;
-    for (uint32_t i = threadIdx.x; i < n; i += kStatThreads) nan_local |= isnan(x[i]) ? 1 : 0;
+    if (sorted) {
+        // The row into shared memory, and one sort record per cell: the
+        // cell's order key (complemented when the largest is best, so that
+        // an ascending sort puts the best first) above its index, so equal
+        // values keep the lowest index first.  Padding sorts last.
+        float* xs = reinterpret_cast<float*>(ssm + stats_rowcopy_offset(leaf_cap));
+        rec = reinterpret_cast<unsigned long long*>(ssm + stats_sortrec_offset(leaf_cap, n));
+        for (uint32_t i = threadIdx.x; i < w; i += kStatThreads) {
+            if (i < n) {
+                const float v = x[i];
+                xs[i] = v;
+                nan_local |= isnan(v) ? 1 : 0;
+                const uint32_t k = use_max ? ~fkey(v) : fkey(v);
+                rec[i] = ((unsigned long long)k << 32) | i;
+            } else {
+                rec[i] = ~0ull;
+            }
+        }
+        x = xs;
+    } else {
+        for (uint32_t i = threadIdx.x; i < n; i += kStatThreads) nan_local |= isnan(x[i]) ? 1 : 0;
+    }
     if (nan_local) atomicOr(&s_nan, 1);
+    __syncthreads();
 
     // np.mean, then np.std as in numpy's _var: mean kept as float32, the
     // squared deviations summed pairwise, divided by n, square root.
@@ -219,6 +303,60 @@ __global__ void __launch_bounds__(kStatThreads)
     const float ssq = pairwise_row(x, n, T_SQDEV, mean, n_leaves, leaf_lo, leaf_len, leaf);
     const float stdv = __fsqrt_rn(__fdiv_rn(ssq, fn));
     const bool any_nan = s_nan != 0;
+    if (sorted) {
+        bitonic_sort(rec, w);
+        // Values in ascending order: rec holds them best first.
+        auto asc = [&](uint32_t pos) -> float {
+            const uint32_t k = (uint32_t)(rec[use_max ? n - 1 - pos : pos] >> 32);
+            return unkey(use_max ? ~k : k);
+        };
+        if (threadIdx.x == 0) {
+            float med = __uint_as_float(0x7FC00000u), mad = med;
+            if (!any_nan && n > 0) {
+                // np.median: the middle value, or the mean of the two
+                // middle values (np.mean of a two-element array).
+                const uint32_t k1 = (n - 1) / 2;
+                med = (n % 2) ? asc(k1)
+                              : __fdiv_rn(__fadd_rn(__fadd_rn(-0.0f, asc(k1)), asc(k1 + 1)),
+                                          2.0f);
+                // MAD: the deviations |v - med| of the values below the
+                // median, taken downwards, and of the rest, taken upwards,
+                // are two non-decreasing sequences (rounding is monotone);
+                // their merged order statistics give np.median of |x - med|.
+                uint32_t lo = 0, hi = n;  // la = number of values below med
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) / 2;
+                    if (asc(mid) < med) lo = mid + 1;
+                    else hi = mid;
+                }
+                const uint32_t la = lo;
+                auto A = [&](uint32_t i) { return fabsf(__fsub_rn(asc(la - 1 - i), med)); };
+                auto B = [&](uint32_t j) { return fabsf(__fsub_rn(asc(la + j), med)); };
+                const float d1 = kth_of_merge(A, la, B, n - la, k1);
+                mad = (n % 2) ? d1
+                              : __fdiv_rn(__fadd_rn(__fadd_rn(-0.0f, d1),
+                                                    kth_of_merge(A, la, B, n - la, k1 + 1)),
+                                          2.0f);
+            }
+            stats[4 * c + 0] = mean;
+            stats[4 * c + 1] = stdv;
+            stats[4 * c + 2] = med;
+            stats[4 * c + 3] = mad;
+        }
+        // The n_top best: the first records, best first, lowest index
+        // first among equal values; -1 / 0 beyond the row.
+        for (uint32_t a = threadIdx.x; a < n_top; a += kStatThreads) {
+            if (a < n) {
+                const uint32_t i = (uint32_t)rec[a];
+                top_idx[c * n_top + a] = i;
+                top_val[c * n_top + a] = x[i];
+            } else {
+                top_idx[c * n_top + a] = -1;
+                top_val[c * n_top + a] = 0.0f;
+            }
+        }
+        return;
+    }
     const float med = median_row(x, n, T_X, 0.0f, any_nan, hist);
     const float mad = median_row(x, n, T_ABSDEV, med, any_nan, hist);
     if (threadIdx.x == 0) {
@@ -373,7 +511,9 @@ cudaError_t launch_stats(const float* pg, uint64_t n_curves, uint32_t n_cells, i
                          cudaStream_t s) {
     if (n_curves == 0) return cudaSuccess;
     const uint32_t leaves = n_cells ? stats_leaf_count(n_cells) : 1;
-    const size_t smem = (size_t)leaves * 12;
+    size_t smem = (size_t)leaves * 12;
+    if (n_cells <= kSortMax)
+        smem = stats_sortrec_offset(leaves, n_cells) + (size_t)sort_width(n_cells) * 8;
     if (smem > 200u * 1024u) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(stats_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
