@@ -12,6 +12,8 @@ import threading
 
 import numpy as np
 
+from . import _hostptr
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpfb200.so")
 
@@ -240,12 +242,19 @@ for _name in ("__setitem__", "__delitem__", "__iadd__", "__imul__", "append", "e
 
 def host_pointers(arrs, lengths):
     """Data pointers (uintp) of float32 curves, and the object that keeps
-    them valid.  Short curves are gathered into one buffer, whose pointers
-    are arithmetic (taking an array's address costs about a microsecond,
-    more than copying a thousand points); longer ones are used in place."""
+    them valid.  1-D contiguous float32 arrays are used in place (their
+    addresses read by the compiled helper); otherwise short curves are
+    gathered into one buffer, whose pointers are arithmetic (taking an
+    array's address from Python costs about a microsecond, more than copying
+    a thousand points), and longer ones converted one by one."""
     n = len(lengths)
     if isinstance(arrs, FlatList) and arrs.ptrs is not None and len(arrs.ptrs) == n:
         return arrs.ptrs, arrs
+    if n:
+        ptrs = np.empty(n, dtype=np.uintp)
+        lens = np.empty(n, dtype=np.uint64)
+        if _hostptr.curve_pointers(arrs, lens, ptrs) and np.array_equal(lens, lengths):
+            return ptrs, arrs
     total = int(lengths.sum()) if n else 0
     if 0 < n and total <= 1024 * n and total <= (1 << 22):
         buf = np.concatenate(arrs).astype(np.float32, copy=False)
@@ -266,6 +275,17 @@ class CurveBatch:
     def __init__(self, times, mags):
         n = len(times)
         self.n = n
+        if n and len(mags) == n and not isinstance(mags, FlatList):
+            # Arrays used in place, lengths and addresses read in one pass.
+            lt, lm = np.empty(n, dtype=np.uint64), np.empty(n, dtype=np.uint64)
+            pt, pm = np.empty(n, dtype=np.uintp), np.empty(n, dtype=np.uintp)
+            if _hostptr.curve_pointers(times, lt, pt) and _hostptr.curve_pointers(mags, lm, pm):
+                if not np.array_equal(lt, lm):
+                    raise ValueError("times and mags must have the same length for every curve")
+                self.lengths = lt
+                self.tptr, self._times = pt, times
+                self.mptr, self._mags = pm, mags
+                return
         self.lengths = np.fromiter((len(t) for t in times), dtype=np.uint64, count=n)
         mlen = np.fromiter((len(m) for m in mags), dtype=np.uint64, count=len(mags))
         if not np.array_equal(mlen, self.lengths):

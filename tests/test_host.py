@@ -290,6 +290,19 @@ def test_curve_pointers_address_the_curves():
         assert norm.ptrs is None
         bc = nat.CurveBatch(ts, norm)
         np.testing.assert_array_equal(read(bc.mptr[0], sizes[0]), norm[0])
+    # 1-D contiguous float32 arrays are addressed in place (the compiled
+    # helper reads their addresses); a strided view is not, and takes the
+    # converting path.
+    ts32 = [rng.uniform(0, 100, k).astype(np.float32) for k in (7, 300)]
+    ms32 = [rng.normal(15, 0.3, k).astype(np.float32) for k in (7, 300)]
+    b = nat.CurveBatch(ts32, ms32)
+    assert b.lengths.tolist() == [7, 300]
+    assert [int(p) for p in b.tptr] == [a.ctypes.data for a in ts32]
+    assert [int(p) for p in b.mptr] == [a.ctypes.data for a in ms32]
+    strided = [np.arange(20, dtype=np.float32)[::2], ms32[1][:10]]
+    b = nat.CurveBatch([ts32[1][:10], ts32[1][10:20]], strided)
+    for c in range(2):
+        np.testing.assert_array_equal(read(b.mptr[c], 10), strided[c])
     with pytest.raises(ValueError):
         nat.CurveBatch([np.zeros(3, np.float32)], [np.zeros(4, np.float32)])
 
