@@ -188,6 +188,8 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
     }
     const double qb = cta_qbound_of<BLOCK>(p, my_pmin, period_dt);
     const bool fast = __syncthreads_and(fin ? 1 : 0) && qb * (double)nP < 1073741824.0;  // 2^30
+    // |q| < 2^19 as well: the phase's 32 fraction bits come from one FMA.
+    const bool fast32 = fast && qb < 524288.0;
 
     const double nd20 = (double)nP * 1048576.0;
     const uint32_t n_neg = 0u - nP;
@@ -195,6 +197,10 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
     // the fraction bits moved to the top of the word.
     const uint32_t edge_add = p.edge_d << 12;
     const uint32_t edge_lim = (2u * p.edge_d) << 12;
+    // The same guard in units of 2^-32 of a bin for fast_bin32, widened by
+    // n_phase + 2 units for the truncation of the phase to 32 bits.
+    const uint32_t edge32_add = edge_add + nP + 2u;
+    const uint32_t edge32_lim = 2u * edge32_add;
 
     auto stage = [&](uint32_t base, uint32_t cnt) {
         const float4* gt = reinterpret_cast<const float4*>(p.t + cd.off + base);
@@ -274,6 +280,25 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
             ev = ylo * 4096u + edge_add;
             return __funnelshift_r(ylo, yhi, 20) + (uint32_t)__double2loint(r) * n_neg;
         };
+        // |q| < 2^19: y = RD(q' * 2^32 + 1.5*2^52) holds floor(frac(q') * 2^32)
+        // in its low word f, so the row is the high word of f * n (one
+        // integer multiply) and the low word is the position within the
+        // row (plus the guard, for the edge test): two FP64 operations per
+        // point instead of three.  The row carries no bias.
+        auto fast_bin32 = [&](double td, auto has_pdt_tag, uint32_t& ev) -> uint32_t {
+            constexpr bool HAS_PDT = decltype(has_pdt_tag)::value;
+            double a;
+            if constexpr (HAS_PDT) {
+                a = td - s.c * td * td;
+            } else {
+                a = td;
+            }
+            const double qh = __dmul_rn(a, s.yhi);
+            const double y = __fma_rd(qh, 4294967296.0, kMagic15);
+            const uint32_t f = (uint32_t)__double2loint(y);
+            ev = f * nP + edge32_add;
+            return __umulhi(f, nP);
+        };
         // The reference's exact sequence (correctly rounded quotient, float
         // fold, f32 divide, then % n_phase: a folded phase of 1.0f gives bin
         // n_phase, which wraps to 0): the bin (+2^31 bias).
@@ -295,8 +320,16 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
             }
         };
 
-        auto body = [&](auto has_pdt_tag, auto fast_tag) {
+        auto body = [&](auto has_pdt_tag, auto fast_tag, auto f32_tag) {
             constexpr bool FAST = decltype(fast_tag)::value;
+            constexpr bool F32 = decltype(f32_tag)::value;
+            // Fast bin (unbiased with F32, +2^31 otherwise; the counter
+            // address is the same either way) and its edge limit.
+            auto bin_of = [&](double td, uint32_t& ev) -> uint32_t {
+                if constexpr (F32) return fast_bin32(td, has_pdt_tag, ev);
+                else return fast_bin(td, has_pdt_tag, ev);
+            };
+            const uint32_t lim = F32 ? edge32_lim : edge_lim;
             if constexpr (FAST) {
                 // Groups of 32 points: no branch per point; a group whose
                 // smallest edge-test value is below the limit is revisited
@@ -311,7 +344,7 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
                         for (uint32_t ii = 0; ii < 32u; ii++) {
                             const BinPoint pt = load_point(g + ii);
                             uint32_t ev;
-                            const uint32_t row = fast_bin(pt.t, has_pdt_tag, ev);
+                            const uint32_t row = bin_of(pt.t, ev);
                             emin = min(emin, ev);
                             add(row, pt, 1u);
                         }
@@ -320,18 +353,19 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
                         for (uint32_t i = g; i < gend; i++) {
                             const BinPoint pt = load_point(i);
                             uint32_t ev;
-                            const uint32_t row = fast_bin(pt.t, has_pdt_tag, ev);
+                            const uint32_t row = bin_of(pt.t, ev);
                             emin = min(emin, ev);
                             add(row, pt, 1u);
                         }
                     }
-                    if (emin < edge_lim) {
+                    if (emin < lim) {
                         for (uint32_t i = g; i < gend; i++) {
                             const BinPoint pt = tile[i];
                             uint32_t ev;
-                            const uint32_t row = fast_bin(pt.t, has_pdt_tag, ev);
-                            if (ev < edge_lim) {
-                                const uint32_t ex = exact_bin(pt.t, has_pdt_tag);
+                            const uint32_t row = bin_of(pt.t, ev);
+                            if (ev < lim) {
+                                const uint32_t ex =
+                                    exact_bin(pt.t, has_pdt_tag) - (F32 ? 0x80000000u : 0u);
                                 if (ex != row) {
                                     add(row, pt, 0xFFFFFFFFu);
                                     add(ex, pt, 1u);
@@ -348,12 +382,16 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
                 }
             }
         };
+        using T_ = std::true_type;
+        using F_ = std::false_type;
         if (period_dt != 0.0f) {
-            if (fast) body(std::true_type{}, std::true_type{});
-            else body(std::true_type{}, std::false_type{});
+            if (fast32) body(T_{}, T_{}, T_{});
+            else if (fast) body(T_{}, T_{}, F_{});
+            else body(T_{}, F_{}, F_{});
         } else {
-            if (fast) body(std::false_type{}, std::true_type{});
-            else body(std::false_type{}, std::false_type{});
+            if (fast32) body(F_{}, T_{}, T_{});
+            else if (fast) body(F_{}, T_{}, F_{});
+            else body(F_{}, F_{}, F_{});
         }
     }
     // Every lane of the warp reaches this barrier (inactive lanes skip the
