@@ -245,6 +245,7 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
     const uint32_t pi = w.p0 + (active ? jr : 0u);
     Cell s;
     cell_setup<FOLD_EXACT>(s, p.periods[pi], period_dt);
+    const double y32 = s.yhi * 4294967296.0;  // RN(1/P) * 2^32, exact
     for (uint32_t k = 0; k < slots; k++)
         reinterpret_cast<uint32_t*>(cnt_raw)[k * BLOCK + tid] = 0u;
 
@@ -280,11 +281,14 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
             ev = ylo * 4096u + edge_add;
             return __funnelshift_r(ylo, yhi, 20) + (uint32_t)__double2loint(r) * n_neg;
         };
-        // |q| < 2^19: y = RD(q' * 2^32 + 1.5*2^52) holds floor(frac(q') * 2^32)
-        // in its low word f, so the row is the high word of f * n (one
-        // integer multiply) and the low word is the position within the
-        // row (plus the guard, for the edge test): two FP64 operations per
-        // point instead of three.  The row carries no bias.
+        // |q| < 2^19: y = RD(t_corr * (RN(1/P) * 2^32) + 1.5*2^52), one FMA
+        // on the exact product (closer to t_corr / P than the rounded
+        // product fast_bin uses, so the same guard holds), leaves
+        // floor(frac(q') * 2^32) in its low word f.  The 64-bit product
+        // f * n then holds the row in its high word and the position within
+        // the row in its low word (plus the guard, for the edge test): one
+        // FP64 operation and one integer multiply per point.  The row
+        // carries no bias.
         auto fast_bin32 = [&](double td, auto has_pdt_tag, uint32_t& ev) -> uint32_t {
             constexpr bool HAS_PDT = decltype(has_pdt_tag)::value;
             double a;
@@ -293,11 +297,11 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
             } else {
                 a = td;
             }
-            const double qh = __dmul_rn(a, s.yhi);
-            const double y = __fma_rd(qh, 4294967296.0, kMagic15);
+            const double y = __fma_rd(a, y32, kMagic15);
             const uint32_t f = (uint32_t)__double2loint(y);
-            ev = f * nP + edge32_add;
-            return __umulhi(f, nP);
+            const unsigned long long fn = (unsigned long long)f * nP;
+            ev = (uint32_t)fn + edge32_add;
+            return (uint32_t)(fn >> 32);
         };
         // The reference's exact sequence (correctly rounded quotient, float
         // fold, f32 divide, then % n_phase: a folded phase of 1.0f gives bin
