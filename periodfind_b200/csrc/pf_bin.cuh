@@ -150,7 +150,12 @@ __device__ __forceinline__ double aov_sbx_fast(uint32_t tbase, uint32_t nP, uint
 template <int ALGO, bool CNT16, int BLOCK, bool REF_STATS, int ROUNDS>
 __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, uint32_t item) {
     extern __shared__ __align__(16) unsigned char smem[];
+    // CE: one 16-byte record per point.  AOV: the times (doubles) and the
+    // fixed-point magnitudes in two arrays, so four points take three
+    // 128-bit loads instead of four.
     BinPoint* tile = reinterpret_cast<BinPoint*>(smem);
+    double* tile_t = reinterpret_cast<double*>(smem);
+    uint32_t* tile_a = reinterpret_cast<uint32_t*>(smem + kBinTile * sizeof(double));
     unsigned char* cnt_raw = smem + kBinTile * sizeof(BinPoint);
     const uint32_t cnt_base = (uint32_t)__cvta_generic_to_shared(cnt_raw);
 
@@ -223,10 +228,9 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
             for (uint32_t i4 = tid; i4 < n4; i4 += BLOCK) {
                 const float4 q = gt[i4];
                 const uint4 a = ga[i4];
-                tile[4 * i4 + 0] = BinPoint{(double)q.x, a.x, 0u};
-                tile[4 * i4 + 1] = BinPoint{(double)q.y, a.y, 0u};
-                tile[4 * i4 + 2] = BinPoint{(double)q.z, a.z, 0u};
-                tile[4 * i4 + 3] = BinPoint{(double)q.w, a.w, 0u};
+                reinterpret_cast<double2*>(tile_t)[2 * i4] = make_double2(q.x, q.y);
+                reinterpret_cast<double2*>(tile_t)[2 * i4 + 1] = make_double2(q.z, q.w);
+                reinterpret_cast<uint4*>(tile_a)[i4] = a;
             }
         }
     };
@@ -258,10 +262,15 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
         }
         if (!active) continue;
 
-    // One 128-bit shared load per point record.
+        // One point: a 128-bit shared load of its record (CE), or its time
+        // and magnitude from the two arrays (AOV).
         auto load_point = [&](uint32_t i) -> BinPoint {
-            const uint4 raw = reinterpret_cast<const uint4*>(tile)[i];
-            return BinPoint{__hiloint2double((int)raw.y, (int)raw.x), raw.z, raw.w};
+            if constexpr (ALGO == ALGO_CE) {
+                const uint4 raw = reinterpret_cast<const uint4*>(tile)[i];
+                return BinPoint{__hiloint2double((int)raw.y, (int)raw.x), raw.z, raw.w};
+            } else {
+                return BinPoint{tile_t[i], tile_a[i], 0u};
+            }
         };
         // Fast bin of one point: row (+2^31 bias) and the edge-test value
         // ((fraction + D) << 12); the point is near an edge iff ev < edge_lim.
@@ -344,13 +353,29 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
                     if (gend - g == 32u) {
                         // A full group unrolled completely: no loop control
                         // per point (measured 10% faster than unrolling by 4).
-#pragma unroll
-                        for (uint32_t ii = 0; ii < 32u; ii++) {
-                            const BinPoint pt = load_point(g + ii);
+                        auto one = [&](const BinPoint& pt) {
                             uint32_t ev;
                             const uint32_t row = bin_of(pt.t, ev);
                             emin = min(emin, ev);
                             add(row, pt, 1u);
+                        };
+                        if constexpr (ALGO == ALGO_CE) {
+#pragma unroll
+                            for (uint32_t ii = 0; ii < 32u; ii++) one(load_point(g + ii));
+                        } else {
+                            // Four points per two 128-bit loads of times
+                            // and one of magnitudes (g is a multiple of 32).
+                            const double2* t2 = reinterpret_cast<const double2*>(tile_t) + g / 2;
+                            const uint4* a4 = reinterpret_cast<const uint4*>(tile_a) + g / 4;
+#pragma unroll 4
+                            for (uint32_t ii = 0; ii < 8u; ii++) {
+                                const double2 ta = t2[2 * ii], tb = t2[2 * ii + 1];
+                                const uint4 aa = a4[ii];
+                                one(BinPoint{ta.x, aa.x, 0u});
+                                one(BinPoint{ta.y, aa.y, 0u});
+                                one(BinPoint{tb.x, aa.z, 0u});
+                                one(BinPoint{tb.y, aa.w, 0u});
+                            }
                         }
                     } else {
 #pragma unroll 4
@@ -364,7 +389,7 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
                     }
                     if (emin < lim) {
                         for (uint32_t i = g; i < gend; i++) {
-                            const BinPoint pt = tile[i];
+                            const BinPoint pt = load_point(i);
                             uint32_t ev;
                             const uint32_t row = bin_of(pt.t, ev);
                             if (ev < lim) {
@@ -381,7 +406,7 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
             } else {
 #pragma unroll 4
                 for (uint32_t i = 0; i < cnt; i++) {
-                    const BinPoint pt = tile[i];
+                    const BinPoint pt = load_point(i);
                     add(exact_bin(pt.t, has_pdt_tag), pt, 1u);
                 }
             }
