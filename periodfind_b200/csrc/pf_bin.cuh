@@ -23,7 +23,12 @@
 // about 3e-5 of evaluations take that branch at n = 10.
 //
 // Valid while |q| * n < 2^30 (checked per CTA from the batch's max|t|;
-// otherwise the CTA runs the generic loop).
+// otherwise the CTA runs the generic loop).  While also |q| < 2^19 one FP64
+// operation does it (fast_bin32): y = RD(t_corr * (RN(1/P) * 2^32) +
+// 1.5*2^52) on the exact product leaves floor(frac(q') * 2^32) in its low
+// word f, and the 64-bit product f * n holds the row (high word) and the
+// position within it (low word, tested against the same guard in units of
+// 2^-32, widened by n + 2 for the truncation).
 //
 // CE counters are 16-bit halves of 32-bit words when every count fits
 // (curve length * overlaps < 65536), doubling the CTAs per SM; AOV keeps a
@@ -321,13 +326,18 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
             const uint32_t pb = min(trunc_u(folded / p.phase_bin_size), nP);
             return 0x80000000u + (pb == nP ? 0u : pb);
         };
+        // AOV bytes per bin row, kept opaque to the compiler so that the
+        // counter address is one multiply-add (a power-of-two constant
+        // would become a shift and a separate add).
+        uint32_t aov_row_bytes = 2 * BLOCK * 4;
+        asm("" : "+r"(aov_row_bytes));
         auto add = [&](uint32_t row, const BinPoint& pt, uint32_t sign) {
             // sign is 1 (add) or 0xFFFFFFFF (take back); u32 wraparound keeps
             // packed 16-bit halves and sums exact.
             if constexpr (ALGO == ALGO_CE) {
                 red_shared_u32(row * row_stride + pt.a + tbase, pt.b * sign);
             } else {
-                const uint32_t a0 = row * (2 * BLOCK * 4) + tbase;
+                const uint32_t a0 = row * aov_row_bytes + tbase;
                 red_shared_u32(a0, sign);
                 red_shared_u32(a0 + BLOCK * 4, pt.a * sign);
             }

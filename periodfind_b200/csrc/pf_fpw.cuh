@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(BLOCK)
     // Chosen form: the fast bin is exact away from bin edges while
     // |q| * n_bins < 2^30 (the same bound as the chosen CE / AOV kernels),
     // checked for the CTA from max|t| and its smallest |P|.
-    bool fast = false;
+    bool fast = false, fast32 = false;
     if constexpr (CHOSEN) {
         double mn = fabs((double)period);
 #pragma unroll
@@ -123,18 +123,35 @@ __global__ void __launch_bounds__(BLOCK)
         const double qb = p.tmax / pmin + fabs((double)period_dt) * p.tmax * p.tmax /
                                               (2.0 * pmin * pmin);
         fast = qb * (double)nb < 1073741824.0;  // 2^30
+        // |q| < 2^19 as well: the one-FMA bin below.
+        fast32 = fast && qb < 524288.0;
     }
     const double nd20 = (double)nb * 1048576.0;
     const uint32_t n_neg = 0u - nb;
     const uint32_t edge_add = p.edge_d << 12;
     const uint32_t edge_lim = (2u * p.edge_d) << 12;
+    // The guard in units of 2^-32 of a bin, widened by n_bins + 2 units for
+    // the truncation of the phase to 32 bits.
+    const uint32_t edge32_add = edge_add + nb + 2u;
+    const uint32_t edge32_lim = 2u * edge32_add;
+    const double y32 = s.yhi * 4294967296.0;  // RN(1/P) * 2^32, exact
 
     // The reference's bin of point time t (the fast bin when the CTA's
     // bound allows, the reference sequence near an edge or otherwise).
     auto bin_of = [&](TT t) -> uint32_t {
         if constexpr (CHOSEN) {
             const double td = t;
-            if (fast) {
+            if (fast32) {
+                // One FMA on the exact product t * (RN(1/P) * 2^32) leaves
+                // floor(frac(q') * 2^32) in the low word f; the 64-bit
+                // product f * n_bins holds the bin (high word) and the
+                // position within it (low word, for the edge test).
+                const double a = has_pdt ? td - s.c * td * td : td;
+                const double y = __fma_rd(a, y32, kMagic15);
+                const uint32_t f = (uint32_t)__double2loint(y);
+                const unsigned long long fn = (unsigned long long)f * nb;
+                if ((uint32_t)fn + edge32_add >= edge32_lim) return (uint32_t)(fn >> 32);
+            } else if (fast) {
                 const double a = has_pdt ? td - s.c * td * td : td;
                 const double qh = __dmul_rn(a, s.yhi);
                 const double r = __dadd_rd(qh, kMagic15);
