@@ -142,6 +142,20 @@ __device__ __forceinline__ float rint_small(float x) {
     return __fsub_rn(__fadd_rn(x, 12582912.0f), 12582912.0f);  // |x| < 2^22
 }
 
+// The same phase without a period derivative in four operations: r, the
+// integer nearest t*fhi (the exact product against 1.5*2^23 in one FMA: ulp 1
+// there, |t*fhi| < 2^22), then t*fhi - r and t*flo each added on the exact
+// product in one FMA.  Two roundings of the reduced phase: |error| <= 2^-24
+// turns (fold_df: 2^-25 in seven operations).  Used for curves of at least
+// kPhase4MinPoints points; on shorter ones the LS sums can be near-singular
+// (a two-point curve's power moved by a quarter under a one-ulp phase
+// change), and they keep fold_df.
+constexpr uint32_t kPhase4MinPoints = 32;
+__device__ __forceinline__ float fold_df4(float t, const Cell& s) {
+    const float r = __fsub_rn(__fmaf_rn(t, s.fhi, 12582912.0f), 12582912.0f);
+    return __fmaf_rn(t, s.flo, __fmaf_rn(t, s.fhi, -r));
+}
+
 template <bool HAS_PDT>
 __device__ __forceinline__ float fold_df(float t, const Cell& s) {
     const float p = __fmul_rn(t, s.fhi);
@@ -340,28 +354,36 @@ __device__ __forceinline__ void accumulate(const FoldParams& p, const Views& v, 
 
         if constexpr (ALGO == ALGO_LS && FOLD == FOLD_DF && !ALT) {
             // Four points per pair of 128-bit broadcast loads; the tail (not
-            // the zero padding) one point at a time.
-            auto ls_point = [&](float t, float mag) {
-                const float ph = fold_df<HAS_PDT>(t, s);
-                float sin_val, cos_val;
-                sincosf(kTwoPi * ph, &sin_val, &cos_val);
-                ls.mag_cos += mag * cos_val;
-                ls.mag_sin += mag * sin_val;
-                ls.cos_cos += cos_val * cos_val;
-                ls.cos_sin += cos_val * sin_val;
-            };
-            const float4* t4 = reinterpret_cast<const float4*>(tile_t);
-            const float4* m4 = reinterpret_cast<const float4*>(v.tile_a);
-            const uint32_t full = cnt & ~3u;
+            // the zero padding) one point at a time.  The phase form is
+            // uniform over the CTA (one curve per item).
+            auto ls_tile = [&](auto phase_of) {
+                auto ls_point = [&](float t, float mag) {
+                    const float ph = phase_of(t);
+                    float sin_val, cos_val;
+                    sincosf(kTwoPi * ph, &sin_val, &cos_val);
+                    ls.mag_cos += mag * cos_val;
+                    ls.mag_sin += mag * sin_val;
+                    ls.cos_cos += cos_val * cos_val;
+                    ls.cos_sin += cos_val * sin_val;
+                };
+                const float4* t4 = reinterpret_cast<const float4*>(tile_t);
+                const float4* m4 = reinterpret_cast<const float4*>(v.tile_a);
+                const uint32_t full = cnt & ~3u;
 #pragma unroll 2
-            for (uint32_t i = 0; i < full; i += 4) {
-                const float4 tt = t4[i >> 2], mm = m4[i >> 2];
-                ls_point(tt.x, mm.x);
-                ls_point(tt.y, mm.y);
-                ls_point(tt.z, mm.z);
-                ls_point(tt.w, mm.w);
-            }
-            for (uint32_t i = full; i < cnt; i++) ls_point(tile_t[i], __uint_as_float(v.tile_a[i]));
+                for (uint32_t i = 0; i < full; i += 4) {
+                    const float4 tt = t4[i >> 2], mm = m4[i >> 2];
+                    ls_point(tt.x, mm.x);
+                    ls_point(tt.y, mm.y);
+                    ls_point(tt.z, mm.z);
+                    ls_point(tt.w, mm.w);
+                }
+                for (uint32_t i = full; i < cnt; i++)
+                    ls_point(tile_t[i], __uint_as_float(v.tile_a[i]));
+            };
+            if (!HAS_PDT && n >= kPhase4MinPoints)
+                ls_tile([&](float t) { return fold_df4(t, s); });
+            else
+                ls_tile([&](float t) { return fold_df<HAS_PDT>(t, s); });
             continue;
         }
 
@@ -666,7 +688,8 @@ __global__ void ce_magbin_kernel(const float* __restrict__ m, uint32_t* __restri
 
 // Folded phase of each (period, time) pair with one fold variant, as the
 // fold kernels compute it (precision studies): out[p * n + i].  FOLD_DF
-// returns turns in [-1, 1]; the others [0, 1].
+// returns turns in [-1, 1] (the four-operation form where the LS kernel uses
+// it: no derivative and n >= kPhase4MinPoints); the others [0, 1].
 template <int FOLD>
 __global__ void phase_probe_kernel(const float* __restrict__ t, uint64_t n,
                                    const float* __restrict__ periods, uint64_t n_per,
@@ -687,7 +710,9 @@ __global__ void phase_probe_kernel(const float* __restrict__ t, uint64_t n,
         } else if constexpr (FOLD == FOLD_F32) {
             ph = fold_f32(ti, s);
         } else {
-            ph = (period_dt != 0.0f) ? fold_df<true>(ti, s) : fold_df<false>(ti, s);
+            ph = (period_dt != 0.0f) ? fold_df<true>(ti, s)
+                 : (n >= kPhase4MinPoints) ? fold_df4(ti, s)
+                                           : fold_df<false>(ti, s);
         }
         out[k] = ph;
     }
