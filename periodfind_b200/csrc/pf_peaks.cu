@@ -130,6 +130,42 @@ __device__ __forceinline__ void warp_promote(WarpTop& w, int lane) {
 
 // Dynamic shared memory: [kChunk int64 extrema indices][kChunk f32 values]
 // [n_peaks int64][n_peaks f32] (the best-first list).
+// The streaming state machine over one chunk's compacted extrema (index
+// order), by one warp holding the top list across its lanes: extrema that
+// do not beat the threshold are skipped by ballot, the others fed in turn
+// (peaks.rs:18-238: promotion of a due candidate, candidate replacement,
+// promotion once min_distance samples have been fed).
+__device__ __forceinline__ void warp_replay(WarpTop& w, int lane, const int64_t* ext_idx,
+                                            const float* ext_val, uint32_t ne, uint64_t md,
+                                            bool use_max) {
+    for (uint32_t b0 = 0; b0 < ne; b0 += 32) {
+        const uint32_t e = b0 + lane;
+        const bool in = e < ne;
+        const int64_t my_i = in ? ext_idx[e] : 0;
+        const float my_v = in ? ext_val[e] : 0.0f;
+        uint32_t pending =
+            __ballot_sync(0xffffffffu, in && better(use_max, my_v, w.thr));
+        while (pending) {
+            const int k = __ffs(pending) - 1;
+            const int64_t i = __shfl_sync(0xffffffffu, my_i, k);
+            const float v = __shfl_sync(0xffffffffu, my_v, k);
+            if (w.has_cand && (uint64_t)w.cand_idx + (md > 0 ? md - 1 : 0) <
+                                  (uint64_t)i)
+                warp_promote(w, lane);
+            if (better(use_max, v, w.thr) &&
+                (!w.has_cand || better(use_max, v, w.cand_val))) {
+                w.cand_idx = i;
+                w.cand_val = v;
+                w.has_cand = true;
+            }
+            if (w.has_cand && (uint64_t)(i - w.cand_idx) + 1 >= md)
+                warp_promote(w, lane);
+            pending &= ~(1u << k);
+            pending &= __ballot_sync(0xffffffffu, better(use_max, my_v, w.thr));
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kPeakThreads)
     peaks_kernel(const float* __restrict__ pg, uint64_t flat_len, uint32_t n_peaks,
                  uint32_t min_distance, int use_max_i, int64_t* __restrict__ out_idx,
@@ -228,33 +264,7 @@ __global__ void __launch_bounds__(kPeakThreads)
         // index order.
         if (warp_list) {
             if (wid == 0) {
-                const uint32_t ne = chunk_count;
-                for (uint32_t b0 = 0; b0 < ne; b0 += 32) {
-                    const uint32_t e = b0 + lane;
-                    const bool in = e < ne;
-                    const int64_t my_i = in ? ext_idx[e] : 0;
-                    const float my_v = in ? ext_val[e] : 0.0f;
-                    uint32_t pending =
-                        __ballot_sync(0xffffffffu, in && better(use_max, my_v, w.thr));
-                    while (pending) {
-                        const int k = __ffs(pending) - 1;
-                        const int64_t i = __shfl_sync(0xffffffffu, my_i, k);
-                        const float v = __shfl_sync(0xffffffffu, my_v, k);
-                        if (w.has_cand && (uint64_t)w.cand_idx + (md > 0 ? md - 1 : 0) <
-                                              (uint64_t)i)
-                            warp_promote(w, lane);
-                        if (better(use_max, v, w.thr) &&
-                            (!w.has_cand || better(use_max, v, w.cand_val))) {
-                            w.cand_idx = i;
-                            w.cand_val = v;
-                            w.has_cand = true;
-                        }
-                        if (w.has_cand && (uint64_t)(i - w.cand_idx) + 1 >= md)
-                            warp_promote(w, lane);
-                        pending &= ~(1u << k);
-                        pending &= __ballot_sync(0xffffffffu, better(use_max, my_v, w.thr));
-                    }
-                }
+                warp_replay(w, lane, ext_idx, ext_val, chunk_count, md, use_max);
                 if (lane == 0) thr_sh = w.thr;
             }
         } else if (tid == 0) {
@@ -304,12 +314,96 @@ __global__ void __launch_bounds__(kPeakThreads)
     }
 }
 
+
+// Top lists of at most 32 peaks: a warp per row, no CTA barrier, so up to 64
+// rows per SM replay their extrema at once (the CTA-per-row kernel above
+// runs one replaying warp per 256 threads while the rest wait at its
+// barriers).  A warp takes 256 samples per step: lane l tests samples
+// base + 32 k + l (k < 8; coalesced loads, neighbours from the same
+// lines), the extrema that beat the current threshold are compacted in
+// index order by ballot into the warp's shared buffer, then replayed.
+constexpr int kRowWarps = 4;
+constexpr uint32_t kWarpStep = 256;
+
+__global__ void __launch_bounds__(kRowWarps * 32, 10)
+    peaks_warp_kernel(const float* __restrict__ pg, uint64_t n_rows, uint64_t flat_len,
+                      uint32_t n_peaks, uint32_t min_distance, int use_max_i,
+                      int64_t* __restrict__ out_idx, float* __restrict__ out_val) {
+    __shared__ int64_t s_idx[kRowWarps][kWarpStep];
+    __shared__ float s_val[kRowWarps][kWarpStep];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint64_t c = (uint64_t)blockIdx.x * kRowWarps + wid;
+    if (c >= n_rows) return;  // the whole warp; no CTA-wide barrier follows
+    const float* d = pg + c * flat_len;
+    const bool use_max = use_max_i != 0;
+    int64_t* ext_idx = s_idx[wid];
+    float* ext_val = s_val[wid];
+
+    WarpTop w;
+    w.idx = -1;
+    w.val = 0.0f;
+    w.count = 0;
+    w.n_peaks = n_peaks;
+    w.use_max = use_max;
+    w.has_cand = false;
+    w.cand_idx = -1;
+    w.cand_val = use_max ? -INFINITY : INFINITY;
+    w.thr = use_max ? -INFINITY : INFINITY;
+    const uint64_t md = min_distance;
+    const unsigned lt_mask = (1u << lane) - 1u;
+
+    const uint64_t last = (flat_len >= 2) ? flat_len - 2 : 0;
+    for (uint64_t base = 1; flat_len >= 3 && base <= last; base += kWarpStep) {
+        const float thr0 = w.thr;  // uniform across the warp
+        float v[8];
+        bool pk[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint64_t i = base + (uint64_t)k * 32 + lane;
+            pk[k] = false;
+            v[k] = 0.0f;
+            if (i <= last) {
+                const float l = d[i - 1], x = d[i], r = d[i + 1];
+                v[k] = x;
+                pk[k] = use_max ? (x > l && x > r && x > thr0) : (x < l && x < r && x < thr0);
+            }
+        }
+        uint32_t ne = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const unsigned m = __ballot_sync(0xffffffffu, pk[k]);
+            if (pk[k]) {
+                const uint32_t pos = ne + __popc(m & lt_mask);
+                ext_idx[pos] = (int64_t)(base + (uint64_t)k * 32 + lane);
+                ext_val[pos] = v[k];
+            }
+            ne += __popc(m);
+        }
+        __syncwarp();
+        warp_replay(w, lane, ext_idx, ext_val, ne, md, use_max);
+        __syncwarp();
+    }
+    warp_promote(w, lane);
+    if (lane < (int)n_peaks) {
+        const bool have = (uint32_t)lane < w.count;
+        out_idx[c * n_peaks + lane] = have ? w.idx : -1;
+        out_val[c * n_peaks + lane] = have ? w.val : 0.0f;
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_peaks(const float* pg, uint64_t n_curves, uint64_t flat_len,
                          uint32_t n_peaks, uint32_t min_distance, int use_max,
                          int64_t* out_idx, float* out_val, cudaStream_t stream) {
     if (n_curves == 0 || n_peaks == 0) return cudaSuccess;
+    if (n_peaks <= 32) {
+        const uint64_t blocks = (n_curves + kRowWarps - 1) / kRowWarps;
+        if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+        peaks_warp_kernel<<<(unsigned)blocks, kRowWarps * 32, 0, stream>>>(
+            pg, n_curves, flat_len, n_peaks, min_distance, use_max, out_idx, out_val);
+        return cudaGetLastError();
+    }
     const size_t smem = (size_t)kChunk * 12 + (size_t)n_peaks * 12;
     if (smem > 227u * 1024u) return cudaErrorInvalidValue;  // n_peaks > ~18000
     cudaError_t e = cudaFuncSetAttribute(peaks_kernel,
