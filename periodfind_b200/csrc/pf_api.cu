@@ -466,6 +466,7 @@ struct Layout {
     std::vector<uint32_t> order;  // queue kernels: curves longest first
     size_t total_pts = 0;      // padded
     size_t o_t = 0, o_m = 0, o_curves = 0, o_work = 0, o_periods = 0, o_pdts = 0, o_srcoff = 0;
+    size_t o_tmax = 0;  // host-packed calls: max |t| of the batch (float bits)
     size_t bytes = 0;
     uint32_t n_work = 0;
     uint32_t max_len = 0;
@@ -648,14 +649,19 @@ void build_order(const Layout& L, uint64_t n_curves, uint32_t* order) {
                      [&](uint32_t a, uint32_t b) { return L.len[a] > L.len[b]; });
 }
 
-// Copy one curve into the packed staging area, checking times are finite.
-bool copy_curve(const float* t, const float* m, uint32_t n, float* dt, float* dm, uint32_t pad) {
+// Copy one curve into the packed staging area, checking times are finite
+// and raising tmax to their largest magnitude.
+bool copy_curve(const float* t, const float* m, uint32_t n, float* dt, float* dm, uint32_t pad,
+                float& tmax) {
     bool ok = true;
+    float mx = tmax;
     for (uint32_t i = 0; i < n; i++) {
         const float x = t[i];
         ok &= std::isfinite(x);
+        mx = std::max(mx, std::fabs(x));
         dt[i] = x;
     }
+    tmax = mx;
     if (n) memcpy(dm, m, (size_t)n * sizeof(float));
     for (uint32_t i = n; i < pad; i++) {
         dt[i] = 0.0f;
@@ -714,6 +720,8 @@ int plan(pf_ctx* ctx, const Job& j, const uint64_t* lengths, bool with_points, b
     if (with_grid) o = align_up(o + j.n_pdt * 4, 256);
     L.o_srcoff = o;
     if (!with_points) o = align_up(o + j.n_curves * 8, 256);
+    L.o_tmax = o;
+    if (with_points) o = align_up(o + 4, 256);
     L.bytes = o;
     return PF_OK;
 }
@@ -1054,7 +1062,8 @@ int launch_classes(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig&
 // Device pipeline shared by both entry styles: preparation kernel, fused
 // kernel, optional peak search.  `p` has the input pointers set.
 int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig& cfg,
-                    FoldParams& p, CurveDesc* dcurves, float* d_out, cudaStream_t s) {
+                    FoldParams& p, CurveDesc* dcurves, float* d_out, cudaStream_t s,
+                    const unsigned* d_tmax_staged = nullptr) {
     const bool cpu = use_cpu_semantics(j.mode);
     p.n_per = (uint32_t)j.n_per;
     p.n_pdt = (uint32_t)j.n_pdt;
@@ -1073,10 +1082,15 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
     int rc;
     if ((rc = ensure_dev(ctx, ctx->d_misc, 256)) != PF_OK) return rc;
     static_assert(kCounterOffset + 4 * (kClasses + 1) <= 256, "counters fit the misc block");
-    p.tmax_bits = (const unsigned*)ctx->d_misc.p;
     Stage stage_prep("pf prepare");
-    PF_CUDA(launch_tmax(p.t, L.total_pts, (unsigned*)ctx->d_misc.p, s), "max|t| kernel");
-    ctx->launches++;
+    if (d_tmax_staged) {
+        // Host-packed inputs: max |t| came with them.
+        p.tmax_bits = d_tmax_staged;
+    } else {
+        p.tmax_bits = (const unsigned*)ctx->d_misc.p;
+        PF_CUDA(launch_tmax(p.t, L.total_pts, (unsigned*)ctx->d_misc.p, s), "max|t| kernel");
+        ctx->launches++;
+    }
     if (cfg.kind == KIND_BIN && j.algo == ALGO_CE) {
         if ((rc = ensure_dev(ctx, ctx->d_aux64, L.total_pts * 8 + 32)) != PF_OK) return rc;
         p.aux64 = (const uint64_t*)ctx->d_aux64.p;
@@ -1136,14 +1150,16 @@ int device_pipeline(pf_ctx* ctx, const Job& j, const Layout& L, const FoldConfig
         ctx->timed_pending = true;
     }
     if (j.stats) {
+        // One block: [curve][mean, std, median, mad], then the best cells'
+        // indices and values, so the results come back in one copy.
         Stage stage_stats("pf statistics");
         const size_t pk = (size_t)j.n_curves * std::max<uint32_t>(j.n_top, 1u);
-        if ((rc = ensure_dev(ctx, ctx->d_pidx, pk * 8)) != PF_OK) return rc;
-        if ((rc = ensure_dev(ctx, ctx->d_pval, pk * 4)) != PF_OK) return rc;
-        if ((rc = ensure_dev(ctx, ctx->d_stat, (size_t)j.n_curves * 16)) != PF_OK) return rc;
+        const size_t b_st = (size_t)j.n_curves * 16;
+        if ((rc = ensure_dev(ctx, ctx->d_stat, b_st + pk * 12)) != PF_OK) return rc;
+        char* st = (char*)ctx->d_stat.p;
         PF_CUDA(launch_stats(d_out, j.n_curves, (uint32_t)(j.n_per * j.n_pdt),
-                             j.algo == ALGO_CE ? 0 : 1, j.n_top, (float*)ctx->d_stat.p,
-                             (int64_t*)ctx->d_pidx.p, (float*)ctx->d_pval.p, s),
+                             j.algo == ALGO_CE ? 0 : 1, j.n_top, (float*)st,
+                             (int64_t*)(st + b_st), (float*)(st + b_st + pk * 8), s),
                 "statistics kernel launch");
         ctx->launches++;
     }
@@ -1279,11 +1295,12 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
         Stage stage_pack("pf pack");
         const CurveTasks T = curve_tasks(L.off, L.total_pts);
         std::vector<int> bad(T.count(), 0);
+        std::vector<float> tmx(T.count(), 0.0f);
         auto worker = [&](unsigned w) {
             for (uint64_t c = T.first[w]; c < T.first[w + 1]; c++) {
                 const uint32_t n = L.len[c];
                 const uint32_t pad = (uint32_t)align_up(n, 4);
-                if (!copy_curve(times[c], mags[c], n, ht + L.off[c], hm + L.off[c], pad))
+                if (!copy_curve(times[c], mags[c], n, ht + L.off[c], hm + L.off[c], pad, tmx[w]))
                     bad[w] = 1;
                 // Magnitude preparation fused into the packing (numpy's
                 // values, as pf_normalize_mags / pf_center_mags).
@@ -1296,6 +1313,11 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
         ctx->pool.run(T.count(), T.width, worker);
         for (int b : bad)
             if (b) return fail(ctx, PF_EINVAL, "times must be finite");
+        // The kernels' range guard reads max |t| as float bits: found while
+        // packing, so no reduction kernel is needed.
+        float tmax = 0.0f;
+        for (float x : tmx) tmax = std::max(tmax, x);
+        memcpy(hb + L.o_tmax, &tmax, 4);
     }
     fill_meta(ctx, j, L, cfg, hb);
     if (!j.fgrid) memcpy(hb + L.o_periods, j.periods, j.n_per * 4);
@@ -1327,7 +1349,7 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
         p.bins = (uint32_t*)ctx->d_bins.p;
     }
     rc = device_pipeline(ctx, j, L, cfg, p, (CurveDesc*)(db + L.o_curves), (float*)ctx->d_out.p,
-                         s);
+                         s, (const unsigned*)(db + L.o_tmax));
     if (rc != PF_OK) return rc;
     if (j.out_bins)
         PF_CUDA(cudaMemcpyAsync(j.out_bins, ctx->d_bins.p, bins_bytes, cudaMemcpyDeviceToHost, s),
@@ -1337,14 +1359,16 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
         // after the synchronisation).
         const size_t b_st = (size_t)j.n_curves * 16;
         const size_t pk = (size_t)j.n_curves * j.n_top;
-        if ((rc = ensure_pinned(ctx, ctx->h_res, b_st + pk * 12)) != PF_OK) return rc;
-        if ((rc = queue_result(ctx, j.out_stats, ctx->d_stat.p, b_st, 0, s)) != PF_OK) return rc;
+        const size_t pk1 = (size_t)j.n_curves * std::max<uint32_t>(j.n_top, 1u);  // layout
+        const size_t bytes = pk > 0 ? b_st + pk1 * 12 : b_st;
+        if ((rc = ensure_pinned(ctx, ctx->h_res, bytes)) != PF_OK) return rc;
+        char* hr = (char*)ctx->h_res.p;
+        PF_CUDA(cudaMemcpyAsync(hr, ctx->d_stat.p, bytes, cudaMemcpyDeviceToHost, s),
+                "D2H statistics");
+        ctx->res_copies.push_back(pf_ctx::HostCopy{j.out_stats, hr, b_st});
         if (pk > 0) {
-            if ((rc = queue_result(ctx, j.out_idx, ctx->d_pidx.p, pk * 8, b_st, s)) != PF_OK)
-                return rc;
-            if ((rc = queue_result(ctx, j.out_val, ctx->d_pval.p, pk * 4, b_st + pk * 8, s)) !=
-                PF_OK)
-                return rc;
+            ctx->res_copies.push_back(pf_ctx::HostCopy{j.out_idx, hr + b_st, pk * 8});
+            ctx->res_copies.push_back(pf_ctx::HostCopy{j.out_val, hr + b_st + pk1 * 8, pk * 4});
         }
     } else if (!j.peaks) {
         PF_CUDA(cudaMemcpyAsync(j.out, ctx->d_out.p, out_bytes, cudaMemcpyDeviceToHost, s),
