@@ -357,10 +357,6 @@ class HostBatch:
         self.lens = np.diff(off).astype(np.uint64)
         self.tptr = self.ptrs(t)
         self.mptr = self.ptrs(m)
-        self.m_ce = np.empty_like(m)
-        self.m_ls = np.empty_like(m)
-        self.ceptr = self.ptrs(self.m_ce)
-        self.lsptr = self.ptrs(self.m_ls)
 
     def ptrs(self, a):
         return (np.uint64(a.ctypes.data)
@@ -369,12 +365,12 @@ class HostBatch:
 
 def e2e_cabi(hb, periods, pdts, steps, warmup, device):
     """Wall time per step of CE + AOV + LS peaks through the C ABI from host
-    buffers: host magnitude preparation (pf_normalize_mags /
-    pf_center_mags), and the peak calls -- each packs its curves into pinned
-    staging, copies them to the GPU, runs the kernels and the peak search
-    and copies the peaks back -- pipelined with PF_ASYNC so that host work
-    overlaps the GPU.  Returns (s per step, H2D bytes, D2H bytes, kernel
-    launches per step)."""
+    buffers: the peak calls -- each packs its curves into pinned staging
+    with the magnitude preparation (PF_HOST_NORMALIZE / PF_HOST_CENTER),
+    copies them to the GPU, runs the kernels and the peak search and copies
+    the peaks back -- pipelined with PF_ASYNC so that host work overlaps the
+    GPU.  Returns (s per step, H2D bytes, D2H bytes, kernel launches per
+    step)."""
     from periodfind_b200 import _native as nat
 
     ctx = nat.Context(device)
@@ -385,9 +381,11 @@ def e2e_cabi(hb, periods, pdts, steps, warmup, device):
     flags = nat.PF_MODE_CHOSEN | nat.PF_ASYNC
     grid = (periods.ctypes.data, len(periods), pdts.ctypes.data, len(pdts))
 
-    def peaks(algo, mptr, k):
-        args = (h, hb.tptr.ctypes.data, mptr.ctypes.data, hb.lens.ctypes.data, n) + grid
-        out = (flags, idx[k].ctypes.data, val[k].ctypes.data)
+    def peaks(algo, k, a, e, prep):
+        # Curves [a, e): pointers, lengths and output rows from offset a.
+        ptr = lambda arr, itemsize: arr.ctypes.data + a * itemsize
+        args = (h, ptr(hb.tptr, 8), ptr(hb.mptr, 8), ptr(hb.lens, 8), e - a) + grid
+        out = (flags | prep, ptr(idx[k], 8 * N_PEAKS), ptr(val[k], 4 * N_PEAKS))
         if algo == "ce":
             rc = lib.pf_ce_peaks(*args, 10, 10, 1, 1, N_PEAKS, 1, *out)
         elif algo == "aov":
@@ -396,16 +394,19 @@ def e2e_cabi(hb, periods, pdts, steps, warmup, device):
             rc = lib.pf_ls_peaks(*args, N_PEAKS, 1, *out)
         ctx.check(rc)
 
+    q = n // 4
+
     def step():
-        ctx.check(lib.pf_normalize_mags(hb.mptr.ctypes.data, hb.lens.ctypes.data, n,
-                                        hb.ceptr.ctypes.data))
-        peaks("ce", hb.ceptr, 0)
-        peaks("aov", hb.mptr, 1)
-        # Centring for LS runs on the host while the GPU works.
-        ctx.check(lib.pf_center_mags(hb.mptr.ctypes.data, hb.lens.ctypes.data, n,
-                                     hb.lsptr.ctypes.data))
+        # The magnitudes are normalised (CE) or centred (LS) as they are
+        # packed (numpy's values).  CE goes in two calls, a quarter of the
+        # curves first, so that the GPU starts once that quarter is packed;
+        # each later call is packed while the GPU runs the one before.
+        peaks("ce", 0, 0, q, nat.PF_HOST_NORMALIZE)
+        peaks("ce", 0, q, n, nat.PF_HOST_NORMALIZE)
         ctx.check(lib.pf_wait(h))
-        peaks("ls", hb.lsptr, 2)
+        peaks("aov", 1, 0, n, 0)
+        ctx.check(lib.pf_wait(h))
+        peaks("ls", 2, 0, n, nat.PF_HOST_CENTER)
         ctx.check(lib.pf_wait(h))
         ctx.check(lib.pf_wait(h))
 
@@ -891,8 +892,9 @@ def ragged_main(args):
             "e2e": {"value": n_eval / e2e_s, "unit": "evals/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
                     "path": "C ABI pf_ce_peaks / pf_aov_peaks / pf_ls_peaks from per-curve host "
-                            "arrays (PF_ASYNC pipeline), host magnitude preparation "
-                            "(pf_normalize_mags / pf_center_mags) inside the step"},
+                            "arrays (PF_ASYNC pipeline, CE in two calls), magnitude preparation "
+                            "fused into the packing (PF_HOST_NORMALIZE / PF_HOST_CENTER) "
+                            "inside the step"},
             "e2e_calc": None if calc_s is None else {
                 "s_per_algo": calc_s, "value": n_eval / sum(calc_s.values()),
                 "path": "gpu.ConditionalEntropy / AOV / LombScargle .calc(list of numpy, "

@@ -1,10 +1,12 @@
 # cython: language_level=3, boundscheck=False, wraparound=False
-"""Curve lengths and data pointers of a list of numpy arrays, for the
-host-pointer entry points of the C ABI.
+"""Host-side helpers of the ctypes path, compiled because the Python route
+costs more than the work it wraps.
 
-Taking one array's address from Python (``a.ctypes.data``) costs about a
-microsecond; a batch of 100 000 light curves spent a fifth of a second per
-array list on it.  Here the addresses are read from the array structs.
+curve_pointers: curve lengths and data addresses of a list of numpy arrays.
+    Taking one array's address from Python (``a.ctypes.data``) costs about a
+    microsecond; a batch of 100 000 light curves spent a fifth of a second
+    per array list on it.  Here the addresses are read from the array
+    structs.
 """
 
 cimport numpy as cnp
@@ -35,3 +37,4 @@ def curve_pointers(arrs, cnp.uint64_t[::1] lengths, size_t[::1] pointers):
         lengths[i] = <cnp.uint64_t>cnp.PyArray_DIM(a, 0)
         pointers[i] = <size_t>cnp.PyArray_DATA(a)
     return True
+

@@ -12,7 +12,7 @@ import threading
 
 import numpy as np
 
-from . import _hostptr
+from . import _host
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpfb200.so")
@@ -253,7 +253,7 @@ def host_pointers(arrs, lengths):
     if n:
         ptrs = np.empty(n, dtype=np.uintp)
         lens = np.empty(n, dtype=np.uint64)
-        if _hostptr.curve_pointers(arrs, lens, ptrs) and np.array_equal(lens, lengths):
+        if _host.curve_pointers(arrs, lens, ptrs) and np.array_equal(lens, lengths):
             return ptrs, arrs
     total = int(lengths.sum()) if n else 0
     if 0 < n and total <= 1024 * n and total <= (1 << 22):
@@ -279,7 +279,7 @@ class CurveBatch:
             # Arrays used in place, lengths and addresses read in one pass.
             lt, lm = np.empty(n, dtype=np.uint64), np.empty(n, dtype=np.uint64)
             pt, pm = np.empty(n, dtype=np.uintp), np.empty(n, dtype=np.uintp)
-            if _hostptr.curve_pointers(times, lt, pt) and _hostptr.curve_pointers(mags, lm, pm):
+            if _host.curve_pointers(times, lt, pt) and _host.curve_pointers(mags, lm, pm):
                 if not np.array_equal(lt, lm):
                     raise ValueError("times and mags must have the same length for every curve")
                 self.lengths = lt

@@ -9,7 +9,7 @@ Outputs:
     dropin/periodfind/*.so  the Cython modules ce, aov, ls, fpw, bls that take
                             the place of periodfind's own .pyx modules inside
                             the periodfind package, calling libpfb200.so
-    _hostptr.*.so           (next to this file) curve lengths and data
+    _host.*.so           (next to this file) curve lengths and data
                             addresses of numpy array lists for the ctypes path
 
 Per-translation-unit flags carry the two arithmetic semantics:
@@ -89,7 +89,7 @@ def build(force: bool = False, verbose: bool = True) -> str:
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + sorted(objs) + ["-lpthread"]
         subprocess.run(cmd, check=True)
     build_dropin(force)
-    build_hostptr(force)
+    build_host(force)
     if verbose:
         print(f"built {LIB}")
     return LIB
@@ -123,28 +123,28 @@ def _dropin_one(name: str, force: bool) -> str:
     return so
 
 
-def build_hostptr(force: bool = False) -> str:
-    """Cython -> C -> periodfind_b200/_hostptr (numpy C API only)."""
+def build_host(force: bool = False) -> str:
+    """Cython -> C -> periodfind_b200/_host (numpy C API only)."""
     import sysconfig
 
     import numpy as np
 
-    pyx = os.path.join(HERE, "_hostptr.pyx")
-    so = os.path.join(HERE, "_hostptr" + sysconfig.get_config_var("EXT_SUFFIX"))
+    pyx = os.path.join(HERE, "_host.pyx")
+    so = os.path.join(HERE, "_host" + sysconfig.get_config_var("EXT_SUFFIX"))
     if not force and _mtime(so) > _mtime(pyx):
         return so
     os.makedirs(OBJ, exist_ok=True)
     c_src = os.path.join(OBJ, "hostptr.c")
     r = subprocess.run([sys.executable, "-m", "cython", "-3", "--module-name",
-                        "periodfind_b200._hostptr", "-o", c_src, pyx],
+                        "periodfind_b200._host", "-o", c_src, pyx],
                        capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"cython failed for _hostptr.pyx:\n{r.stdout}\n{r.stderr}")
+        raise RuntimeError(f"cython failed for _host.pyx:\n{r.stdout}\n{r.stderr}")
     cmd = ["gcc", "-O2", "-shared", "-fPIC", "-DNPY_NO_DEPRECATED_API=NPY_1_7_API_VERSION",
            f"-I{sysconfig.get_paths()['include']}", f"-I{np.get_include()}", c_src, "-o", so]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"gcc failed for _hostptr:\n{r.stdout}\n{r.stderr}")
+        raise RuntimeError(f"gcc failed for _host:\n{r.stdout}\n{r.stderr}")
     return so
 
 
