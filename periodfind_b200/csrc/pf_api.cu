@@ -100,7 +100,15 @@ class WorkerPool {
         }
         while (threads_.size() + 1 < width) {
             const uint32_t g = gen_;  // the new worker waits for the next job
-            threads_.emplace_back([this, g] { work(g); });
+            try {
+                threads_.emplace_back([this, g] { work(g); });
+            } catch (...) {
+                break;  // no more threads to be had: run with those there are
+            }
+        }
+        if (threads_.empty()) {
+            for (unsigned k = 0; k < n_tasks; k++) fn(k);
+            return;
         }
         uint32_t g;
         {
