@@ -363,15 +363,22 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
                     if (gend - g == 32u) {
                         // A full group unrolled completely: no loop control
                         // per point (measured 10% faster than unrolling by 4).
-                        auto one = [&](const BinPoint& pt) {
+                        // Two running minima of the edge test (even and
+                        // odd points), so the minimum is two short
+                        // dependency chains instead of one of 32 links.
+                        uint32_t emin_b = 0xFFFFFFFFu;
+                        auto one = [&](const BinPoint& pt, uint32_t& em) {
                             uint32_t ev;
                             const uint32_t row = bin_of(pt.t, ev);
-                            emin = min(emin, ev);
+                            em = min(em, ev);
                             add(row, pt, 1u);
                         };
                         if constexpr (ALGO == ALGO_CE) {
 #pragma unroll
-                            for (uint32_t ii = 0; ii < 32u; ii++) one(load_point(g + ii));
+                            for (uint32_t ii = 0; ii < 32u; ii += 2) {
+                                one(load_point(g + ii), emin);
+                                one(load_point(g + ii + 1), emin_b);
+                            }
                         } else {
                             // Four points per two 128-bit loads of times
                             // and one of magnitudes (g is a multiple of 32).
@@ -381,12 +388,13 @@ __device__ __forceinline__ void bin_item(const FoldParams& p, const WorkItem w, 
                             for (uint32_t ii = 0; ii < 8u; ii++) {
                                 const double2 ta = t2[2 * ii], tb = t2[2 * ii + 1];
                                 const uint4 aa = a4[ii];
-                                one(BinPoint{ta.x, aa.x, 0u});
-                                one(BinPoint{ta.y, aa.y, 0u});
-                                one(BinPoint{tb.x, aa.z, 0u});
-                                one(BinPoint{tb.y, aa.w, 0u});
+                                one(BinPoint{ta.x, aa.x, 0u}, emin);
+                                one(BinPoint{ta.y, aa.y, 0u}, emin_b);
+                                one(BinPoint{tb.x, aa.z, 0u}, emin);
+                                one(BinPoint{tb.y, aa.w, 0u}, emin_b);
                             }
                         }
+                        emin = min(emin, emin_b);
                     } else {
 #pragma unroll 4
                         for (uint32_t i = g; i < gend; i++) {
