@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import numpy as np
 
+from . import _host
 from . import _native as nat
 from ._utils import ensure_float32, gc_paused, prepare_magnitudes, validate_inputs
 from .results import Periodogram, Statistics
@@ -63,16 +64,17 @@ def _grid(a, name):
     return np.ascontiguousarray(a)
 
 
-def _fused_prep(mags, center, normalize):
+def _fused_prep(mags, center, normalize, known_ok=False):
     """(magnitudes to pass, extra mode bits).  For float32 1-D curves that
     are all non-empty the native packing prepares the magnitudes itself
     (PF_HOST_CENTER / PF_HOST_NORMALIZE: numpy's values, no separate pass
     or copy); anything else is prepared here as the reference does.  The
-    centre / normalise conflict is settled by the caller."""
+    centre / normalise conflict is settled by the caller.  known_ok: the
+    batch was already found to have that form."""
     if not (center or normalize):
         return mags, 0
-    if all(isinstance(m, np.ndarray) and m.ndim == 1 and m.size and m.dtype == np.float32
-           for m in mags):
+    if known_ok or all(isinstance(m, np.ndarray) and m.ndim == 1 and m.size
+                       and m.dtype == np.float32 for m in mags):
         return mags, (nat.PF_HOST_CENTER if center else nat.PF_HOST_NORMALIZE)
     return prepare_magnitudes(mags, center, normalize), 0
 
@@ -322,9 +324,14 @@ class _Periodogram:
             raise NotImplementedError(
                 f'Output type "{output}" is not implemented. '
                 f'Use "stats", "periodogram", or "peaks".')
-        validate_inputs(times, mags)
-        ensure_float32(times, "times")
-        ensure_float32(mags, "mags")
+        # A batch already in the native calls' form (float32 1-D contiguous
+        # curves, lengths pairing up) needs none of the per-array checks;
+        # anything else gets them, with the reference's exceptions.
+        form = _host.curve_check(times, mags)
+        if not form:
+            validate_inputs(times, mags)
+            ensure_float32(times, "times")
+            ensure_float32(mags, "mags")
         periods = _grid(periods, "periods")
         period_dts = _grid(period_dts, "period_dts")
         if output == "peaks":
@@ -338,7 +345,7 @@ class _Periodogram:
         if center and normalize:  # the reference's conflict warning, then centre
             prepare_magnitudes([], center, normalize)
             normalize = False
-        mags_use, extra = _fused_prep(mags, center, normalize)
+        mags_use, extra = _fused_prep(mags, center, normalize, known_ok=form == 2)
 
         if (output == "stats" and 1 <= int(n_stats) < len(periods) * len(period_dts)
                 and (not self._use_max or len(period_dts) == 1)):
