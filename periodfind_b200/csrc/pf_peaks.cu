@@ -17,7 +17,11 @@
 //     end if no such index is fed;
 //   - a better extremum fed before that replaces it.
 // The sorted top-N list lives in shared memory (threshold in a register)
-// and is written to the caller's rows at the end.
+// and is written to the caller's rows at the end.  Lists of at most 32
+// peaks take peaks_warp_kernel instead: a warp per curve holds the list
+// across its lanes and does the flagging, compaction and replay itself.
+// (Both kernels give the same results: the state machine is the same and
+// only the chunking of the extrema differs.)
 //
 // Extrema that cannot pass the peak test are dropped before the replay.
 // The threshold only ever gets stricter (a full list only takes a better
