@@ -758,6 +758,16 @@ def batch_secondary(torch, device, flush, clocks, steps=3):
 # ------------------------------------------------------------------ main
 
 
+def _measured_hbm_gbs():
+    """The copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json
+    beside this file), else the earlier measurement on the pool."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback (earlier measurement on the pool)"
+
+
 def _roofline(kernel_ms, evals_algo, pipes, off, periods, pdts):
     """Roofline of the kernel with the most time, and each kernel's
     fraction of its own bound."""
@@ -779,6 +789,7 @@ def _roofline(kernel_ms, evals_algo, pipes, off, periods, pdts):
                       "bound": ROOFLINE[a]["bound"],
                       "frac": frac(ROOFLINE[a]["pipe"], ROOFLINE[a]["ops"], kernel_ms[a])[2]}
                   for a in kernel_ms}
+    hbm_peak, hbm_src = _measured_hbm_gbs()
     in_bytes = int(off[-1]) * 8 + len(periods) * 4
     out_bytes = (len(off) - 1) * len(periods) * len(pdts) * 4
     hbm_gbs = (in_bytes + out_bytes) / (kernel_ms[dom] * 1e-3) / 1e9
@@ -787,7 +798,8 @@ def _roofline(kernel_ms, evals_algo, pipes, off, periods, pdts):
             "kernel_ms": kernel_ms[dom],
             "peak_source": f"measured on this GPU (pipe_peaks.cu, {rf['pipe']})",
             "traffic": RAGGED_TRAFFIC[dom], "views": views, "per_kernel": per_kernel,
-            "hbm_view": {"achieved_gbs": hbm_gbs, "peak_gbs": 6453.7, "frac": hbm_gbs / 6453.7}}
+            "hbm_view": {"achieved_gbs": hbm_gbs, "peak_gbs": hbm_peak,
+                         "frac": hbm_gbs / hbm_peak, "peak_source": hbm_src}}
 
 
 def ragged_main(args):
