@@ -463,13 +463,14 @@ def test_preparation_fused_into_packing_is_bit_exact():
     """PF_HOST_NORMALIZE / PF_HOST_CENTER prepare the magnitudes while the
     library packs them: the periodograms equal those of magnitudes prepared
     by numpy first, bit for bit (CE normalised, LS centred, AOV centred),
-    with a constant and a one-point curve among them."""
+    with a constant and a one-point curve among them, and enough points
+    (~90 000) that the packing runs on several of the context's threads."""
     from periodfind_b200 import _native as nat
     from periodfind_b200 import gpu
 
     rng = np.random.default_rng(61)
     ts, ms = [], []
-    for n in (1, 7, 8, 9, 129, 300, 1025, 4097):
+    for n in (1, 7, 8, 9, 129, 300, 1025, 4097) + (2000,) * 40:
         t = lc.uniform_times(rng, n, 200.0)
         ts.append(t)
         ms.append(lc.noisy(rng, lc.sinusoid(t, float(rng.uniform(1, 4)), 0.3, 0.0, 15.0), 0.05))
