@@ -217,10 +217,14 @@ def measure_pipes():
 #   AOV bin kernel  two shared reductions (count, fixed-point sum); 3 FP64.
 #   LS fold kernel  MUFU sine and cosine.
 ROOFLINE = {
-    "ce": {"kernel": "bin_kernel<CE> (chosen)", "bound": "fp64", "pipe": "dfma", "ops": 3.0,
-           "views": {"shared_atomic": ("atoms_u32_private", 1.0)}},
+    # Operations the chosen kernels perform per evaluation: CE one shared
+    # u32 reduction (its 16-bit counter) and one FP64 FMA; AOV two
+    # reductions (count, fixed-point sum) and one FP64 FMA; LS a MUFU sine
+    # and cosine.  (Without a period derivative, |q| < 2^19.)
+    "ce": {"kernel": "bin_kernel<CE> (chosen)", "bound": "shared-atomic",
+           "pipe": "atoms_u32_private", "ops": 1.0, "views": {"fp64": ("dfma", 1.0)}},
     "aov": {"kernel": "bin_kernel<AOV> (chosen)", "bound": "shared-atomic",
-            "pipe": "atoms_u32_private", "ops": 2.0, "views": {"fp64": ("dfma", 3.0)}},
+            "pipe": "atoms_u32_private", "ops": 2.0, "views": {"fp64": ("dfma", 1.0)}},
     "ls": {"kernel": "fold_kernel<LS, split-precision> (chosen)", "bound": "mufu",
            "pipe": "mufu_sin+cos", "ops": 2.0, "views": {}},
 }
