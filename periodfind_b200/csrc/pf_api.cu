@@ -184,6 +184,17 @@ struct pf_ctx {
     uint64_t stamp_n_curves = 0;
     cudaStream_t stamp_stream = nullptr;
     PinnedBuf h_in;
+    // Host-pointer calls alternate between two device input blocks (d_in,
+    // d_in2) and copy on copy_stream, so that a call's inputs cross PCIe
+    // while the previous call's kernels run.  ev_in_free[i] follows the last
+    // kernel that read block i, ev_copied[i] the copy into it.  cur_slot is
+    // the block of the call being finished (-1: not a host call, which
+    // frees both).
+    DevBuf d_in2;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_in_free[2] = {nullptr, nullptr};
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr};
+    int in_slot = 0, cur_slot = -1;
     // Small results (statistics, best cells, synchronous peaks) land here
     // and are copied into the caller's arrays after the synchronisation: a
     // device-to-host copy into pageable memory costs more than the memcpy.
@@ -262,8 +273,31 @@ int order_after_previous(pf_ctx* ctx, cudaStream_t s) {
 int mark_done(pf_ctx* ctx, cudaStream_t s) {
     PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
     ctx->done_recorded = true;
+    // The input blocks this call's kernels read are free once they are
+    // done: a host call's own block; both for any other call.
+    for (int i = 0; i < 2; i++)
+        if (ctx->cur_slot < 0 || ctx->cur_slot == i)
+            PF_CUDA(cudaEventRecord(ctx->ev_in_free[i], s), "event");
+    ctx->cur_slot = -1;
     return PF_OK;
 }
+
+// Marks a host call's end on its stream when it returns early, after its
+// copy or kernels were queued: the input blocks count as in use until then.
+struct CallEnd {
+    pf_ctx* ctx;
+    cudaStream_t s;
+    bool armed = true;
+    ~CallEnd() {
+        if (!armed) return;
+        cudaEventRecord(ctx->ev_done, s);
+        ctx->done_recorded = true;
+        cudaEventRecord(ctx->ev_in_free[0], s);
+        cudaEventRecord(ctx->ev_in_free[1], s);
+        ctx->cur_slot = -1;
+        cudaGetLastError();
+    }
+};
 
 int ensure_dev(pf_ctx* ctx, DevBuf& b, size_t bytes) {
     if (bytes <= b.cap) return PF_OK;
@@ -1293,7 +1327,9 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
     if ((rc = plan(ctx, j, lengths, true, true, L, cfg)) != PF_OK) return rc;
     if ((rc = staging_ready(ctx)) != PF_OK) return rc;
     if ((rc = ensure_pinned(ctx, ctx->h_in, L.bytes)) != PF_OK) return rc;
-    if ((rc = ensure_dev(ctx, ctx->d_in, L.bytes)) != PF_OK) return rc;
+    const int slot = ctx->in_slot;
+    DevBuf& din = slot ? ctx->d_in2 : ctx->d_in;
+    if ((rc = ensure_dev(ctx, din, L.bytes)) != PF_OK) return rc;
     char* hb = (char*)ctx->h_in.p;
     float* ht = (float*)(hb + L.o_t);
     float* hm = (float*)(hb + L.o_m);
@@ -1332,14 +1368,23 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
     memcpy(hb + L.o_pdts, j.pdts, j.n_pdt * 4);
 
     cudaStream_t s = ctx->stream;
-    char* db = (char*)ctx->d_in.p;
+    char* db = (char*)din.p;
     if ((rc = order_after_previous(ctx, s)) != PF_OK) return rc;
+    // The copy waits only for the kernels that last read this input block
+    // (two host calls back), not for the previous call, whose kernels it
+    // overlaps; the kernels of this call wait for the copy.
+    CallEnd call_end{ctx, s};
     {
         Stage stage_h2d("pf H2D");
-        PF_CUDA(cudaMemcpyAsync(db, hb, L.bytes, cudaMemcpyHostToDevice, s), "H2D inputs");
+        PF_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_in_free[slot], 0), "stream wait");
+        PF_CUDA(cudaMemcpyAsync(db, hb, L.bytes, cudaMemcpyHostToDevice, ctx->copy_stream),
+                "H2D inputs");
+        PF_CUDA(cudaEventRecord(ctx->ev_copied[slot], ctx->copy_stream), "event");
     }
-    PF_CUDA(cudaEventRecord(ctx->ev_staged, s), "event");
+    PF_CUDA(cudaEventRecord(ctx->ev_staged, ctx->copy_stream), "event");
     ctx->staged_pending = true;
+    ctx->in_slot = slot ^ 1;
+    PF_CUDA(cudaStreamWaitEvent(s, ctx->ev_copied[slot], 0), "stream wait");
 
     FoldParams p{};
     p.t = (const float*)(db + L.o_t);
@@ -1385,8 +1430,14 @@ int run_host(pf_ctx* ctx, const Job& j, const float* const* times, const float* 
         if ((rc = copy_peaks_back(ctx, j, async, s)) != PF_OK) return rc;
         // PF_ASYNC: the call returns with its work queued.  The staging
         // block stays marked in use until the H2D copy above has finished.
-        if (async) return mark_done(ctx, s);
+        if (async) {
+            ctx->cur_slot = slot;
+            call_end.armed = false;
+            return mark_done(ctx, s);
+        }
     }
+    ctx->cur_slot = slot;
+    call_end.armed = false;
     return finish_sync(ctx, s);
 }
 
@@ -1453,9 +1504,7 @@ int run_dev(pf_ctx* ctx, const Job& j, const float* d_times, const float* d_mags
     }
     rc = device_pipeline(ctx, j, L, cfg, p, dcurves, j.out, s);
     if (rc != PF_OK) return rc;
-    PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
-    ctx->done_recorded = true;
-    return PF_OK;
+    return mark_done(ctx, s);
 }
 
 // Copy a host CSR offsets array into the context's device metadata block,
@@ -1736,7 +1785,16 @@ int pf_ctx_create(pf_ctx** out, int device) {
             cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->pend[1].done, cudaEventDisableTiming)) !=
             cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&ctx->ev_prep, cudaEventDisableTiming)) != cudaSuccess) {
+        (e = cudaEventCreateWithFlags(&ctx->ev_prep, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_in_free[0], cudaEventDisableTiming)) !=
+            cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_in_free[1], cudaEventDisableTiming)) !=
+            cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_copied[0], cudaEventDisableTiming)) !=
+            cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_copied[1], cudaEventDisableTiming)) !=
+            cudaSuccess) {
         g_create_error = cudaGetErrorString(e);
         pf_ctx_destroy(ctx);
         return PF_ECUDA;
@@ -1749,11 +1807,12 @@ void pf_ctx_destroy(pf_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     if (ctx->done_recorded) cudaEventSynchronize(ctx->ev_done);
     if (ctx->prep_pending) cudaEventSynchronize(ctx->ev_prep);
     for (DevBuf* b : {&ctx->d_in, &ctx->d_aux32, &ctx->d_aux64, &ctx->d_out, &ctx->d_pidx,
                       &ctx->d_pval, &ctx->d_pack, &ctx->d_misc, &ctx->d_stamps, &ctx->d_stat, &ctx->d_bins,
-                      &ctx->d_prep})
+                      &ctx->d_prep, &ctx->d_in2})
         if (b->p) cudaFree(b->p);
     if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
     if (ctx->h_res.p) cudaFreeHost(ctx->h_res.p);
@@ -1766,6 +1825,10 @@ void pf_ctx_destroy(pf_ctx* ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->ev_staged) cudaEventDestroy(ctx->ev_staged);
     if (ctx->ev_done) cudaEventDestroy(ctx->ev_done);
+    for (cudaEvent_t ev : {ctx->ev_in_free[0], ctx->ev_in_free[1], ctx->ev_copied[0],
+                           ctx->ev_copied[1]})
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1885,9 +1948,7 @@ int pf_ls_eval_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
     const int order = d_d2pdw2 ? 2 : (d_dpdw ? 1 : 0);
     PF_CUDA(launch_ls_eval(p, order, s), "LS derivative kernel");
     ctx->launches++;
-    PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
-    ctx->done_recorded = true;
-    return PF_OK;
+    return mark_done(ctx, s);
 }
 
 int pf_ls_backward_dev(pf_ctx* ctx, const float* d_times, const int64_t* offsets,
@@ -1919,9 +1980,7 @@ int pf_ls_backward_dev(pf_ctx* ctx, const float* d_times, const int64_t* offsets
     p.grad_mags = d_grad_mags;
     PF_CUDA(launch_ls_grad(p, max_len, s), "LS backward kernel");
     ctx->launches++;
-    PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
-    ctx->done_recorded = true;
-    return PF_OK;
+    return mark_done(ctx, s);
 }
 
 int pf_ls_refine_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
@@ -1951,9 +2010,7 @@ int pf_ls_refine_dev(pf_ctx* ctx, const float* d_times, const float* d_mags,
     p.omega_out = d_omega;
     PF_CUDA(launch_ls_refine(p, s), "LS Newton refinement kernel");
     ctx->launches++;
-    PF_CUDA(cudaEventRecord(ctx->ev_done, s), "event");
-    ctx->done_recorded = true;
-    return PF_OK;
+    return mark_done(ctx, s);
 }
 
 int pf_fold_phase_dev(pf_ctx* ctx, int mode, const float* d_times, uint64_t n,
