@@ -264,7 +264,9 @@ int cuda_fail(pf_ctx* ctx, cudaError_t e, const char* what) {
 // on the caller's).  Each call orders its first use of the buffers after
 // the previous call's last (order_after_previous) and marks its own end
 // (mark_done), so a call never overwrites inputs, descriptors or queue
-// counters that an earlier call's kernels still read.
+// counters that an earlier call's kernels still read.  The one exception is
+// a host call's input copy, which goes to the input block the previous call
+// did not use and waits only for that block's last reader (ev_in_free).
 int order_after_previous(pf_ctx* ctx, cudaStream_t s) {
     if (ctx->done_recorded) PF_CUDA(cudaStreamWaitEvent(s, ctx->ev_done, 0), "stream wait");
     return PF_OK;
