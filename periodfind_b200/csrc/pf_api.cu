@@ -1619,7 +1619,9 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
     const size_t bytes = o_pdt + align_up(n_pdt * 4, 256);
     if ((rc = staging_ready(ctx)) != PF_OK) return rc;
     if ((rc = ensure_pinned(ctx, ctx->h_in, bytes)) != PF_OK) return rc;
-    if ((rc = ensure_dev(ctx, ctx->d_in, bytes)) != PF_OK) return rc;
+    const int slot = ctx->in_slot;  // the input block (see run_host)
+    DevBuf& din = slot ? ctx->d_in2 : ctx->d_in;
+    if ((rc = ensure_dev(ctx, din, bytes)) != PF_OK) return rc;
     char* hb = (char*)ctx->h_in.p;
     float* ht = (float*)hb;
     float* hiv = (float*)(hb + o_iv);
@@ -1669,11 +1671,19 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
     memcpy(hb + o_per, periods, n_per * 4);
     memcpy(hb + o_pdt, pdts, n_pdt * 4);
     cudaStream_t s = ctx->stream;
-    char* db = (char*)ctx->d_in.p;
+    char* db = (char*)din.p;
     if ((rc = order_after_previous(ctx, s)) != PF_OK) return rc;
-    PF_CUDA(cudaMemcpyAsync(db, hb, bytes, cudaMemcpyHostToDevice, s), "H2D inputs");
-    PF_CUDA(cudaEventRecord(ctx->ev_staged, s), "event");
+    // As run_host: the copy on the copy stream after this block's last
+    // reader, the kernels after the copy.
+    CallEnd call_end{ctx, s};
+    PF_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_in_free[slot], 0), "stream wait");
+    PF_CUDA(cudaMemcpyAsync(db, hb, bytes, cudaMemcpyHostToDevice, ctx->copy_stream),
+            "H2D inputs");
+    PF_CUDA(cudaEventRecord(ctx->ev_copied[slot], ctx->copy_stream), "event");
+    PF_CUDA(cudaEventRecord(ctx->ev_staged, ctx->copy_stream), "event");
     ctx->staged_pending = true;
+    ctx->in_slot = slot ^ 1;
+    PF_CUDA(cudaStreamWaitEvent(s, ctx->ev_copied[slot], 0), "stream wait");
     const size_t out_bytes = (size_t)n_curves * n_cells * 4;
     if ((rc = ensure_dev(ctx, ctx->d_out, out_bytes)) != PF_OK) return rc;
     FpwParams p{};
@@ -1724,11 +1734,17 @@ int run_fpw(pf_ctx* ctx, const float* const* times, const float* const* mags,
             ctx->launches++;
         }
         if ((rc = copy_peaks_back(ctx, j, async, s)) != PF_OK) return rc;
-        if (async) return mark_done(ctx, s);
+        if (async) {
+            ctx->cur_slot = slot;
+            call_end.armed = false;
+            return mark_done(ctx, s);
+        }
     } else {
         PF_CUDA(cudaMemcpyAsync(out, p.out, out_bytes, cudaMemcpyDeviceToHost, s),
                 "D2H periodogram");
     }
+    ctx->cur_slot = slot;
+    call_end.armed = false;
     return finish_sync(ctx, s);
 }
 
